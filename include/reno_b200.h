@@ -1,0 +1,196 @@
+/*
+ * reno_b200.h -- C ABI of the B200 sweep engine for Renormalizer's MPS sweep
+ * hot path (effective-Hamiltonian matvec, environment updates, Krylov /
+ * Davidson vector kernels, quantum-number block gather/scatter).
+ *
+ * Conventions
+ *  - Every entry point returns an int status; RENO_OK (0) is success.  The
+ *    message of the last failure is returned by reno_last_error().
+ *  - Tensor arguments are DEVICE pointers owned by the caller, C-contiguous, in
+ *    the reference's index order (cited per entry point).  complex128 is
+ *    interleaved (re, im) doubles, 16-byte aligned.
+ *  - Hot calls never allocate: scratch memory ("workspace") is passed in by
+ *    the caller and sized by the matching *_workspace_bytes query.
+ *  - Work is enqueued on the context's stream (reno_ctx_set_stream); calls are
+ *    asynchronous unless documented otherwise.  One context per host thread.
+ *
+ * Reference interfaces replaced (paths inside the Renormalizer project):
+ *  - reno_heff_apply   <- renormalizer/mps/hop_expr.py:7-117  hop_expr(...)(psi)
+ *  - reno_env_update   <- renormalizer/mps/lib.py:169-250     contract_one_site
+ *  - reno_vec_*        <- renormalizer/lib/krylov/krylov.py:27-84 (vdot, norm,
+ *                         axpy, V @ coeffs, allclose) and the vector algebra
+ *                         of renormalizer/lib/davidson/davidson.py:154-441
+ *  - reno_qn_gather / reno_qn_scatter_cols
+ *                      <- renormalizer/mps/svd_qn.py:177-213 (block take) and
+ *                         svd_qn.py:89-96 blockrecover, lib.py:302-316
+ *                         select_basis column copy
+ *  - reno_heff_diag    <- renormalizer/mps/gs.py:419-445 hdiag einsums
+ */
+#ifndef RENO_B200_H
+#define RENO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (the Python shim maps them onto the reference's exceptions) */
+enum {
+  RENO_OK = 0,
+  RENO_ERR_INVALID = 1,   /* shape / argument violation   -> AssertionError/ValueError */
+  RENO_ERR_OOM = 2,       /* device allocation failure    -> MemoryError */
+  RENO_ERR_CUDA = 3,      /* CUDA runtime error           -> RuntimeError */
+  RENO_ERR_WORKSPACE = 4, /* workspace smaller than query -> MemoryError */
+  RENO_ERR_NONFINITE = 5, /* NaN/Inf met                  -> FloatingPointError */
+  RENO_ERR_UNSUPPORTED = 6
+};
+
+/* element types */
+enum { RENO_F64 = 0, RENO_C128 = 1 };
+
+/* arithmetic used for the tensor contractions */
+enum {
+  RENO_PREC_FP64 = 0,   /* FP64 DMMA, complex as four real products          */
+  RENO_PREC_BF16X3 = 1, /* BF16 hi/lo split, three products, FP32 accumulate */
+  RENO_PREC_TF32X3 = 2  /* TF32 hi/lo split, three products, FP32 accumulate */
+};
+
+typedef struct reno_ctx reno_ctx;
+
+int reno_version(void);
+int reno_ctx_create(int device, reno_ctx** out);
+int reno_ctx_destroy(reno_ctx* ctx);
+/* stream: a cudaStream_t (NULL = legacy default stream) */
+int reno_ctx_set_stream(reno_ctx* ctx, void* stream);
+const char* reno_last_error(const reno_ctx* ctx);
+/* blocks until the context's stream is idle */
+int reno_ctx_synchronize(reno_ctx* ctx);
+
+/* ------------------------------------------------------------------------
+ * Effective Hamiltonian matvec, hop_expr.py:57-103 (single layer, no ancilla)
+ *   nsite 0:  y[a,l]     = sum L[a,b,c] R[l,b,k] C[c,k]                 (57-67)
+ *   nsite 1:  y[a,d,l]   = sum L[a,b,c] W1[b,d,e,f] R[l,f,k] psi[c,e,k] (68-79)
+ *   nsite 2:  y[a,d,g,l] = sum L[a,b,c] W1[b,d,e,f] W2[f,g,h,j]
+ *                              R[l,j,k] psi[c,e,h,k]                     (92-103)
+ * Shapes: L (ml, wl, ml); R (mr, wr, mr) (nsite 0: wr == wl);
+ *         W1 (wl, d1, d1, wm) for nsite 2 and (wl, d1, d1, wr) for nsite 1;
+ *         W2 (wm, d2, d2, wr); psi / y (ml, [d1, [d2,]] mr).
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int32_t nsite;
+  int32_t ml, mr;
+  int32_t wl, wm, wr;
+  int32_t d1, d2;
+  int32_t psi_dtype; /* RENO_F64 / RENO_C128; y has the result dtype */
+  int32_t env_dtype; /* dtype of L and R */
+  int32_t mpo_dtype; /* dtype of W1 / W2 */
+  int32_t prec;      /* RENO_PREC_* */
+} reno_heff_desc;
+
+int reno_heff_workspace_bytes(const reno_heff_desc* desc, size_t* bytes);
+int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
+                    const void* W1, const void* W2, const void* R,
+                    const void* psi, void* y, void* workspace,
+                    size_t workspace_bytes);
+
+/* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
+ *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]
+ *   nsite 2: hdiag[a,c,d,f] = sum L[a,b,a] W1[b,c,c,e] W2[e,d,d,g] R[f,g,f]
+ * Only the real part is kept (the Davidson preconditioner is real). */
+int reno_heff_diag(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
+                   const void* W1, const void* W2, const void* R,
+                   double* hdiag);
+
+/* ------------------------------------------------------------------------
+ * Environment update, lib.py:169-250 contract_one_site (3-leg site tensors).
+ *  side 0 ("L", lib.py:200-205):
+ *    out[f,g,h] = sum E[a,b,c] bra[a,d,f] W[b,d,e,g] ket[c,e,h]
+ *    E (mb_in, w_in, mk_in); bra (mb_in, d, mb_out); ket (mk_in, d, mk_out);
+ *    W (w_in, d, d, w_out); out (mb_out, w_out, mk_out)
+ *  side 1 ("R", lib.py:232-237):
+ *    out[f,g,h] = sum bra[f,d,a] E[a,b,c] W[g,d,e,b] ket[h,e,c]
+ *    E (mb_in, w_in, mk_in); bra (mb_out, d, mb_in); ket (mk_out, d, mk_in);
+ *    W (w_out, d, d, w_in); out (mb_out, w_out, mk_out)
+ *  bra is the ALREADY-CONJUGATED bra tensor (the reference's ms_conj); pass
+ *  NULL to use conj(ket) as the reference does when ms_conj is None.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int32_t side;
+  int32_t d;
+  int32_t w_in, w_out;
+  int32_t mk_in, mk_out;
+  int32_t mb_in, mb_out;
+  int32_t env_dtype, ket_dtype, bra_dtype, mpo_dtype;
+  int32_t prec;
+} reno_env_desc;
+
+int reno_env_workspace_bytes(const reno_env_desc* desc, size_t* bytes);
+int reno_env_update(reno_ctx* ctx, const reno_env_desc* desc, const void* E,
+                    const void* W, const void* ket, const void* bra, void* out,
+                    void* workspace, size_t workspace_bytes);
+
+/* ------------------------------------------------------------------------
+ * Vector kernels for the Lanczos exponential (krylov.py:27-84) and Davidson
+ * (davidson.py:154-441).  n counts elements of type dtype.  Scalars that the
+ * reference keeps on the host live in caller-owned DEVICE double arrays here
+ * (complex scalars as (re, im) pairs) so that no host sync is needed between
+ * kernels.  All reductions are two-pass and deterministic (no atomics).
+ * workspace: reno_vec_workspace_bytes(n) bytes.
+ * ---------------------------------------------------------------------- */
+int reno_vec_workspace_bytes(int64_t n, size_t* bytes);
+/* out[0..1] = sum_i conj(x_i) * y_i  (numpy vdot(x, y)) */
+int reno_vec_dotc(reno_ctx* ctx, int64_t n, int32_t dtype, const void* x,
+                  const void* y, double* out, void* workspace, size_t ws_bytes);
+/* out[0] = ||x||_2 ; sets RENO_ERR_NONFINITE status when it is not finite */
+int reno_vec_norm(reno_ctx* ctx, int64_t n, int32_t dtype, const void* x,
+                  double* out, void* workspace, size_t ws_bytes);
+/* Lanczos three-term step, krylov.py:244-245:
+ *   w -= ab[2*j] * v + (j > 0 ? ab[2*j-1] * vprev : 0);  ab[2*j+1] = ||w||
+ * where ab is the device array (alpha_0, beta_0, alpha_1, beta_1, ...). */
+int reno_krylov_orth(reno_ctx* ctx, int64_t n, int32_t dtype, void* w,
+                     const void* v, const void* vprev, double* ab, int32_t j,
+                     void* workspace, size_t ws_bytes);
+/* alpha_j = Re vdot(w, v) into ab[2*j], krylov.py:231 */
+int reno_krylov_alpha(reno_ctx* ctx, int64_t n, int32_t dtype, const void* w,
+                      const void* v, double* ab, int32_t j, void* workspace,
+                      size_t ws_bytes);
+/* out = x / s[0]   (krylov.py:256, V[j+1] = w / beta[j]) */
+int reno_vec_scale_inv(reno_ctx* ctx, int64_t n, int32_t dtype, const void* x,
+                       const double* s, void* out);
+/* out = sum_{j<k} coef[j] * V[j]  with V rows of stride ldv elements;
+ * coef complex (re, im) pairs on the device (krylov.py:24 V @ coeffs). */
+int reno_vec_lincomb(reno_ctx* ctx, int64_t n, int32_t k, int32_t dtype,
+                     const void* V, int64_t ldv, const double* coef, void* out);
+/* flag[0] = 1.0 if allclose(a, b, rtol, atol) elementwise (numpy semantics,
+ * |a-b| <= atol + rtol*|b|, complex modulus) else 0.0   (krylov.py:252) */
+int reno_vec_allclose(reno_ctx* ctx, int64_t n, int32_t dtype, const void* a,
+                      const void* b, double rtol, double atol, double* flag,
+                      void* workspace, size_t ws_bytes);
+/* y += c[0..1] * x   (complex scalar on the device; c_sign multiplies it) */
+int reno_vec_axpy(reno_ctx* ctx, int64_t n, int32_t dtype, void* y,
+                  const void* x, const double* c, double c_sign);
+/* Davidson preconditioner, gs.py:532: out = r / (hdiag - e[0] + shift) */
+int reno_vec_precond(reno_ctx* ctx, int64_t n, int32_t dtype, const void* r,
+                     const double* hdiag, const double* e, double shift,
+                     void* out);
+
+/* ------------------------------------------------------------------------
+ * Quantum-number block movers (svd_qn.py:177-213, 89-96; lib.py:302-316).
+ * reno_qn_gather: out[i, j] = src[rows[i] * ld + cols[j]]   (nr x nc)
+ * reno_qn_scatter_cols: dst[rows[i] * ldd + dcols[j]] = scale_j * src[i * lds + j]
+ *   with scale_j = (sigma ? sigma[j] : 1); rows/cols are int64 device arrays.
+ * ---------------------------------------------------------------------- */
+int reno_qn_gather(reno_ctx* ctx, int32_t dtype, const void* src, int64_t ld,
+                   const int64_t* rows, int64_t nr, const int64_t* cols,
+                   int64_t nc, void* out);
+int reno_qn_scatter_cols(reno_ctx* ctx, int32_t dtype, const void* src,
+                         int64_t lds, const int64_t* rows, int64_t nr,
+                         const int64_t* dcols, int64_t nc, const double* sigma,
+                         void* dst, int64_t ldd);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RENO_B200_H */

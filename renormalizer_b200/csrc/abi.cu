@@ -1,0 +1,42 @@
+// Context management of the C ABI (reno_b200.h).
+#include "reno_common.cuh"
+
+using namespace reno;
+
+extern "C" int reno_version(void) { return 100; }
+
+extern "C" int reno_ctx_create(int device, reno_ctx** out) {
+  if (!out) return RENO_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || device < 0 || device >= n) return RENO_ERR_CUDA;
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return RENO_ERR_CUDA;
+  reno_ctx* c = new reno_ctx();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  *out = c;
+  return RENO_OK;
+}
+
+extern "C" int reno_ctx_destroy(reno_ctx* ctx) {
+  delete ctx;
+  return RENO_OK;
+}
+
+extern "C" int reno_ctx_set_stream(reno_ctx* ctx, void* stream) {
+  if (!ctx) return RENO_ERR_INVALID;
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  return RENO_OK;
+}
+
+extern "C" const char* reno_last_error(const reno_ctx* ctx) {
+  if (!ctx) return "null context";
+  return ctx->last_error.c_str();
+}
+
+extern "C" int reno_ctx_synchronize(reno_ctx* ctx) {
+  if (!ctx) return RENO_ERR_INVALID;
+  return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "reno_ctx_synchronize");
+}

@@ -1,0 +1,241 @@
+// Strided batched FP64 GEMM on the sm_100a double-precision MMA pipe
+// (mma.sync m8n8k4 .f64), complex handled as four real products.
+//
+//   C[b][m][n] (+)= sum_k opA(A)[b][m][k] * opB(B)[b][k][n]
+//
+// Every stage of the H_eff matvec and of the environment update is one call
+// of this kernel with the strides of the reference's C-order tensors, so no
+// operand is ever permuted in HBM (hop_expr.py:57-103, lib.py:200-237).
+// Operands are staged global -> shared with cp.async (zero-filled tails) in a
+// 3-stage ring; each warp owns a 32x32 output tile = 4x4 m8n8 fragments.
+#pragma once
+#include "reno_common.cuh"
+
+namespace reno {
+
+struct GemmOperand {
+  const void* ptr = nullptr;
+  int64_t s_outer = 0;  // stride of the M (A) or N (B) index, in elements
+  int64_t s_k = 0;      // stride of the K index
+  int64_t s_batch = 0;
+  int is_complex = 0;
+  int conj = 0;
+};
+
+struct GemmParams {
+  int M = 0, N = 0, K = 0, batch = 1;
+  GemmOperand A, B;
+  void* C = nullptr;
+  int64_t sCm = 0, sCn = 0, sCb = 0;
+  int accumulate = 0;
+};
+
+namespace fp64gemm {
+
+constexpr int BM = 64, BN = 64, BK = 16, BKP = BK + 4, STAGES = 3, THREADS = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, bool valid) {
+  const int src_bytes = valid ? BYTES : 0;
+  if constexpr (BYTES == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(src_bytes));
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(src_bytes));
+  }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+// Copy one BM(or BN) x BK tile of an operand into shared memory laid out
+// [outer][k] with row pitch BKP.  Thread->element mapping follows whichever
+// global index is unit-stride so that the global reads coalesce.
+template <bool CPLX>
+__device__ __forceinline__ void load_tile(void* smem, const GemmOperand& op, const char* base,
+                                          int outer0, int outer_max, int k0, int K, int tid) {
+  using T = typename std::conditional<CPLX, double2, double>::type;
+  T* s = reinterpret_cast<T*>(smem);
+  const T* g = reinterpret_cast<const T*>(base);
+  constexpr int ELEMS = BM * BK / THREADS;
+  const bool k_fast = (op.s_k == 1);
+#pragma unroll
+  for (int i = 0; i < ELEMS; ++i) {
+    const int idx = tid + i * THREADS;
+    int o, k;
+    if (k_fast) {
+      k = idx % BK;
+      o = idx / BK;
+    } else {
+      o = idx % BM;
+      k = idx / BM;
+    }
+    const int go = outer0 + o, gk = k0 + k;
+    const bool valid = (go < outer_max) && (gk < K);
+    const T* src = valid ? g + (int64_t)go * op.s_outer + (int64_t)gk * op.s_k : g;
+    cp_async_zfill<sizeof(T)>(s + o * BKP + k, src, valid);
+  }
+}
+
+template <bool AC, bool BC>
+__global__ void __launch_bounds__(THREADS) gemm_kernel(GemmParams p) {
+  constexpr bool CC = AC || BC;
+  using TA = typename std::conditional<AC, double2, double>::type;
+  using TB = typename std::conditional<BC, double2, double>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TA* sA = reinterpret_cast<TA*>(smem_raw);
+  TB* sB = reinterpret_cast<TB*>(smem_raw + STAGES * BM * BKP * sizeof(TA));
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm0 = (warp & 1) * 32, wn0 = (warp >> 1) * 32;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int64_t b = blockIdx.z;
+  const char* baseA = reinterpret_cast<const char*>(p.A.ptr) + b * p.A.s_batch * sizeof(TA);
+  const char* baseB = reinterpret_cast<const char*>(p.B.ptr) + b * p.B.s_batch * sizeof(TB);
+
+  double accr[4][4][2], acci[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      accr[i][j][0] = accr[i][j][1] = 0.0;
+      acci[i][j][0] = acci[i][j][1] = 0.0;
+    }
+
+  const int nk = (int)ceil_div(p.K, BK);
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) {
+      load_tile<AC>(sA + s * BM * BKP, p.A, baseA, m0, p.M, s * BK, p.K, tid);
+      load_tile<BC>(sB + s * BN * BKP, p.B, baseB, n0, p.N, s * BK, p.K, tid);
+    }
+    cp_async_commit();
+  }
+
+  const double sgnA = p.A.conj ? -1.0 : 1.0, sgnB = p.B.conj ? -1.0 : 1.0;
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const TA* a_s = sA + (kt % STAGES) * BM * BKP;
+    const TB* b_s = sB + (kt % STAGES) * BN * BKP;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double ar[4], ai[4], br[4], bi[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const TA va = a_s[(wm0 + i * 8 + (lane >> 2)) * BKP + kk + (lane & 3)];
+        if constexpr (AC) {
+          ar[i] = va.x;
+          ai[i] = sgnA * va.y;
+        } else {
+          ar[i] = va;
+          ai[i] = 0.0;
+        }
+        const TB vb = b_s[(wn0 + i * 8 + (lane >> 2)) * BKP + kk + (lane & 3)];
+        if constexpr (BC) {
+          br[i] = vb.x;
+          bi[i] = sgnB * vb.y;
+        } else {
+          br[i] = vb;
+          bi[i] = 0.0;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(accr[i][j][0], accr[i][j][1], ar[i], br[j]);
+          if constexpr (AC && BC) dmma(accr[i][j][0], accr[i][j][1], -ai[i], bi[j]);
+          if constexpr (BC) dmma(acci[i][j][0], acci[i][j][1], ar[i], bi[j]);
+          if constexpr (AC) dmma(acci[i][j][0], acci[i][j][1], ai[i], br[j]);
+        }
+      }
+    }
+    const int ks = kt + STAGES - 1;
+    if (ks < nk) {
+      load_tile<AC>(sA + (ks % STAGES) * BM * BKP, p.A, baseA, m0, p.M, ks * BK, p.K, tid);
+      load_tile<BC>(sB + (ks % STAGES) * BN * BKP, p.B, baseB, n0, p.N, ks * BK, p.K, tid);
+    }
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+
+  // epilogue: fragment (i,j) element e sits at row lane/4, column 2*(lane%4)+e
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int m = m0 + wm0 + i * 8 + (lane >> 2);
+    if (m >= p.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int n = n0 + wn0 + j * 8 + (lane & 3) * 2 + e;
+        if (n >= p.N) continue;
+        const int64_t off = b * p.sCb + (int64_t)m * p.sCm + (int64_t)n * p.sCn;
+        if constexpr (CC) {
+          double2* c = reinterpret_cast<double2*>(p.C) + off;
+          double2 v = make_double2(accr[i][j][e], acci[i][j][e]);
+          if (p.accumulate) {
+            const double2 o = *c;
+            v.x += o.x;
+            v.y += o.y;
+          }
+          *c = v;
+        } else {
+          double* c = reinterpret_cast<double*>(p.C) + off;
+          double v = accr[i][j][e];
+          if (p.accumulate) v += *c;
+          *c = v;
+        }
+      }
+    }
+  }
+}
+
+template <bool AC, bool BC>
+inline size_t smem_bytes() {
+  return STAGES * (BM * BKP * (AC ? 16 : 8) + BN * BKP * (BC ? 16 : 8));
+}
+
+template <bool AC, bool BC>
+inline cudaError_t launch_t(const GemmParams& p, cudaStream_t st) {
+  const size_t sm = smem_bytes<AC, BC>();
+  static bool attr_set = false;  // per process; all devices are sm_100a
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<AC, BC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  dim3 grid((unsigned)ceil_div(p.N, BN), (unsigned)ceil_div(p.M, BM), (unsigned)p.batch);
+  gemm_kernel<AC, BC><<<grid, THREADS, sm, st>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace fp64gemm
+
+// Launch the FP64 GEMM; returns a CUDA error code.
+inline cudaError_t gemm_fp64(const GemmParams& p, cudaStream_t st) {
+  if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return cudaSuccess;
+  const bool ac = p.A.is_complex, bc = p.B.is_complex;
+  if (ac && bc) return fp64gemm::launch_t<true, true>(p, st);
+  if (ac) return fp64gemm::launch_t<true, false>(p, st);
+  if (bc) return fp64gemm::launch_t<false, true>(p, st);
+  return fp64gemm::launch_t<false, false>(p, st);
+}
+
+}  // namespace reno

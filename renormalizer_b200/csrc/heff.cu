@@ -1,0 +1,429 @@
+// Effective-Hamiltonian matvec (hop_expr) and environment update
+// (contract_one_site) as chains of strided GEMM stages.
+//
+// Stage order (all operands in the reference's C-order layouts, no permutes):
+//   1-site  (hop_expr.py:68-79):  T1[a,b,e,k] = L[ab,c] psi[c,ek]
+//                                  T2[a,d,f,k] = Wt[df,be] T1[a][be,k]   (batched over a)
+//                                  y[a,d,l]    = T2[ad,fk] R[l,fk]
+//   2-site  (hop_expr.py:92-103): T1 = L.psi ; T2 = Wt1.T1[a] ; T3 = Wt2.T2[a,d] ; y = T3.R^T
+//   0-site  (hop_expr.py:57-67):  T1[a,b,k] = L[ab,c] C[c,k] ; y[a,l] = T1[a,bk] R[l,bk]
+//   env L   (lib.py:200-205):     T1 = E.ket ; T2 = Wt.T1[a] ; out[f,gh] = bra[ad,f] T2[ad,gh]
+//   env R   (lib.py:232-237):     the L form on the bond-transposed bra/ket and W with its
+//                                  two MPO bonds swapped (an R update is an L update of the
+//                                  mirrored chain)
+#include "reno_common.cuh"
+#include "gemm_fp64.cuh"
+#include "split_gemm.cuh"
+
+namespace reno {
+
+static inline int64_t esz(int dt) { return dt == RENO_C128 ? 16 : 8; }
+static inline int promote(int a, int b) { return (a == RENO_C128 || b == RENO_C128) ? RENO_C128 : RENO_F64; }
+static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Wt[(dd, r), (c, e)] from W.  mode 0: W is (nc, d, d, nr) indexed [c,dd,e,r];
+// mode 1: W is (nr, d, d, nc) indexed [r,dd,e,c] (MPO bonds swapped).
+template <typename T>
+__global__ void wt_kernel(const T* __restrict__ W, T* __restrict__ Wt, int nc, int d, int nr, int mode) {
+  const int64_t total = (int64_t)d * nr * nc * d;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int e = idx % d;
+    const int c = (idx / d) % nc;
+    const int r = (idx / ((int64_t)d * nc)) % nr;
+    const int dd = idx / ((int64_t)d * nc * nr);
+    int64_t widx;
+    if (mode == 0)
+      widx = (((int64_t)c * d + dd) * d + e) * nr + r;
+    else
+      widx = (((int64_t)r * d + dd) * d + e) * nc + c;
+    Wt[idx] = W[widx];
+  }
+}
+
+// out[c,e,h] = in[h,e,c] : in (n0, d, n2) -> out (n2, d, n0)
+template <typename T>
+__global__ void swap13_kernel(const T* __restrict__ in, T* __restrict__ out, int n0, int d, int n2) {
+  const int64_t total = (int64_t)n0 * d * n2;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int h = idx % n0;
+    const int e = (idx / n0) % d;
+    const int c = idx / ((int64_t)n0 * d);
+    out[idx] = in[((int64_t)h * d + e) * n2 + c];
+  }
+}
+
+static int grid_for(int64_t total) {
+  int64_t g = ceil_div(total, 256);
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+static cudaError_t launch_wt(const void* W, void* Wt, int dt, int nc, int d, int nr, int mode, cudaStream_t st) {
+  const int64_t total = (int64_t)d * nr * nc * d;
+  if (dt == RENO_C128)
+    wt_kernel<double2><<<grid_for(total), 256, 0, st>>>((const double2*)W, (double2*)Wt, nc, d, nr, mode);
+  else
+    wt_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)W, (double*)Wt, nc, d, nr, mode);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_swap13(const void* in, void* out, int dt, int n0, int d, int n2, cudaStream_t st) {
+  const int64_t total = (int64_t)n0 * d * n2;
+  if (dt == RENO_C128)
+    swap13_kernel<double2><<<grid_for(total), 256, 0, st>>>((const double2*)in, (double2*)out, n0, d, n2);
+  else
+    swap13_kernel<double><<<grid_for(total), 256, 0, st>>>((const double*)in, (double*)out, n0, d, n2);
+  return cudaGetLastError();
+}
+
+static GemmOperand opnd(const void* p, int dt, int64_t s_outer, int64_t s_k, int64_t s_b = 0, int conj = 0) {
+  GemmOperand o;
+  o.ptr = p;
+  o.is_complex = dt == RENO_C128;
+  o.s_outer = s_outer;
+  o.s_k = s_k;
+  o.s_batch = s_b;
+  o.conj = conj;
+  return o;
+}
+
+static GemmParams gp(int M, int N, int K, int batch, GemmOperand A, GemmOperand B, void* C, int64_t sCm,
+                     int64_t sCn, int64_t sCb = 0) {
+  GemmParams p;
+  p.M = M;
+  p.N = N;
+  p.K = K;
+  p.batch = batch;
+  p.A = A;
+  p.B = B;
+  p.C = C;
+  p.sCm = sCm;
+  p.sCn = sCn;
+  p.sCb = sCb;
+  return p;
+}
+
+// Dispatch one GEMM stage at the requested arithmetic.  `big` marks the
+// O(M^3) stages that the split-precision tensor-core kernel takes over.
+static cudaError_t run_stage(const GemmParams& p, int prec, void* split_ws, size_t split_ws_bytes, cudaStream_t st) {
+  if (prec == RENO_PREC_FP64) return gemm_fp64(p, st);
+  return split_gemm(p, prec, split_ws, split_ws_bytes, st);
+}
+
+// ---------------------------------------------------------------- heff
+struct HeffPlan {
+  int dt_T1, dt_T2, dt_T3, dt_y;
+  size_t off_wt1, off_wt2, off_t1, off_t2, off_split, total, split_bytes;
+};
+
+static int validate_heff(const reno_heff_desc* d) {
+  if (!d) return RENO_ERR_INVALID;
+  if (d->nsite < 0 || d->nsite > 2) return RENO_ERR_INVALID;
+  if (d->ml <= 0 || d->mr <= 0 || d->wl <= 0 || d->wr <= 0) return RENO_ERR_INVALID;
+  if (d->nsite >= 1 && d->d1 <= 0) return RENO_ERR_INVALID;
+  if (d->nsite == 2 && (d->d2 <= 0 || d->wm <= 0)) return RENO_ERR_INVALID;
+  if (d->nsite == 0 && d->wl != d->wr) return RENO_ERR_INVALID;
+  for (int t : {d->psi_dtype, d->env_dtype, d->mpo_dtype})
+    if (t != RENO_F64 && t != RENO_C128) return RENO_ERR_INVALID;
+  if (d->prec < RENO_PREC_FP64 || d->prec > RENO_PREC_TF32X3) return RENO_ERR_INVALID;
+  return RENO_OK;
+}
+
+static HeffPlan plan_heff(const reno_heff_desc* d) {
+  HeffPlan p{};
+  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wm = d->wm, wr = d->wr, d1 = d->d1, d2 = d->d2;
+  p.dt_T1 = promote(d->env_dtype, d->psi_dtype);
+  p.dt_T2 = promote(p.dt_T1, d->mpo_dtype);
+  p.dt_T3 = p.dt_T2;
+  p.dt_y = promote(p.dt_T2, d->env_dtype);
+  size_t off = 0;
+  int64_t n_wt1 = 0, n_wt2 = 0, n_t1 = 0, n_t2 = 0;
+  if (d->nsite == 0) {
+    p.dt_T2 = p.dt_T1;
+    p.dt_y = p.dt_T1;
+    n_t1 = ml * wl * mr;
+  } else if (d->nsite == 1) {
+    n_wt1 = d1 * wr * wl * d1;
+    n_t1 = ml * wl * d1 * mr;
+    n_t2 = ml * d1 * wr * mr;
+  } else {
+    n_wt1 = d1 * wm * wl * d1;
+    n_wt2 = d2 * wr * wm * d2;
+    n_t1 = std::max(ml * wl * d1 * d2 * mr, ml * d1 * d2 * wr * mr);  // T1, later reused for T3
+    n_t2 = ml * d1 * wm * d2 * mr;
+  }
+  p.off_wt1 = off;
+  off = align256(off + n_wt1 * esz(d->mpo_dtype));
+  p.off_wt2 = off;
+  off = align256(off + n_wt2 * esz(d->mpo_dtype));
+  p.off_t1 = off;
+  off = align256(off + n_t1 * esz(p.dt_T2));
+  p.off_t2 = off;
+  off = align256(off + n_t2 * esz(p.dt_T2));
+  p.off_split = off;
+  p.split_bytes = 0;
+  if (d->prec != RENO_PREC_FP64) {
+    // the split kernel stages operands of the largest GEMM in its own format
+    const int64_t big_a = std::max<int64_t>(ml * wl * ml, ml * d1 * std::max<int64_t>(d2, 1) * wr * mr);
+    const int64_t big_b = std::max<int64_t>(ml * d1 * std::max<int64_t>(d2, 1) * mr, wr * mr * mr);
+    p.split_bytes = split_gemm_workspace_bytes(big_a, big_b);
+    off = align256(off + p.split_bytes);
+  }
+  p.total = off;
+  return p;
+}
+
+}  // namespace reno
+
+using namespace reno;
+
+extern "C" int reno_heff_workspace_bytes(const reno_heff_desc* d, size_t* bytes) {
+  if (validate_heff(d) != RENO_OK || !bytes) return RENO_ERR_INVALID;
+  *bytes = plan_heff(d).total;
+  return RENO_OK;
+}
+
+extern "C" int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* d, const void* L, const void* W1,
+                               const void* W2, const void* R, const void* psi, void* y, void* ws,
+                               size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (validate_heff(d) != RENO_OK) return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply: invalid descriptor");
+  if (!L || !R || !psi || !y || (d->nsite >= 1 && !W1) || (d->nsite == 2 && !W2))
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply: null tensor pointer");
+  const HeffPlan p = plan_heff(d);
+  if (ws_bytes < p.total || (p.total > 0 && !ws))
+    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heff_apply: workspace too small");
+  char* w = static_cast<char*>(ws);
+  void* Wt1 = w + p.off_wt1;
+  void* Wt2 = w + p.off_wt2;
+  void* T1 = w + p.off_t1;
+  void* T2 = w + p.off_t2;
+  void* sws = w + p.off_split;
+  cudaStream_t st = ctx->stream;
+  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wm = d->wm, wr = d->wr, d1 = d->d1, d2 = d->d2;
+  const int ev = d->env_dtype, pv = d->psi_dtype, mv = d->mpo_dtype;
+  cudaError_t e = cudaSuccess;
+
+  if (d->nsite == 0) {
+    e = run_stage(gp(ml * wl, mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, mr), T1, mr, 1), d->prec, sws,
+                  p.split_bytes, st);
+    if (e == cudaSuccess)
+      e = run_stage(gp(ml, mr, wl * mr, 1, opnd(T1, p.dt_T1, wl * mr, 1), opnd(R, ev, wl * mr, 1), y, mr, 1),
+                    d->prec, sws, p.split_bytes, st);
+  } else if (d->nsite == 1) {
+    e = launch_wt(W1, Wt1, mv, wl, d1, wr, 0, st);
+    if (e == cudaSuccess)
+      e = run_stage(gp(ml * wl, d1 * mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, d1 * mr), T1, d1 * mr, 1),
+                    d->prec, sws, p.split_bytes, st);
+    if (e == cudaSuccess)
+      e = run_stage(gp(d1 * wr, mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1), opnd(T1, p.dt_T1, 1, mr, wl * d1 * mr),
+                       T2, mr, 1, d1 * wr * mr),
+                    RENO_PREC_FP64, sws, p.split_bytes, st);
+    if (e == cudaSuccess)
+      e = run_stage(gp(ml * d1, mr, wr * mr, 1, opnd(T2, p.dt_T2, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1),
+                    d->prec, sws, p.split_bytes, st);
+  } else {
+    e = launch_wt(W1, Wt1, mv, wl, d1, wm, 0, st);
+    if (e == cudaSuccess) e = launch_wt(W2, Wt2, mv, wm, d2, wr, 0, st);
+    const int64_t n12 = d1 * d2 * mr;
+    if (e == cudaSuccess)
+      e = run_stage(gp(ml * wl, n12, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, n12), T1, n12, 1), d->prec, sws,
+                    p.split_bytes, st);
+    if (e == cudaSuccess)
+      e = run_stage(gp(d1 * wm, d2 * mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1),
+                       opnd(T1, p.dt_T1, 1, d2 * mr, wl * d1 * d2 * mr), T2, d2 * mr, 1, d1 * wm * d2 * mr),
+                    RENO_PREC_FP64, sws, p.split_bytes, st);
+    void* T3 = T1;
+    if (e == cudaSuccess)
+      e = run_stage(gp(d2 * wr, mr, wm * d2, ml * d1, opnd(Wt2, mv, wm * d2, 1),
+                       opnd(T2, p.dt_T2, 1, mr, wm * d2 * mr), T3, mr, 1, d2 * wr * mr),
+                    RENO_PREC_FP64, sws, p.split_bytes, st);
+    if (e == cudaSuccess)
+      e = run_stage(gp(ml * d1 * d2, mr, wr * mr, 1, opnd(T3, p.dt_T3, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr,
+                       1),
+                    d->prec, sws, p.split_bytes, st);
+  }
+  return check_cuda(ctx, e, "reno_heff_apply");
+}
+
+// ---------------------------------------------------------------- env update
+namespace reno {
+struct EnvPlan {
+  int dt_T1, dt_T2, dt_out;
+  size_t off_ketT, off_braT, off_wt, off_t1, off_t2, off_split, total, split_bytes;
+};
+
+static int validate_env(const reno_env_desc* d) {
+  if (!d) return RENO_ERR_INVALID;
+  if (d->side != 0 && d->side != 1) return RENO_ERR_INVALID;
+  if (d->d <= 0 || d->w_in <= 0 || d->w_out <= 0 || d->mk_in <= 0 || d->mk_out <= 0 || d->mb_in <= 0 ||
+      d->mb_out <= 0)
+    return RENO_ERR_INVALID;
+  for (int t : {d->env_dtype, d->ket_dtype, d->bra_dtype, d->mpo_dtype})
+    if (t != RENO_F64 && t != RENO_C128) return RENO_ERR_INVALID;
+  if (d->prec < RENO_PREC_FP64 || d->prec > RENO_PREC_TF32X3) return RENO_ERR_INVALID;
+  return RENO_OK;
+}
+
+static EnvPlan plan_env(const reno_env_desc* d) {
+  EnvPlan p{};
+  const int64_t dd = d->d, wi = d->w_in, wo = d->w_out, ki = d->mk_in, ko = d->mk_out, bi = d->mb_in,
+                bo = d->mb_out;
+  p.dt_T1 = promote(d->env_dtype, d->ket_dtype);
+  p.dt_T2 = promote(p.dt_T1, d->mpo_dtype);
+  p.dt_out = promote(p.dt_T2, d->bra_dtype);
+  size_t off = 0;
+  p.off_ketT = off;
+  if (d->side == 1) off = align256(off + ki * dd * ko * esz(d->ket_dtype));
+  p.off_braT = off;
+  if (d->side == 1) off = align256(off + bi * dd * bo * esz(d->bra_dtype));
+  p.off_wt = off;
+  off = align256(off + dd * wo * wi * dd * esz(d->mpo_dtype));
+  p.off_t1 = off;
+  off = align256(off + bi * wi * dd * ko * esz(p.dt_T1));
+  p.off_t2 = off;
+  off = align256(off + bi * dd * wo * ko * esz(p.dt_T2));
+  p.off_split = off;
+  p.split_bytes = 0;
+  if (d->prec != RENO_PREC_FP64) {
+    const int64_t big_a = std::max<int64_t>(bi * wi * ki, bo * bi * dd);
+    const int64_t big_b = std::max<int64_t>(ki * dd * ko, bi * dd * wo * ko);
+    p.split_bytes = split_gemm_workspace_bytes(big_a, big_b);
+    off = align256(off + p.split_bytes);
+  }
+  p.total = off;
+  return p;
+}
+}  // namespace reno
+
+extern "C" int reno_env_workspace_bytes(const reno_env_desc* d, size_t* bytes) {
+  if (validate_env(d) != RENO_OK || !bytes) return RENO_ERR_INVALID;
+  *bytes = plan_env(d).total;
+  return RENO_OK;
+}
+
+extern "C" int reno_env_update(reno_ctx* ctx, const reno_env_desc* d, const void* E, const void* W,
+                               const void* ket, const void* bra, void* out, void* ws, size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (validate_env(d) != RENO_OK) return set_error(ctx, RENO_ERR_INVALID, "reno_env_update: invalid descriptor");
+  if (!E || !W || !ket || !out) return set_error(ctx, RENO_ERR_INVALID, "reno_env_update: null tensor pointer");
+  if (!bra && (d->mb_in != d->mk_in || d->mb_out != d->mk_out))
+    return set_error(ctx, RENO_ERR_INVALID, "reno_env_update: bra == NULL needs bra dims == ket dims");
+  const EnvPlan p = plan_env(d);
+  if (ws_bytes < p.total || !ws) return set_error(ctx, RENO_ERR_WORKSPACE, "reno_env_update: workspace too small");
+  char* w = static_cast<char*>(ws);
+  cudaStream_t st = ctx->stream;
+  const int64_t dd = d->d, wi = d->w_in, wo = d->w_out, ki = d->mk_in, ko = d->mk_out, bi = d->mb_in,
+                bo = d->mb_out;
+  const void* k_op = ket;
+  const void* b_op = bra;
+  int bra_dt = bra ? d->bra_dtype : d->ket_dtype;
+  cudaError_t e = cudaSuccess;
+  if (d->side == 1) {
+    // mirror: ketT[c,e,h] = ket[h,e,c], braT[a,d,f] = bra[f,d,a]
+    e = launch_swap13(ket, w + p.off_ketT, d->ket_dtype, (int)ko, (int)dd, (int)ki, st);
+    k_op = w + p.off_ketT;
+    if (e == cudaSuccess && bra) {
+      e = launch_swap13(bra, w + p.off_braT, d->bra_dtype, (int)bo, (int)dd, (int)bi, st);
+      b_op = w + p.off_braT;
+    }
+  }
+  const int conj_bra = bra ? 0 : 1;
+  if (!bra) b_op = k_op;
+  void* Wt = w + p.off_wt;
+  void* T1 = w + p.off_t1;
+  void* T2 = w + p.off_t2;
+  void* sws = w + p.off_split;
+  if (e == cudaSuccess) e = launch_wt(W, Wt, d->mpo_dtype, (int)wi, (int)dd, (int)wo, d->side == 1 ? 1 : 0, st);
+  if (e == cudaSuccess)
+    e = run_stage(gp(bi * wi, dd * ko, ki, 1, opnd(E, d->env_dtype, ki, 1), opnd(k_op, d->ket_dtype, 1, dd * ko), T1,
+                     dd * ko, 1),
+                  d->prec, sws, p.split_bytes, st);
+  if (e == cudaSuccess)
+    e = run_stage(gp(dd * wo, ko, wi * dd, bi, opnd(Wt, d->mpo_dtype, wi * dd, 1),
+                     opnd(T1, p.dt_T1, 1, ko, wi * dd * ko), T2, ko, 1, dd * wo * ko),
+                  RENO_PREC_FP64, sws, p.split_bytes, st);
+  if (e == cudaSuccess)
+    e = run_stage(gp(bo, wo * ko, bi * dd, 1, opnd(b_op, bra_dt, 1, bo, 0, conj_bra), opnd(T2, p.dt_T2, 1, wo * ko),
+                     out, wo * ko, 1),
+                  d->prec, sws, p.split_bytes, st);
+  return check_cuda(ctx, e, "reno_env_update");
+}
+
+// ---------------------------------------------------------------- hdiag
+namespace reno {
+__device__ __forceinline__ double real_of(double v) { return v; }
+__device__ __forceinline__ double real_of(double2 v) { return v.x; }
+
+// hdiag[a, c, (dd,) f] = Re sum L[a,b,a] W1[b,c,c,e] (W2[e,dd,dd,g]) R[f,g,f]
+// Real part only: the reference forms it from real DMRG tensors (gs.py:419-445).
+template <typename TE, typename TW>
+__global__ void hdiag_kernel(const TE* L, const TW* W1, const TW* W2, const TE* R, double* out, int nsite, int ml,
+                             int mr, int wl, int wm, int wr, int d1, int d2) {
+  const int dd2 = nsite == 2 ? d2 : 1;
+  const int64_t total = (int64_t)ml * d1 * dd2 * mr;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int f = idx % mr;
+    const int dd = (idx / mr) % dd2;
+    const int c = (idx / ((int64_t)mr * dd2)) % d1;
+    const int a = idx / ((int64_t)mr * dd2 * d1);
+    double acc = 0.0;
+    if (nsite == 1) {
+      for (int b = 0; b < wl; ++b) {
+        const double lv = real_of(L[((int64_t)a * wl + b) * ml + a]);
+        if (lv == 0.0) continue;
+        for (int g = 0; g < wr; ++g) {
+          const double wv = real_of(W1[(((int64_t)b * d1 + c) * d1 + c) * wr + g]);
+          if (wv == 0.0) continue;
+          acc += lv * wv * real_of(R[((int64_t)f * wr + g) * mr + f]);
+        }
+      }
+    } else {
+      for (int b = 0; b < wl; ++b) {
+        const double lv = real_of(L[((int64_t)a * wl + b) * ml + a]);
+        if (lv == 0.0) continue;
+        for (int e = 0; e < wm; ++e) {
+          const double w1 = real_of(W1[(((int64_t)b * d1 + c) * d1 + c) * wm + e]);
+          if (w1 == 0.0) continue;
+          for (int g = 0; g < wr; ++g) {
+            const double w2 = real_of(W2[(((int64_t)e * d2 + dd) * d2 + dd) * wr + g]);
+            if (w2 == 0.0) continue;
+            acc += lv * w1 * w2 * real_of(R[((int64_t)f * wr + g) * mr + f]);
+          }
+        }
+      }
+    }
+    out[idx] = acc;
+  }
+}
+}  // namespace reno
+
+extern "C" int reno_heff_diag(reno_ctx* ctx, const reno_heff_desc* d, const void* L, const void* W1, const void* W2,
+                              const void* R, double* hdiag) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (validate_heff(d) != RENO_OK || d->nsite < 1)
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heff_diag: invalid descriptor");
+  if (!L || !W1 || !R || !hdiag || (d->nsite == 2 && !W2))
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heff_diag: null pointer");
+  const int64_t total = (int64_t)d->ml * d->d1 * (d->nsite == 2 ? d->d2 : 1) * d->mr;
+  const int g = grid_for(total);
+  const bool ec = d->env_dtype == RENO_C128, wc = d->mpo_dtype == RENO_C128;
+#define HD(TE, TW)                                                                                         \
+  hdiag_kernel<TE, TW><<<g, 256, 0, ctx->stream>>>((const TE*)L, (const TW*)W1, (const TW*)W2, (const TE*)R, \
+                                                    hdiag, d->nsite, d->ml, d->mr, d->wl, d->wm, d->wr, d->d1,   \
+                                                    d->d2)
+  if (ec && wc)
+    HD(double2, double2);
+  else if (ec)
+    HD(double2, double);
+  else if (wc)
+    HD(double, double2);
+  else
+    HD(double, double);
+#undef HD
+  return check_cuda(ctx, cudaGetLastError(), "reno_heff_diag");
+}

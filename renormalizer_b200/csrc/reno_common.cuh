@@ -1,0 +1,43 @@
+// Shared definitions for the sweep-engine kernels (sm_100a).
+//
+// Every C-ABI entry point returns an int status (RENO_OK == 0).  Errors are
+// recorded in the context (reno_last_error) so the Python shim can raise the
+// exception type the reference raises for the same condition.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include "../../include/reno_b200.h"
+
+struct reno_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  std::string last_error;
+  // pinned host slots for scalars read back by the host (Krylov alpha/beta ...)
+  double* host_scalars = nullptr;
+};
+
+namespace reno {
+
+inline int set_error(reno_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return code;
+}
+
+inline int check_cuda(reno_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return RENO_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return set_error(ctx, e == cudaErrorMemoryAllocation ? RENO_ERR_OOM : RENO_ERR_CUDA, m);
+}
+
+#define RENO_LAUNCH_CHECK(ctx, what)                                     \
+  do {                                                                   \
+    cudaError_t _e = cudaGetLastError();                                 \
+    if (_e != cudaSuccess) return ::reno::check_cuda((ctx), _e, (what)); \
+  } while (0)
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace reno
