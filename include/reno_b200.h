@@ -20,7 +20,7 @@
  *  - reno_vec_*        <- renormalizer/lib/krylov/krylov.py:27-84 (vdot, norm,
  *                         axpy, V @ coeffs, allclose) and the vector algebra
  *                         of renormalizer/lib/davidson/davidson.py:154-441
- *  - reno_qn_gather / reno_qn_scatter_cols
+ *  - reno_qn_gather / reno_qn_scatter
  *                      <- renormalizer/mps/svd_qn.py:177-213 (block take) and
  *                         svd_qn.py:89-96 blockrecover, lib.py:302-316
  *                         select_basis column copy
@@ -67,6 +67,8 @@ int reno_ctx_set_stream(reno_ctx* ctx, void* stream);
 const char* reno_last_error(const reno_ctx* ctx);
 /* blocks until the context's stream is idle */
 int reno_ctx_synchronize(reno_ctx* ctx);
+/* number of kernels this library has launched in the process so far */
+int reno_launch_count(long long* count);
 
 /* ------------------------------------------------------------------------
  * Effective Hamiltonian matvec, hop_expr.py:57-103 (single layer, no ancilla)
@@ -94,6 +96,16 @@ int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
                     const void* W1, const void* W2, const void* R,
                     const void* psi, void* y, void* workspace,
                     size_t workspace_bytes);
+
+/* Plain strided GEMM on the same FP64 tensor-core kernel (used for the
+ * bond-absorb products of the sweeps, mps.py:1361/1394 tensordot):
+ *   C[m, n] = sum_k opA(A)[m, k] opB(B)[k, n],  C row stride c_rs, unit column
+ *   stride; A[m,k] at m*a_rs + k*a_cs, B[k,n] at k*b_rs + n*b_cs; *_conj
+ *   conjugates an operand; C is complex128 if A or B is. */
+int reno_gemm(reno_ctx* ctx, int32_t M, int32_t N, int32_t K, const void* A,
+              int32_t a_dtype, int64_t a_rs, int64_t a_cs, int32_t a_conj,
+              const void* B, int32_t b_dtype, int64_t b_rs, int64_t b_cs,
+              int32_t b_conj, void* C, int64_t c_rs, int32_t prec);
 
 /* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
  *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]
@@ -143,7 +155,7 @@ int reno_vec_workspace_bytes(int64_t n, size_t* bytes);
 /* out[0..1] = sum_i conj(x_i) * y_i  (numpy vdot(x, y)) */
 int reno_vec_dotc(reno_ctx* ctx, int64_t n, int32_t dtype, const void* x,
                   const void* y, double* out, void* workspace, size_t ws_bytes);
-/* out[0] = ||x||_2 ; sets RENO_ERR_NONFINITE status when it is not finite */
+/* out[0] = ||x||_2 (the caller checks it for NaN/Inf) */
 int reno_vec_norm(reno_ctx* ctx, int64_t n, int32_t dtype, const void* x,
                   double* out, void* workspace, size_t ws_bytes);
 /* Lanczos three-term step, krylov.py:244-245:
@@ -178,17 +190,21 @@ int reno_vec_precond(reno_ctx* ctx, int64_t n, int32_t dtype, const void* r,
 
 /* ------------------------------------------------------------------------
  * Quantum-number block movers (svd_qn.py:177-213, 89-96; lib.py:302-316).
- * reno_qn_gather: out[i, j] = src[rows[i] * ld + cols[j]]   (nr x nc)
- * reno_qn_scatter_cols: dst[rows[i] * ldd + dcols[j]] = scale_j * src[i * lds + j]
- *   with scale_j = (sigma ? sigma[j] : 1); rows/cols are int64 device arrays.
+ * reno_qn_gather: out[i, j] = src[rows[i] * ld + cols[j]]   (nr x nc, dense out)
+ * reno_qn_scatter: dst[rows[i] * dst_rs + dcols[j] * dst_cs] =
+ *                     scale_j * src[i * src_rs + scols[j] * src_cs]
+ *   with scale_j = (sigma ? sigma[j] : 1); rows/scols/dcols are int64 device
+ *   arrays.  Places selected singular vectors (optionally sigma-weighted) of a
+ *   QN block directly into a new site tensor.
  * ---------------------------------------------------------------------- */
 int reno_qn_gather(reno_ctx* ctx, int32_t dtype, const void* src, int64_t ld,
                    const int64_t* rows, int64_t nr, const int64_t* cols,
                    int64_t nc, void* out);
-int reno_qn_scatter_cols(reno_ctx* ctx, int32_t dtype, const void* src,
-                         int64_t lds, const int64_t* rows, int64_t nr,
-                         const int64_t* dcols, int64_t nc, const double* sigma,
-                         void* dst, int64_t ldd);
+int reno_qn_scatter(reno_ctx* ctx, int32_t dtype, const void* src,
+                    int64_t src_rs, int64_t src_cs, const int64_t* rows,
+                    int64_t nr, const int64_t* scols, const int64_t* dcols,
+                    int64_t nc, const double* sigma, void* dst, int64_t dst_rs,
+                    int64_t dst_cs);
 
 #ifdef __cplusplus
 }

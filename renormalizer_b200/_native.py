@@ -1,0 +1,225 @@
+"""ctypes binding of libreno_b200.so (include/reno_b200.h).
+
+The library is the only compute path: if it is missing, or no CUDA device is
+present, every entry point raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+from typing import Optional
+
+import torch
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libreno_b200.so"
+
+RENO_OK, RENO_ERR_INVALID, RENO_ERR_OOM, RENO_ERR_CUDA, RENO_ERR_WORKSPACE, RENO_ERR_NONFINITE, \
+    RENO_ERR_UNSUPPORTED = range(7)
+RENO_F64, RENO_C128 = 0, 1
+PREC = {"fp64": 0, "bf16x3": 1, "tf32x3": 2}
+
+_c_int, _c_i64, _c_sz, _vp, _dp = ctypes.c_int, ctypes.c_int64, ctypes.c_size_t, ctypes.c_void_p, \
+    ctypes.POINTER(ctypes.c_double)
+
+
+class HeffDesc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in
+                ("nsite", "ml", "mr", "wl", "wm", "wr", "d1", "d2", "psi_dtype", "env_dtype", "mpo_dtype", "prec")]
+
+
+class EnvDesc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in
+                ("side", "d", "w_in", "w_out", "mk_in", "mk_out", "mb_in", "mb_out", "env_dtype", "ket_dtype",
+                 "bra_dtype", "mpo_dtype", "prec")]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "reno_version": (_c_int, []),
+    "reno_ctx_create": (_c_int, [_c_int, ctypes.POINTER(_vp)]),
+    "reno_ctx_destroy": (_c_int, [_vp]),
+    "reno_ctx_set_stream": (_c_int, [_vp, _vp]),
+    "reno_last_error": (ctypes.c_char_p, [_vp]),
+    "reno_ctx_synchronize": (_c_int, [_vp]),
+    "reno_launch_count": (_c_int, [ctypes.POINTER(ctypes.c_longlong)]),
+    "reno_heff_workspace_bytes": (_c_int, [ctypes.POINTER(HeffDesc), ctypes.POINTER(_c_sz)]),
+    "reno_heff_apply": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
+    "reno_gemm": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _c_i64, _c_i64, _c_int, _vp, _c_int, _c_i64,
+                           _c_i64, _c_int, _vp, _c_i64, _c_int]),
+    "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),
+    "reno_env_workspace_bytes": (_c_int, [ctypes.POINTER(EnvDesc), ctypes.POINTER(_c_sz)]),
+    "reno_env_update": (_c_int, [_vp, ctypes.POINTER(EnvDesc), _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
+    "reno_vec_workspace_bytes": (_c_int, [_c_i64, ctypes.POINTER(_c_sz)]),
+    "reno_vec_dotc": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, _vp, _c_sz]),
+    "reno_vec_norm": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, _c_sz]),
+    "reno_krylov_orth": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, _vp, _c_int, _vp, _c_sz]),
+    "reno_krylov_alpha": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, _c_int, _vp, _c_sz]),
+    "reno_vec_scale_inv": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp]),
+    "reno_vec_lincomb": (_c_int, [_vp, _c_i64, _c_int, _c_int, _vp, _c_i64, _vp, _vp]),
+    "reno_vec_allclose": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp, _vp,
+                                   _c_sz]),
+    "reno_vec_axpy": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, ctypes.c_double]),
+    "reno_vec_precond": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, ctypes.c_double, _vp]),
+    "reno_qn_gather": (_c_int, [_vp, _c_int, _vp, _c_i64, _vp, _c_i64, _vp, _c_i64, _vp]),
+    "reno_qn_scatter": (_c_int, [_vp, _c_int, _vp, _c_i64, _c_i64, _vp, _c_i64, _vp, _vp, _c_i64, _vp, _vp, _c_i64,
+                                 _c_i64]),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def launch_count() -> int:
+    """Kernels launched by libreno_b200 in this process so far."""
+    n = ctypes.c_longlong(0)
+    load_library().reno_launch_count(ctypes.byref(n))
+    return int(n.value)
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def load_library(path: Optional[Path] = None):
+    """Load libreno_b200.so and declare every entry point (no GPU needed)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            p = Path(path) if path else LIB_PATH
+            if not p.exists():
+                raise RuntimeError(f"{p} is missing: build it with `python -m renormalizer_b200.build` "
+                                   "(the sweep engine has no CPU fallback)")
+            lib = ctypes.CDLL(str(p))
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def _raise(status: int, msg: str):
+    if status in (RENO_ERR_OOM, RENO_ERR_WORKSPACE):
+        raise MemoryError(msg)
+    if status == RENO_ERR_INVALID:
+        raise AssertionError(msg)
+    if status == RENO_ERR_NONFINITE:
+        raise FloatingPointError(msg)
+    if status == RENO_ERR_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    raise RuntimeError(msg)
+
+
+def dtype_code(t: torch.Tensor) -> int:
+    if t.dtype == torch.complex128:
+        return RENO_C128
+    if t.dtype == torch.float64:
+        return RENO_F64
+    raise TypeError(f"the sweep engine works on float64/complex128 tensors, got {t.dtype}")
+
+
+def ptr(t: Optional[torch.Tensor]):
+    if t is None:
+        return None
+    assert t.is_cuda, "sweep-engine tensors live on the GPU"
+    assert t.is_contiguous(), "sweep-engine tensors are C-contiguous"
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Engine:
+    """One C-ABI context per CUDA device plus a growable device workspace.
+
+    The workspace is allocated outside the hot calls (torch's caching
+    allocator) and handed to the kernels, which never allocate."""
+
+    _engines = {}
+
+    def __init__(self, device: int):
+        if not torch.cuda.is_available():
+            raise RuntimeError("renormalizer_b200 needs a CUDA device (B200, sm_100a); none is visible")
+        self.lib = load_library()
+        self.device = device
+        ctx = _vp()
+        with torch.cuda.device(device):
+            st = self.lib.reno_ctx_create(device, ctypes.byref(ctx))
+        if st != RENO_OK:
+            raise RuntimeError(f"reno_ctx_create failed on device {device} (status {st})")
+        self.ctx = ctx
+        self._stream_handle = None
+        self._ws = None
+        self._vec_ws = None
+        self.scalars = torch.zeros(4096, dtype=torch.float64, device=f"cuda:{device}")
+        self.launches = 0
+
+    @classmethod
+    def get(cls, device=None) -> "Engine":
+        if device is None:
+            device = torch.cuda.current_device()
+        if isinstance(device, torch.device):
+            device = device.index if device.index is not None else torch.cuda.current_device()
+        eng = cls._engines.get(device)
+        if eng is None:
+            eng = cls(device)
+            cls._engines[device] = eng
+        eng.sync_stream()
+        return eng
+
+    def sync_stream(self):
+        h = torch.cuda.current_stream(self.device).cuda_stream
+        if h != self._stream_handle:
+            self.lib.reno_ctx_set_stream(self.ctx, _vp(h))
+            self._stream_handle = h
+
+    def check(self, status: int, what: str):
+        if status != RENO_OK:
+            msg = self.lib.reno_last_error(self.ctx)
+            _raise(status, f"{what}: {msg.decode() if msg else 'error'}")
+
+    def workspace(self, nbytes: int) -> torch.Tensor:
+        if self._ws is None or self._ws.numel() < nbytes:
+            grow = max(int(nbytes), int(1.25 * (self._ws.numel() if self._ws is not None else 0)), 1 << 20)
+            self._ws = None
+            self._ws = torch.empty(grow, dtype=torch.uint8, device=f"cuda:{self.device}")
+        return self._ws
+
+    def vec_workspace(self) -> torch.Tensor:
+        if self._vec_ws is None:
+            n = _c_sz()
+            self.check(self.lib.reno_vec_workspace_bytes(0, ctypes.byref(n)), "reno_vec_workspace_bytes")
+            self._vec_ws = torch.empty(int(n.value), dtype=torch.uint8, device=f"cuda:{self.device}")
+        return self._vec_ws
+
+    # ------------------------------------------------------------ wrappers
+    def heff_apply(self, desc: HeffDesc, L, W1, W2, R, psi, y):
+        n = _c_sz()
+        self.check(self.lib.reno_heff_workspace_bytes(ctypes.byref(desc), ctypes.byref(n)), "reno_heff_workspace_bytes")
+        ws = self.workspace(int(n.value))
+        self.check(self.lib.reno_heff_apply(self.ctx, ctypes.byref(desc), ptr(L), ptr(W1), ptr(W2), ptr(R), ptr(psi),
+                                            ptr(y), ptr(ws), ws.numel()), "reno_heff_apply")
+        self.launches += 1
+
+    def heff_diag(self, desc: HeffDesc, L, W1, W2, R, out):
+        self.check(self.lib.reno_heff_diag(self.ctx, ctypes.byref(desc), ptr(L), ptr(W1), ptr(W2), ptr(R), ptr(out)),
+                   "reno_heff_diag")
+
+    def matmul(self, A: torch.Tensor, B: torch.Tensor, conj_a=False, conj_b=False) -> torch.Tensor:
+        """C = op(A) @ op(B) for 2-D device tensors (any strides) on the FP64 kernel."""
+        assert A.dim() == 2 and B.dim() == 2 and A.shape[1] == B.shape[0]
+        cplx = A.is_complex() or B.is_complex()
+        C = torch.empty((A.shape[0], B.shape[1]), dtype=torch.complex128 if cplx else torch.float64, device=A.device)
+        self.check(self.lib.reno_gemm(self.ctx, A.shape[0], B.shape[1], A.shape[1], _vp(A.data_ptr()), dtype_code(A),
+                                      A.stride(0), A.stride(1), int(conj_a), _vp(B.data_ptr()), dtype_code(B),
+                                      B.stride(0), B.stride(1), int(conj_b), _vp(C.data_ptr()), C.stride(0), 0),
+                   "reno_gemm")
+        self.launches += 1
+        return C
+
+    def env_update(self, desc: EnvDesc, E, W, ket, bra, out):
+        n = _c_sz()
+        self.check(self.lib.reno_env_workspace_bytes(ctypes.byref(desc), ctypes.byref(n)), "reno_env_workspace_bytes")
+        ws = self.workspace(int(n.value))
+        self.check(self.lib.reno_env_update(self.ctx, ctypes.byref(desc), ptr(E), ptr(W), ptr(ket), ptr(bra),
+                                            ptr(out), ptr(ws), ws.numel()), "reno_env_update")
+        self.launches += 1

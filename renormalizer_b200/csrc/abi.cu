@@ -40,3 +40,9 @@ extern "C" int reno_ctx_synchronize(reno_ctx* ctx) {
   if (!ctx) return RENO_ERR_INVALID;
   return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "reno_ctx_synchronize");
 }
+
+extern "C" int reno_launch_count(long long* count) {
+  if (!count) return RENO_ERR_INVALID;
+  *count = g_launches.load();
+  return RENO_OK;
+}

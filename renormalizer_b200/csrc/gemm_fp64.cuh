@@ -222,6 +222,7 @@ inline cudaError_t launch_t(const GemmParams& p, cudaStream_t st) {
     attr_set = true;
   }
   dim3 grid((unsigned)ceil_div(p.N, BN), (unsigned)ceil_div(p.M, BM), (unsigned)p.batch);
+  count_launch();
   gemm_kernel<AC, BC><<<grid, THREADS, sm, st>>>(p);
   return cudaGetLastError();
 }

@@ -63,6 +63,7 @@ static int grid_for(int64_t total) {
 
 static cudaError_t launch_wt(const void* W, void* Wt, int dt, int nc, int d, int nr, int mode, cudaStream_t st) {
   const int64_t total = (int64_t)d * nr * nc * d;
+  count_launch();
   if (dt == RENO_C128)
     wt_kernel<double2><<<grid_for(total), 256, 0, st>>>((const double2*)W, (double2*)Wt, nc, d, nr, mode);
   else
@@ -72,6 +73,7 @@ static cudaError_t launch_wt(const void* W, void* Wt, int dt, int nc, int d, int
 
 static cudaError_t launch_swap13(const void* in, void* out, int dt, int n0, int d, int n2, cudaStream_t st) {
   const int64_t total = (int64_t)n0 * d * n2;
+  count_launch();
   if (dt == RENO_C128)
     swap13_kernel<double2><<<grid_for(total), 256, 0, st>>>((const double2*)in, (double2*)out, n0, d, n2);
   else
@@ -412,6 +414,7 @@ extern "C" int reno_heff_diag(reno_ctx* ctx, const reno_heff_desc* d, const void
   const int64_t total = (int64_t)d->ml * d->d1 * (d->nsite == 2 ? d->d2 : 1) * d->mr;
   const int g = grid_for(total);
   const bool ec = d->env_dtype == RENO_C128, wc = d->mpo_dtype == RENO_C128;
+  count_launch();
 #define HD(TE, TW)                                                                                         \
   hdiag_kernel<TE, TW><<<g, 256, 0, ctx->stream>>>((const TE*)L, (const TW*)W1, (const TW*)W2, (const TE*)R, \
                                                     hdiag, d->nsite, d->ml, d->mr, d->wl, d->wm, d->wr, d->d1,   \
@@ -426,4 +429,18 @@ extern "C" int reno_heff_diag(reno_ctx* ctx, const reno_heff_desc* d, const void
     HD(double, double);
 #undef HD
   return check_cuda(ctx, cudaGetLastError(), "reno_heff_diag");
+}
+
+// ---------------------------------------------------------------- plain GEMM
+extern "C" int reno_gemm(reno_ctx* ctx, int32_t M, int32_t N, int32_t K, const void* A, int32_t a_dtype,
+                         int64_t a_rs, int64_t a_cs, int32_t a_conj, const void* B, int32_t b_dtype, int64_t b_rs,
+                         int64_t b_cs, int32_t b_conj, void* C, int64_t c_rs, int32_t prec) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (M < 0 || N < 0 || K < 0 || !A || !B || !C || (a_dtype != RENO_F64 && a_dtype != RENO_C128) ||
+      (b_dtype != RENO_F64 && b_dtype != RENO_C128) || c_rs < N)
+    return set_error(ctx, RENO_ERR_INVALID, "reno_gemm: bad arguments");
+  if (prec != RENO_PREC_FP64) return set_error(ctx, RENO_ERR_UNSUPPORTED, "reno_gemm: FP64 only");
+  GemmParams p = gp(M, N, K, 1, opnd(A, a_dtype, a_rs, a_cs, 0, a_conj), opnd(B, b_dtype, b_cs, b_rs, 0, b_conj), C,
+                    c_rs, 1);
+  return check_cuda(ctx, gemm_fp64(p, ctx->stream), "reno_gemm");
 }

@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <atomic>
 #include "../../include/reno_b200.h"
 
 struct reno_ctx {
@@ -20,6 +21,10 @@ struct reno_ctx {
 };
 
 namespace reno {
+
+// every kernel launch of the library bumps this (host-side, per process)
+inline std::atomic<long long> g_launches{0};
+inline void count_launch(long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 inline int set_error(reno_ctx* ctx, int code, const std::string& msg) {
   if (ctx) ctx->last_error = msg;

@@ -204,6 +204,7 @@ extern "C" int reno_vec_dotc(reno_ctx* ctx, int64_t n, int32_t dtype, const void
                              void* ws, size_t ws_bytes) {
   VEC_PRE(ctx, n, dtype, ws, ws_bytes);
   const int nb = vec_blocks(n);
+  count_launch(2);
   dot_partial<<<nb, VT, 0, ctx->stream>>>(n, dtype == RENO_C128, x, y, 0, (double2*)ws);
   dot_final<<<1, VT, 0, ctx->stream>>>(nb, (double2*)ws, 0, out);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_dotc");
@@ -213,6 +214,7 @@ extern "C" int reno_vec_norm(reno_ctx* ctx, int64_t n, int32_t dtype, const void
                              size_t ws_bytes) {
   VEC_PRE(ctx, n, dtype, ws, ws_bytes);
   const int nb = vec_blocks(n);
+  count_launch(2);
   dot_partial<<<nb, VT, 0, ctx->stream>>>(n, dtype == RENO_C128, x, x, 1, (double2*)ws);
   dot_final<<<1, VT, 0, ctx->stream>>>(nb, (double2*)ws, 1, out);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_norm");
@@ -223,6 +225,7 @@ extern "C" int reno_krylov_alpha(reno_ctx* ctx, int64_t n, int32_t dtype, const 
   VEC_PRE(ctx, n, dtype, ws, ws_bytes);
   if (j < 0 || !ab) return set_error(ctx, RENO_ERR_INVALID, "reno_krylov_alpha: bad index");
   const int nb = vec_blocks(n);
+  count_launch(2);
   dot_partial<<<nb, VT, 0, ctx->stream>>>(n, dtype == RENO_C128, w, v, 0, (double2*)ws);
   dot_final<<<1, VT, 0, ctx->stream>>>(nb, (double2*)ws, 2, ab + 2 * j);
   return check_cuda(ctx, cudaGetLastError(), "reno_krylov_alpha");
@@ -233,6 +236,7 @@ extern "C" int reno_krylov_orth(reno_ctx* ctx, int64_t n, int32_t dtype, void* w
   VEC_PRE(ctx, n, dtype, ws, ws_bytes);
   if (j < 0 || !ab || (j > 0 && !vprev)) return set_error(ctx, RENO_ERR_INVALID, "reno_krylov_orth: bad args");
   const int nb = vec_blocks(n);
+  count_launch(2);
   orth_partial<<<nb, VT, 0, ctx->stream>>>(n, dtype == RENO_C128, w, v, vprev, ab, j, (double2*)ws);
   dot_final<<<1, VT, 0, ctx->stream>>>(nb, (double2*)ws, 1, ab + 2 * j + 1);
   return check_cuda(ctx, cudaGetLastError(), "reno_krylov_orth");
@@ -242,6 +246,7 @@ extern "C" int reno_vec_scale_inv(reno_ctx* ctx, int64_t n, int32_t dtype, const
                                   void* out) {
   if (!ctx) return RENO_ERR_INVALID;
   if (!dt_ok(dtype) || n < 0 || !s) return set_error(ctx, RENO_ERR_INVALID, "reno_vec_scale_inv: bad args");
+  count_launch(1);
   scale_inv_kernel<<<vec_blocks(n), VT, 0, ctx->stream>>>(n, dtype == RENO_C128, x, s, out);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_scale_inv");
 }
@@ -251,6 +256,7 @@ extern "C" int reno_vec_lincomb(reno_ctx* ctx, int64_t n, int32_t k, int32_t dty
   if (!ctx) return RENO_ERR_INVALID;
   if (!dt_ok(dtype) || n < 0 || k < 0 || ldv < n || !coef)
     return set_error(ctx, RENO_ERR_INVALID, "reno_vec_lincomb: bad args");
+  count_launch(1);
   lincomb_kernel<<<vec_blocks(n), VT, 0, ctx->stream>>>(n, k, dtype == RENO_C128, V, ldv, coef, out);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_lincomb");
 }
@@ -259,6 +265,7 @@ extern "C" int reno_vec_allclose(reno_ctx* ctx, int64_t n, int32_t dtype, const 
                                  double atol, double* flag, void* ws, size_t ws_bytes) {
   VEC_PRE(ctx, n, dtype, ws, ws_bytes);
   const int nb = vec_blocks(n);
+  count_launch(2);
   allclose_partial<<<nb, VT, 0, ctx->stream>>>(n, dtype == RENO_C128, a, b, rtol, atol, (double2*)ws);
   allclose_final<<<1, VT, 0, ctx->stream>>>(nb, (double2*)ws, flag);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_allclose");
@@ -268,6 +275,7 @@ extern "C" int reno_vec_axpy(reno_ctx* ctx, int64_t n, int32_t dtype, void* y, c
                              double c_sign) {
   if (!ctx) return RENO_ERR_INVALID;
   if (!dt_ok(dtype) || n < 0 || !c) return set_error(ctx, RENO_ERR_INVALID, "reno_vec_axpy: bad args");
+  count_launch(1);
   axpy_kernel<<<vec_blocks(n), VT, 0, ctx->stream>>>(n, dtype == RENO_C128, y, x, c, c_sign);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_axpy");
 }
@@ -276,6 +284,7 @@ extern "C" int reno_vec_precond(reno_ctx* ctx, int64_t n, int32_t dtype, const v
                                 const double* e, double shift, void* out) {
   if (!ctx) return RENO_ERR_INVALID;
   if (!dt_ok(dtype) || n < 0 || !hdiag || !e) return set_error(ctx, RENO_ERR_INVALID, "reno_vec_precond: bad args");
+  count_launch(1);
   precond_kernel<<<vec_blocks(n), VT, 0, ctx->stream>>>(n, dtype == RENO_C128, r, hdiag, e, shift, out);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_precond");
 }
