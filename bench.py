@@ -247,8 +247,9 @@ class HeffTimer:
         self.events = []
 
     def install(self):
+        import importlib
         import torch
-        from renormalizer_b200 import hop_expr as H
+        H = importlib.import_module("renormalizer_b200.hop_expr")
         orig = H.HeffOperator.apply
         timer = self
 
@@ -269,13 +270,54 @@ class HeffTimer:
         return self
 
     def uninstall(self):
-        from renormalizer_b200 import hop_expr as H
-        H.HeffOperator.apply = self._orig
+        import importlib
+        importlib.import_module("renormalizer_b200.hop_expr").HeffOperator.apply = self._orig
 
     def result(self):
         tot_ms = sum(s.elapsed_time(e) for s, e, _ in self.events)
         fl = sum(f for _, _, f in self.events)
         return fl, tot_ms, len(self.events)
+
+
+class PhaseTimer:
+    """CUDA-event device time per phase of the sweep (host-visible breakdown)."""
+
+    def __init__(self):
+        self.events = {}
+        self._saved = []
+
+    def wrap(self, module, name, label):
+        import torch
+        orig = getattr(module, name)
+        events = self.events.setdefault(label, [])
+
+        def wrapped(*a, **k):
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record()
+            r = orig(*a, **k)
+            e.record()
+            events.append((s, e))
+            return r
+
+        setattr(module, name, wrapped)
+        self._saved.append((module, name, orig))
+
+    def install(self):
+        import importlib
+        mps_mod = importlib.import_module("renormalizer_b200.mps")
+        self.wrap(mps_mod, "svd_truncate", "svd_truncate")
+        self.wrap(mps_mod, "qr_split", "qr_split")
+        self.wrap(mps_mod, "expm_krylov", "krylov_total")
+        self.wrap(mps_mod, "contract_one_site", "env_update")
+        return self
+
+    def uninstall(self):
+        for m, n, o in self._saved:
+            setattr(m, n, o)
+
+    def result(self):
+        return {k: round(sum(s.elapsed_time(e) for s, e in v), 1) for k, v in self.events.items()}
 
 
 def fp64_peak_tflops(dev):
@@ -319,6 +361,7 @@ def run_engine(args, rank, world, dist):
         torch.cuda.synchronize()
 
     timer = HeffTimer().install()
+    phases = PhaseTimer().install()
     barrier()
     l0 = launch_count()
     with ClockSampler(local) as clocks:
@@ -330,6 +373,7 @@ def run_engine(args, rank, world, dist):
         barrier()
     launches = launch_count() - l0
     timer.uninstall()
+    phases.uninstall()
     t_ms = s_ev.elapsed_time(e_ev)
     if dist is not None:
         tt = torch.tensor([t_ms], device=dev)
@@ -409,7 +453,8 @@ def run_engine(args, rank, world, dist):
                 "config": {"workload": WORKLOAD, "nsites": 3 * args.nmol, "M": args.M, "nlev": args.nlev,
                            "dt": args.dt, "prec": args.prec, "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (MPS ~1.5 GB, environments ~1 GB resident in HBM)"},
-                "tflops_heff2": achieved, "krylov": kry_timed, "bond_dims_max": max(mps.bond_dims),
+                "tflops_heff2": achieved, "heff2_ms": round(heff_ms, 1), "phase_ms": phases.result(),
+                "krylov": kry_timed, "bond_dims_max": max(mps.bond_dims),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks.summary(), "fp64_engine": fp64}
         print(json.dumps(line), flush=True)

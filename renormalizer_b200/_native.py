@@ -125,7 +125,18 @@ def ptr(t: Optional[torch.Tensor]):
         return None
     assert t.is_cuda, "sweep-engine tensors live on the GPU"
     assert t.is_contiguous(), "sweep-engine tensors are C-contiguous"
+    # torch's lazy conjugate / negative views keep unconjugated memory behind a flag
+    assert not (t.is_conj() or t.is_neg()), "resolve_conj()/resolve_neg() before passing a view to the engine"
     return ctypes.c_void_p(t.data_ptr())
+
+
+def raw_view(t: torch.Tensor) -> torch.Tensor:
+    """A tensor whose memory holds the values it denotes (no lazy conj/neg bit)."""
+    if t.is_conj():
+        t = t.resolve_conj()
+    if t.is_neg():
+        t = t.resolve_neg()
+    return t
 
 
 class Engine:
@@ -207,6 +218,12 @@ class Engine:
     def matmul(self, A: torch.Tensor, B: torch.Tensor, conj_a=False, conj_b=False) -> torch.Tensor:
         """C = op(A) @ op(B) for 2-D device tensors (any strides) on the FP64 kernel."""
         assert A.dim() == 2 and B.dim() == 2 and A.shape[1] == B.shape[0]
+        # a lazy conj view is the raw memory of the conjugate: fold it into the kernel's conj flag
+        if A.is_conj():
+            A, conj_a = A.conj(), not conj_a
+        if B.is_conj():
+            B, conj_b = B.conj(), not conj_b
+        A, B = raw_view(A), raw_view(B)
         cplx = A.is_complex() or B.is_complex()
         C = torch.empty((A.shape[0], B.shape[1]), dtype=torch.complex128 if cplx else torch.float64, device=A.device)
         self.check(self.lib.reno_gemm(self.ctx, A.shape[0], B.shape[1], A.shape[1], _vp(A.data_ptr()), dtype_code(A),
@@ -223,3 +240,65 @@ class Engine:
         self.check(self.lib.reno_env_update(self.ctx, ctypes.byref(desc), ptr(E), ptr(W), ptr(ket), ptr(bra),
                                             ptr(out), ptr(ws), ws.numel()), "reno_env_update")
         self.launches += 1
+
+    # vector kernels (krylov.py / davidson.py algebra); scalars live in device arrays
+    def _vws(self):
+        ws = self.vec_workspace()
+        return ptr(ws), ws.numel()
+
+    def vec_norm(self, x, out):
+        w, n = self._vws()
+        self.check(self.lib.reno_vec_norm(self.ctx, x.numel(), dtype_code(x), ptr(x), ptr(out), w, n), "reno_vec_norm")
+
+    def vec_dotc(self, x, y, out):
+        w, n = self._vws()
+        self.check(self.lib.reno_vec_dotc(self.ctx, x.numel(), dtype_code(x), ptr(x), ptr(y), ptr(out), w, n),
+                   "reno_vec_dotc")
+
+    def krylov_alpha(self, w_vec, v, ab, j):
+        w, n = self._vws()
+        self.check(self.lib.reno_krylov_alpha(self.ctx, v.numel(), dtype_code(v), ptr(w_vec), ptr(v), ptr(ab), j, w,
+                                              n), "reno_krylov_alpha")
+
+    def krylov_orth(self, w_vec, v, vprev, ab, j):
+        w, n = self._vws()
+        self.check(self.lib.reno_krylov_orth(self.ctx, v.numel(), dtype_code(v), ptr(w_vec), ptr(v), ptr(vprev),
+                                             ptr(ab), j, w, n), "reno_krylov_orth")
+
+    def scale_inv(self, x, s, out):
+        self.check(self.lib.reno_vec_scale_inv(self.ctx, x.numel(), dtype_code(x), ptr(x), ptr(s), ptr(out)),
+                   "reno_vec_scale_inv")
+
+    def lincomb(self, V, k, coef, out):
+        n = V.shape[1]
+        self.check(self.lib.reno_vec_lincomb(self.ctx, n, k, dtype_code(V), ptr(V), n, ptr(coef), ptr(out)),
+                   "reno_vec_lincomb")
+
+    def allclose(self, a, b, rtol, atol, flag):
+        w, n = self._vws()
+        self.check(self.lib.reno_vec_allclose(self.ctx, a.numel(), dtype_code(a), ptr(a), ptr(b), rtol, atol,
+                                              ptr(flag), w, n), "reno_vec_allclose")
+
+    def axpy(self, y, x, c, sign=1.0):
+        self.check(self.lib.reno_vec_axpy(self.ctx, y.numel(), dtype_code(y), ptr(y), ptr(x), ptr(c), sign),
+                   "reno_vec_axpy")
+
+    def precond(self, r, hdiag, e, shift, out):
+        self.check(self.lib.reno_vec_precond(self.ctx, r.numel(), dtype_code(r), ptr(r), ptr(hdiag), ptr(e), shift,
+                                             ptr(out)), "reno_vec_precond")
+
+    # quantum-number block movers
+    def qn_gather(self, mat, rows, cols, out):
+        """out[i, j] = mat[rows[i], cols[j]] for a C-contiguous 2-D mat"""
+        self.check(self.lib.reno_qn_gather(self.ctx, dtype_code(mat), ptr(mat), mat.shape[1], ptr(rows),
+                                           rows.numel(), ptr(cols), cols.numel(), ptr(out)), "reno_qn_gather")
+
+    def qn_scatter(self, src, rows, scols, dcols, sigma, dst, dst_rs, dst_cs):
+        """dst[rows[i]*dst_rs + dcols[j]*dst_cs] = sigma_j * src[i, scols[j]] for a 2-D view src"""
+        src = raw_view(src)
+        if src.dtype != dst.dtype:
+            src = src.to(dst.dtype)
+        self.check(self.lib.reno_qn_scatter(self.ctx, dtype_code(dst), _vp(src.data_ptr()), src.stride(0),
+                                            src.stride(1), ptr(rows), rows.numel(), ptr(scols), ptr(dcols),
+                                            dcols.numel(), ptr(sigma) if sigma is not None else None, ptr(dst),
+                                            dst_rs, dst_cs), "reno_qn_scatter")

@@ -62,8 +62,11 @@ class HeffOperator:
             d.wm = self.W[0].shape[3]
             assert self.W[0].shape == (wl, d.d1, d.d1, d.wm)
             assert self.W[1].shape == (d.wm, d.d2, d.d2, wr)
+        if self.L.dtype != self.R.dtype:
+            # e.g. the real ones((1,1,1)) boundary sentinel next to a complex environment
+            self.L = self.L.to(torch.complex128)
+            self.R = self.R.to(torch.complex128)
         d.env_dtype = dtype_code(self.L)
-        assert dtype_code(self.R) == d.env_dtype, "L and R must share a dtype"
         d.mpo_dtype = dtype_code(self.W[0]) if self.W else 0
         for w in self.W:
             if dtype_code(w) != d.mpo_dtype:

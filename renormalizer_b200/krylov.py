@@ -11,13 +11,11 @@ reference exactly.
 """
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 import torch
 from scipy.linalg import eigh_tridiagonal
 
-from ._native import Engine, dtype_code, ptr
+from ._native import Engine
 from .hop_expr import as_device
 
 EPS = np.finfo(float).eps
@@ -43,7 +41,6 @@ class _Krylov:
         self.ab = torch.zeros(2 * block_size + 2, dtype=torch.float64, device=device)
         self.tmp = torch.zeros(4, dtype=torch.float64, device=device)
         self.coef = torch.zeros(2 * block_size, dtype=torch.float64, device=device)
-        self.vws = eng.vec_workspace()
 
     def grow(self, block_size):
         V = torch.empty((self.V.shape[0] + block_size, self.n), dtype=self.dtype, device=self.V.device)
@@ -59,9 +56,7 @@ class _Krylov:
         c[0::2] = np.real(coeffs)
         c[1::2] = np.imag(coeffs) if np.iscomplexobj(coeffs) else 0.0
         self.coef[: 2 * k].copy_(torch.from_numpy(c), non_blocking=False)
-        e = self.eng
-        e.check(e.lib.reno_vec_lincomb(e.ctx, self.n, k, self.code, ptr(self.V), self.n, ptr(self.coef), ptr(out)),
-                "reno_vec_lincomb")
+        self.eng.lincomb(self.V, k, self.coef, out)
         return out
 
 
@@ -83,12 +78,12 @@ def expm_krylov(Afunc, dt, vstart, block_size=50):
     K = _Krylov(eng, n, work_dtype, v.device, block_size)
     code = K.code
     # nrmv = ||vstart||; V[0] = vstart / nrmv
-    eng.check(eng.lib.reno_vec_norm(eng.ctx, n, code, ptr(v), ptr(K.tmp), ptr(K.vws), K.vws.numel()), "reno_vec_norm")
+    eng.vec_norm(v, K.tmp)
     nrmv = float(K.tmp[0].item())
     assert nrmv > 0
     if not np.isfinite(nrmv):
         raise FloatingPointError("expm_krylov: start vector is not finite")
-    eng.check(eng.lib.reno_vec_scale_inv(eng.ctx, n, code, ptr(v), ptr(K.tmp), ptr(K.V[0])), "reno_vec_scale_inv")
+    eng.scale_inv(v, K.tmp, K.V[0])
     res_prev = None
     out_a = torch.empty(n, dtype=work_dtype, device=v.device)
     out_b = torch.empty(n, dtype=work_dtype, device=v.device)
@@ -99,8 +94,7 @@ def expm_krylov(Afunc, dt, vstart, block_size=50):
             w = w.to(work_dtype)
         if not w.is_contiguous():
             w = w.contiguous()
-        eng.check(eng.lib.reno_krylov_alpha(eng.ctx, n, code, ptr(w), ptr(K.V[j]), ptr(K.ab), j, ptr(K.vws),
-                                            K.vws.numel()), "reno_krylov_alpha")
+        eng.krylov_alpha(w, K.V[j], K.ab, j)
         if j == n - 1:
             ab = K.ab[: 2 * j + 2].cpu().numpy()
             coeffs = _tridiag_coeffs(ab[0::2][: j + 1], ab[1::2][:j], nrmv, dt)
@@ -108,8 +102,7 @@ def expm_krylov(Afunc, dt, vstart, block_size=50):
         if K.V.shape[0] == j + 1:
             K.grow(block_size)
         vprev = K.V[j - 1] if j > 0 else None
-        eng.check(eng.lib.reno_krylov_orth(eng.ctx, n, code, ptr(w), ptr(K.V[j]), ptr(vprev), ptr(K.ab), j,
-                                           ptr(K.vws), K.vws.numel()), "reno_krylov_orth")
+        eng.krylov_orth(w, K.V[j], vprev, K.ab, j)
         ab = K.ab[: 2 * j + 2].cpu().numpy()
         alpha, beta = ab[0::2][: j + 1], ab[1::2][: j + 1]
         if not np.isfinite(beta[j]):
@@ -122,11 +115,9 @@ def expm_krylov(Afunc, dt, vstart, block_size=50):
             new_res = K.combine(j + 1, coeffs, out_b if res_prev is out_a else out_a)
             if res_prev is not None:
                 flag = K.tmp[2:3]
-                eng.check(eng.lib.reno_vec_allclose(eng.ctx, n, code, ptr(res_prev), ptr(new_res), 1e-5, 1e-8,
-                                                    ptr(flag), ptr(K.vws), K.vws.numel()), "reno_vec_allclose")
+                eng.allclose(res_prev, new_res, 1e-5, 1e-8, flag)
                 if float(flag.item()) == 1.0:
                     return new_res, j + 1
             res_prev = new_res
         # V[j+1] = w / beta[j]
-        eng.check(eng.lib.reno_vec_scale_inv(eng.ctx, n, code, ptr(w), ptr(K.ab[2 * j + 1:]), ptr(K.V[j + 1])),
-                  "reno_vec_scale_inv")
+        eng.scale_inv(w, K.ab[2 * j + 1:], K.V[j + 1])

@@ -80,7 +80,9 @@ class Mps:
 
     @classmethod
     def random(cls, model: Model, qntot, m_max, percent=1.0) -> "Mps":
-        """mps.py:119-185 (host construction of the random left-canonical MPS)."""
+        """mps.py:119-185: a random left-canonical MPS.  The random symmetric
+        blocks are drawn from numpy's global RNG like the reference; their
+        eigendecompositions and the column selection run on the device."""
         mps = cls()
         mps.model = model
         if isinstance(qntot, (int, np.integer)):
@@ -90,26 +92,34 @@ class Mps:
         qn = [np.zeros((1, qn_size), dtype=int)]
         dim_list = [1]
         sites = []
+        dev = backend.device
         for imps in range(model.nsite - 1):
             qnbig = add_outer(qn[imps], model.basis[imps].sigmaqn).reshape(-1, qn_size)
-            u_set, s_set, qnset = [], [], []
+            u_blocks, s_set, qnset = [], [], []
             for iblock in set(tuple(t) for t in qnbig):
                 if np.all(np.array(qntot) < np.array(iblock)):
                     continue
                 indices = [i for i, x in enumerate(qnbig) if tuple(x) == iblock]
                 a = np.random.random([len(indices), len(indices)]) - 0.5
-                a = a + a.T
-                s, u = np.linalg.eigh(a)
-                full = np.zeros((len(qnbig), u.shape[1]))
-                full[indices, :] = u
-                u_set.append(full)
-                s_set.append(s)
+                a = torch.from_numpy(a + a.T).to(dev)
+                s, u = torch.linalg.eigh(a)
+                u_blocks.append((indices, u))
+                s_set.append(s.cpu().numpy())
                 qnset += [iblock] * len(indices)
-            u_set = np.concatenate(u_set, axis=1)
             s_set = np.concatenate(s_set)
             m2 = m_max[imps + 1] if isinstance(m_max, (list, tuple, np.ndarray)) else m_max
             sidx = select_basis_indices(s_set, qnset, m2, percent)
-            mt = u_set[:, sidx]
+            mt = torch.zeros((len(qnbig), len(sidx)), dtype=torch.float64, device=dev)
+            offs = np.cumsum([0] + [u.shape[1] for _, u in u_blocks])
+            sel = np.asarray(sidx)
+            blk = np.searchsorted(offs, sel, side="right") - 1
+            for bi, (idx, u) in enumerate(u_blocks):
+                outs = np.nonzero(blk == bi)[0]
+                if len(outs) == 0:
+                    continue
+                r = torch.as_tensor(idx, device=dev)[:, None]
+                c = torch.as_tensor(outs, device=dev)[None, :]
+                mt[r, c] = u[:, torch.as_tensor(sel[outs] - offs[bi], device=dev)]
             dim_list.append(len(sidx))
             sites.append(mt.reshape((dim_list[imps], -1, dim_list[imps + 1])))
             qn.append(np.array([qnset[i] for i in sidx]).reshape(len(sidx), -1))

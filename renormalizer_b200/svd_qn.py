@@ -18,14 +18,13 @@ them.
 """
 from __future__ import annotations
 
-import ctypes
 from dataclasses import dataclass
 from typing import List, Optional
 
 import numpy as np
 import torch
 
-from ._native import Engine, dtype_code, ptr
+from ._native import Engine
 
 
 def add_outer(a: np.ndarray, b: np.ndarray) -> np.ndarray:
@@ -60,9 +59,7 @@ class QNBlock:
 
 def _gather(eng: Engine, mat: torch.Tensor, lset, rset) -> torch.Tensor:
     out = torch.empty((len(lset), len(rset)), dtype=mat.dtype, device=mat.device)
-    rows, cols = _i64(lset, mat.device), _i64(rset, mat.device)
-    eng.check(eng.lib.reno_qn_gather(eng.ctx, dtype_code(mat), ptr(mat), mat.shape[1], ptr(rows), len(lset),
-                                     ptr(cols), len(rset), ptr(out)), "reno_qn_gather")
+    eng.qn_gather(mat, _i64(lset, mat.device), _i64(rset, mat.device), out)
     return out
 
 
@@ -135,7 +132,8 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
             blocks.append(QNBlock(nl, nr, lset, rset, Q, None, None, R))
         elif system == "R":
             Q1, R1 = torch.linalg.qr(blk.mH, mode="reduced")
-            blocks.append(QNBlock(nl, nr, lset, rset, R1.mH.contiguous(), None, None, Q1.mH.contiguous()))
+            blocks.append(QNBlock(nl, nr, lset, rset, R1.mH.resolve_conj().contiguous(), None, None,
+                                  Q1.mH.resolve_conj().contiguous()))
         else:
             raise AssertionError("system must be L or R for QR")
     if not blocks:
@@ -143,20 +141,13 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
     return blocks, rows, cols
 
 
-def _scatter(eng: Engine, src: torch.Tensor, src_rs, src_cs, rows, scols, dcols, sigma, dst: torch.Tensor, dst_rs,
-             dst_cs):
+def _scatter(eng: Engine, src: torch.Tensor, rows, scols, dcols, sigma, dst: torch.Tensor, dst_rs, dst_cs):
+    """dst[rows[i]*dst_rs + dcols[j]*dst_cs] = sigma_j * src[i, scols[j]] (src: any 2-D view)"""
     if len(rows) == 0 or len(scols) == 0:
         return
     dev = dst.device
-    r, s, d = _i64(rows, dev), _i64(scols, dev), _i64(dcols, dev)
-    sig = None
-    if sigma is not None:
-        sig = torch.as_tensor(np.asarray(sigma, dtype=np.float64), device=dev)
-    if src.dtype != dst.dtype:
-        src = src.to(dst.dtype)
-    eng.check(eng.lib.reno_qn_scatter(eng.ctx, dtype_code(dst), ptr(src), src_rs, src_cs, ptr(r), len(rows), ptr(s),
-                                      ptr(d), len(scols), ptr(sig) if sig is not None else None, ptr(dst), dst_rs,
-                                      dst_cs), "reno_qn_scatter")
+    sig = None if sigma is None else torch.as_tensor(np.asarray(sigma, dtype=np.float64), device=dev)
+    eng.qn_scatter(src, _i64(rows, dev), _i64(scols, dev), _i64(dcols, dev), sig, dst, dst_rs, dst_cs)
 
 
 def select_basis_indices(sset: np.ndarray, qnlist: List[tuple], Mmax: int, percent=0) -> List[int]:
@@ -215,61 +206,98 @@ class TruncatedSplit:
 
 def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_trunc_fn, percent=0,
                  full_matrices=True):
-    """Fused svd_qn(full_matrices=True) + compute_m_trunc + select_basis of
-    mp.py:693-778 for the two-site update.  keep_left=True keeps U
-    (left-to-right sweep: left = U, right = sigma Vh); otherwise V is kept
-    (left = U sigma, right = Vh)."""
-    blocks, rows, cols = qn_block_svd(coef, qnbigl, qnbigr, qntot, full_matrices=full_matrices)
+    """Fused svd_qn + compute_m_trunc + select_basis of mp.py:693-778.
+
+    keep_left=True keeps U (left-to-right sweep: left = U, right = sigma Vh);
+    otherwise V is kept (left = U sigma, right = Vh).  Per QN block X the
+    kept side comes from the Hermitian eigendecomposition of its Gram matrix
+    (X X^H for U, X^H X for V; FP64 GEMM + cuSOLVER), which also supplies the
+    zero-sigma completion columns the reference appends with
+    full_matrices=True (svd_qn.py:12-86).  The singular values used for
+    ordering and truncation are the norms of the projected rows/columns
+    (||u_j^H X|| or ||X v_j||), which stay accurate far below sqrt(eps)."""
     eng = Engine.get(coef.device)
-    # host view of the reference's concatenated order: nonzero parts block by block,
-    # then the zero-sigma paddings block by block (svd_qn.py:222-230)
+    rows = int(np.prod(qnbigl.shape[:-1]))
+    cols = int(np.prod(qnbigr.shape[:-1]))
+    mat = coef.reshape(rows, cols).contiguous()
+    qntot = np.asarray(qntot)
+    qs = len(qntot)
+    lq = qnbigl.reshape(-1, qs)
+    rq = qnbigr.reshape(-1, qs)
+    blocks = []
+    for nl in set(tuple(t) for t in lq):
+        nr = tuple(qntot - np.array(nl))
+        rset = np.where(get_qn_mask(rq, nr))[0]
+        if len(rset) == 0:
+            continue
+        lset = np.where(get_qn_mask(lq, nl))[0]
+        X = _gather(eng, mat, lset, rset)
+        m, n = X.shape
+        dim = min(m, n)
+        upad, vpad = _pad_counts(m, n, full_matrices)
+        if keep_left:
+            G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
+            _, K = torch.linalg.eigh(G)
+            K = torch.flip(K, dims=[1])                       # descending eigenvalues
+            P = eng.matmul(K[:, :dim].transpose(0, 1), X, conj_a=True)   # (dim, n) = sigma Vh
+            S = torch.linalg.vector_norm(P, dim=1)
+            npad = upad
+        else:
+            G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
+            _, K = torch.linalg.eigh(G)
+            K = torch.flip(K, dims=[1])
+            P = eng.matmul(X, K[:, :dim])                     # (m, dim) = U sigma
+            S = torch.linalg.vector_norm(P, dim=0)
+            npad = vpad
+        blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=dim, npad=npad))
+    if not blocks:
+        raise ValueError("Invalid quantum number")
+    Sh = torch.cat([b["S"] for b in blocks]).cpu().numpy()
+    off = 0
+    for b in blocks:
+        b["Sh"] = Sh[off:off + b["dim"]]
+        off += b["dim"]
+    # the reference's concatenated order: nonzero parts block by block, then
+    # the zero-sigma paddings block by block (svd_qn.py:222-230)
     sig, qns, where = [], [], []
     for bi, b in enumerate(blocks):
-        for j in range(len(b.S)):
-            sig.append(b.S[j])
-            qns.append(b.nl if keep_left else b.nr)
-            where.append((bi, j, False))
+        for j in range(b["dim"]):
+            sig.append(b["Sh"][j])
+            qns.append(b["nl"] if keep_left else b["nr"])
+            where.append((bi, j))
     for bi, b in enumerate(blocks):
-        npad = b.upad if keep_left else b.vpad
-        for p in range(npad):
+        for p in range(b["npad"]):
             sig.append(0.0)
-            qns.append(b.nl if keep_left else b.nr)
-            where.append((bi, p, True))
+            qns.append(b["nl"] if keep_left else b["nr"])
+            where.append((bi, b["dim"] + p))
     sig = np.asarray(sig, dtype=np.float64)
-    m = m_trunc_fn(sig)
-    sidx = select_basis_indices(sig, qns, m, percent)
+    mtr = m_trunc_fn(sig)
+    sidx = select_basis_indices(sig, qns, mtr, percent)
     mdim = len(sidx)
     left = torch.zeros((rows, mdim), dtype=coef.dtype, device=coef.device)
     right = torch.zeros((mdim, cols), dtype=coef.dtype, device=coef.device)
     per_block = {}
     for out_col, i in enumerate(sidx):
-        bi, j, pad = where[i]
-        entry = per_block.setdefault(bi, ([], [], [], []))
-        if pad:
-            entry[2].append(j)
-            entry[3].append(out_col)
-        else:
-            entry[0].append(j)
-            entry[1].append(out_col)
-    for bi, (cols_nz, out_nz, cols_pad, out_pad) in per_block.items():
+        bi, j = where[i]
+        per_block.setdefault(bi, ([], []))
+        per_block[bi][0].append(j)
+        per_block[bi][1].append(out_col)
+    for bi, (kc, oc) in per_block.items():
         b = blocks[bi]
-        k = b.U.shape[1]
-        n = b.Vh.shape[1]
-        if cols_nz:
-            s_sel = b.S[cols_nz]
-            # left[lset[i], out_j] = U[i, j] (* sigma_j when V is kept)
-            _scatter(eng, b.U, k, 1, b.lset, cols_nz, out_nz, None if keep_left else s_sel, left, mdim, 1)
-            # right[out_j, rset[i]] = Vh[j, i] (* sigma_j when U is kept)
-            _scatter(eng, b.Vh, 1, n, b.rset, cols_nz, out_nz, s_sel if keep_left else None, right, 1, cols)
-        if cols_pad:
-            npad = max(cols_pad) + 1
-            if keep_left:
-                pad = _completion(b.U.contiguous(), npad).contiguous()
-                _scatter(eng, pad, npad, 1, b.lset, cols_pad, out_pad, None, left, mdim, 1)
-            else:
-                # V columns are the rows of Vh without conjugation (svd_qn.py:212 block_vt.T)
-                pad = _completion(b.Vh.transpose(0, 1).contiguous(), npad).contiguous()
-                _scatter(eng, pad, npad, 1, b.rset, cols_pad, out_pad, None, right, 1, cols)
+        nz = [(j, o) for j, o in zip(kc, oc) if j < b["dim"]]
+        if keep_left:
+            # left[lset[i], out] = K[i, j] (kept basis incl. completion columns)
+            _scatter(eng, b["K"], b["lset"], kc, oc, None, left, mdim, 1)
+            if nz:
+                # right[out, rset[i]] = P[j, i]  (= sigma_j Vh[j, i]); completion rows stay 0
+                _scatter(eng, b["P"].transpose(0, 1), b["rset"], [j for j, _ in nz], [o for _, o in nz], None, right,
+                         1, cols)
+        else:
+            # right[out, rset[i]] = conj(K[i, j]) : the reference's v = Vt.T rows
+            _scatter(eng, b["K"].conj().resolve_conj() if b["K"].is_complex() else b["K"], b["rset"], kc, oc, None,
+                     right, 1, cols)
+            if nz:
+                _scatter(eng, b["P"], b["lset"], [j for j, _ in nz], [o for _, o in nz], None, left, mdim, 1)
     qn_new = np.array([qns[i] for i in sidx]).reshape(mdim, -1)
     return TruncatedSplit(left, right, qn_new, mdim, sig[sidx])
 
@@ -288,9 +316,9 @@ def qr_split(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
     for b, k in zip(blocks, ks):
         cidx = list(range(k))
         out = list(range(off, off + k))
-        _scatter(eng, b.U, b.U.shape[1], 1, b.lset, cidx, out, None, u, ktot, 1)
+        _scatter(eng, b.U, b.lset, cidx, out, None, u, ktot, 1)
         # vt rows: dst (row=off+j, col=rset[i]) <- Vh[j, i]
-        _scatter(eng, b.Vh, 1, b.Vh.shape[1], b.rset, cidx, out, None, vt, 1, cols)
+        _scatter(eng, b.Vh.transpose(0, 1), b.rset, cidx, out, None, vt, 1, cols)
         qnl += [b.nl] * k
         qnr += [b.nr] * k
         off += k
@@ -315,9 +343,9 @@ def svd_qn(coef_array, qnbigl, qnbigr, qntot, QR=False, system=None, full_matric
     off = 0
     for b in blocks:
         k = b.S.size
-        _scatter(eng, b.U, b.U.shape[1], 1, b.lset, list(range(k)), list(range(off, off + k)), None, u, u.shape[1], 1)
-        _scatter(eng, b.Vh, 1, b.Vh.shape[1], b.rset, list(range(k)), list(range(off, off + k)), None, v, v.shape[1],
-                 1)
+        _scatter(eng, b.U, b.lset, list(range(k)), list(range(off, off + k)), None, u, u.shape[1], 1)
+        _scatter(eng, b.Vh.transpose(0, 1), b.rset, list(range(k)), list(range(off, off + k)), None, v,
+                 v.shape[1], 1)
         su.append(b.S)
         sv.append(b.S)
         qnl += [b.nl] * k
@@ -327,15 +355,13 @@ def svd_qn(coef_array, qnbigl, qnbigr, qntot, QR=False, system=None, full_matric
     for b in blocks:
         if b.upad:
             pad = _completion(b.U, b.upad)
-            _scatter(eng, pad, pad.shape[1], 1, b.lset, list(range(b.upad)), list(range(uo, uo + b.upad)), None, u,
-                     u.shape[1], 1)
+            _scatter(eng, pad, b.lset, list(range(b.upad)), list(range(uo, uo + b.upad)), None, u, u.shape[1], 1)
             uo += b.upad
         su.append(np.zeros(b.upad))
         qnl += [b.nl] * b.upad
         if b.vpad:
             pad = _completion(b.Vh.transpose(0, 1).contiguous(), b.vpad).contiguous()
-            _scatter(eng, pad, pad.shape[1], 1, b.rset, list(range(b.vpad)), list(range(vo, vo + b.vpad)), None, v,
-                     v.shape[1], 1)
+            _scatter(eng, pad, b.rset, list(range(b.vpad)), list(range(vo, vo + b.vpad)), None, v, v.shape[1], 1)
             vo += b.vpad
         sv.append(np.zeros(b.vpad))
         qnr += [b.nr] * b.vpad

@@ -41,3 +41,16 @@ def mps_from_golden(d, prefix, compress=None):
 
 def mpo_from_golden(d, prefix, n):
     return [d[f"{prefix}/W_{i}"] for i in range(n)]
+
+
+@pytest.fixture
+def cpu_engine(monkeypatch):
+    """Run the engine's host logic on the CPU stand-in (tests/fake_engine.py)."""
+    import torch
+    from fake_engine import FakeEngine
+    from renormalizer_b200 import _native
+    from renormalizer_b200.backend import Backend
+    fake = FakeEngine()
+    monkeypatch.setattr(_native.Engine, "get", classmethod(lambda cls, device=None: fake))
+    monkeypatch.setattr(Backend, "device", property(lambda self: torch.device("cpu")))
+    return fake
