@@ -235,20 +235,38 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         m, n = X.shape
         dim = min(m, n)
         upad, vpad = _pad_counts(m, n, full_matrices)
-        if keep_left:
+        if keep_left and m <= n:
+            # kept side is the small side: its Gram eigenbasis is the kept basis
             G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
             _, K = torch.linalg.eigh(G)
             K = torch.flip(K, dims=[1])                       # descending eigenvalues
             P = eng.matmul(K[:, :dim].transpose(0, 1), X, conj_a=True)   # (dim, n) = sigma Vh
             S = torch.linalg.vector_norm(P, dim=1)
-            npad = upad
-        else:
+        elif keep_left:
+            # m > n: eigen-solve the small side, orthonormalise X v_j (QR keeps the
+            # column order) and project X onto it
+            G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
+            _, V = torch.linalg.eigh(G)
+            V = torch.flip(V, dims=[1])
+            Us = eng.matmul(X, V)                              # (m, dim) = U sigma
+            S = torch.linalg.vector_norm(Us, dim=0)
+            K, _ = torch.linalg.qr(Us, mode="reduced")
+            P = eng.matmul(K.transpose(0, 1), X, conj_a=True)  # (dim, n)
+        elif n <= m:
             G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
             _, K = torch.linalg.eigh(G)
             K = torch.flip(K, dims=[1])
             P = eng.matmul(X, K[:, :dim])                     # (m, dim) = U sigma
             S = torch.linalg.vector_norm(P, dim=0)
-            npad = vpad
+        else:
+            G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
+            _, U = torch.linalg.eigh(G)
+            U = torch.flip(U, dims=[1])
+            Vs = eng.matmul(X.transpose(0, 1), U, conj_a=True)  # (n, dim): column j = sigma_j v_j
+            S = torch.linalg.vector_norm(Vs, dim=0)
+            K, _ = torch.linalg.qr(Vs, mode="reduced")
+            P = eng.matmul(X, K)                               # (m, dim)
+        npad = upad if keep_left else vpad
         blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=dim, npad=npad))
     if not blocks:
         raise ValueError("Invalid quantum number")
@@ -284,6 +302,10 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         per_block[bi][1].append(out_col)
     for bi, (kc, oc) in per_block.items():
         b = blocks[bi]
+        if max(kc) >= b["K"].shape[1]:
+            # completion columns beyond the computed basis: orthonormal, drawn like
+            # svd_qn.py:52-63 from numpy's global RNG, built only when selected
+            b["K"] = torch.cat([b["K"], _completion(b["K"], max(kc) + 1 - b["K"].shape[1])], dim=1)
         nz = [(j, o) for j, o in zip(kc, oc) if j < b["dim"]]
         if keep_left:
             # left[lset[i], out] = K[i, j] (kept basis incl. completion columns)
