@@ -97,15 +97,24 @@ int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
                     const void* psi, void* y, void* workspace,
                     size_t workspace_bytes);
 
-/* Plain strided GEMM on the same FP64 tensor-core kernel (used for the
- * bond-absorb products of the sweeps, mps.py:1361/1394 tensordot):
+/* Plain strided GEMM on the engine's kernels (bond-absorb products of the
+ * sweeps, mps.py:1361/1394 tensordot; also the unit under test of the split
+ * tensor-core path):
  *   C[m, n] = sum_k opA(A)[m, k] opB(B)[k, n],  C row stride c_rs, unit column
  *   stride; A[m,k] at m*a_rs + k*a_cs, B[k,n] at k*b_rs + n*b_cs; *_conj
- *   conjugates an operand; C is complex128 if A or B is. */
+ *   conjugates an operand; C is complex128 if A or B is.  prec RENO_PREC_FP64
+ *   needs no workspace; the split modes need reno_gemm_workspace_bytes. */
+int reno_gemm_workspace_bytes(int32_t M, int32_t N, int32_t K, int32_t a_dtype,
+                              int32_t b_dtype, int32_t prec, size_t* bytes);
 int reno_gemm(reno_ctx* ctx, int32_t M, int32_t N, int32_t K, const void* A,
               int32_t a_dtype, int64_t a_rs, int64_t a_cs, int32_t a_conj,
               const void* B, int32_t b_dtype, int64_t b_rs, int64_t b_cs,
-              int32_t b_conj, void* C, int64_t c_rs, int32_t prec);
+              int32_t b_conj, void* C, int64_t c_rs, int32_t prec, void* ws,
+              size_t ws_bytes);
+/* Reads and clears the device-side error word of the tensor-core kernels:
+ * 0 = none, 1000 + site = an mbarrier wait that ran out its bounded spin
+ * (the kernel then skipped its remaining work and freed its TMEM). */
+int reno_device_error(reno_ctx* ctx, int32_t* code);
 
 /* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
  *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]

@@ -46,8 +46,10 @@ _SIGS = {
     "reno_launch_count": (_c_int, [ctypes.POINTER(ctypes.c_longlong)]),
     "reno_heff_workspace_bytes": (_c_int, [ctypes.POINTER(HeffDesc), ctypes.POINTER(_c_sz)]),
     "reno_heff_apply": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
+    "reno_gemm_workspace_bytes": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_c_sz)]),
     "reno_gemm": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _c_i64, _c_i64, _c_int, _vp, _c_int, _c_i64,
-                           _c_i64, _c_int, _vp, _c_i64, _c_int]),
+                           _c_i64, _c_int, _vp, _c_i64, _c_int, _vp, _c_sz]),
+    "reno_device_error": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),
     "reno_env_workspace_bytes": (_c_int, [ctypes.POINTER(EnvDesc), ctypes.POINTER(_c_sz)]),
     "reno_env_update": (_c_int, [_vp, ctypes.POINTER(EnvDesc), _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
@@ -211,12 +213,18 @@ class Engine:
                                             ptr(y), ptr(ws), ws.numel()), "reno_heff_apply")
         self.launches += 1
 
+    def device_error(self) -> int:
+        """first timed-out wait of the tensor-core kernels since the last call (0 = none)"""
+        c = ctypes.c_int32(0)
+        self.check(self.lib.reno_device_error(self.ctx, ctypes.byref(c)), "reno_device_error")
+        return int(c.value)
+
     def heff_diag(self, desc: HeffDesc, L, W1, W2, R, out):
         self.check(self.lib.reno_heff_diag(self.ctx, ctypes.byref(desc), ptr(L), ptr(W1), ptr(W2), ptr(R), ptr(out)),
                    "reno_heff_diag")
 
-    def matmul(self, A: torch.Tensor, B: torch.Tensor, conj_a=False, conj_b=False) -> torch.Tensor:
-        """C = op(A) @ op(B) for 2-D device tensors (any strides) on the FP64 kernel."""
+    def matmul(self, A: torch.Tensor, B: torch.Tensor, conj_a=False, conj_b=False, prec="fp64") -> torch.Tensor:
+        """C = op(A) @ op(B) for 2-D device tensors (any strides) on the engine's GEMM."""
         assert A.dim() == 2 and B.dim() == 2 and A.shape[1] == B.shape[0]
         # a lazy conj view is the raw memory of the conjugate: fold it into the kernel's conj flag
         if A.is_conj():
@@ -226,10 +234,18 @@ class Engine:
         A, B = raw_view(A), raw_view(B)
         cplx = A.is_complex() or B.is_complex()
         C = torch.empty((A.shape[0], B.shape[1]), dtype=torch.complex128 if cplx else torch.float64, device=A.device)
+        code = PREC[prec]
+        wsp, wsn = None, 0
+        if code:
+            n = _c_sz()
+            self.check(self.lib.reno_gemm_workspace_bytes(A.shape[0], B.shape[1], A.shape[1], dtype_code(A),
+                                                          dtype_code(B), code, ctypes.byref(n)), "reno_gemm_workspace")
+            ws = self.workspace(int(n.value))
+            wsp, wsn = ptr(ws), ws.numel()
         self.check(self.lib.reno_gemm(self.ctx, A.shape[0], B.shape[1], A.shape[1], _vp(A.data_ptr()), dtype_code(A),
                                       A.stride(0), A.stride(1), int(conj_a), _vp(B.data_ptr()), dtype_code(B),
-                                      B.stride(0), B.stride(1), int(conj_b), _vp(C.data_ptr()), C.stride(0), 0),
-                   "reno_gemm")
+                                      B.stride(0), B.stride(1), int(conj_b), _vp(C.data_ptr()), C.stride(0), code,
+                                      wsp, wsn), "reno_gemm")
         self.launches += 1
         return C
 

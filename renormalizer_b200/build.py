@@ -63,7 +63,7 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_verbose: boo
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(compile_one, _sources()))
     tmp = LIB_PATH.with_suffix(".so.tmp")
-    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcuda"]
+    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc link failed:\n{r.stderr}")

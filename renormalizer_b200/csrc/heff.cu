@@ -14,6 +14,7 @@
 #include "reno_common.cuh"
 #include "gemm_fp64.cuh"
 #include "split_gemm.cuh"
+#include <vector>
 
 namespace reno {
 
@@ -108,17 +109,27 @@ static GemmParams gp(int M, int N, int K, int batch, GemmOperand A, GemmOperand 
   return p;
 }
 
-// Dispatch one GEMM stage at the requested arithmetic.  `big` marks the
-// O(M^3) stages that the split-precision tensor-core kernel takes over.
-static cudaError_t run_stage(const GemmParams& p, int prec, void* split_ws, size_t split_ws_bytes, cudaStream_t st) {
-  if (prec == RENO_PREC_FP64) return gemm_fp64(p, st);
-  return split_gemm(p, prec, split_ws, split_ws_bytes, st);
+// One GEMM stage of a contraction chain at a given arithmetic.
+struct Stage {
+  GemmParams p;
+  int prec;
+};
+
+static cudaError_t run_stage(const Stage& s, void* split_ws, size_t split_ws_bytes, cudaStream_t st) {
+  if (s.prec == RENO_PREC_FP64) return gemm_fp64(s.p, st);
+  return split_gemm(s.p, s.prec, split_ws, split_ws_bytes, st);
+}
+
+static size_t split_need(const std::vector<Stage>& stages) {
+  size_t m = 0;
+  for (const Stage& s : stages) m = std::max(m, split_gemm_required_bytes(s.p, s.prec));
+  return m;
 }
 
 // ---------------------------------------------------------------- heff
-struct HeffPlan {
-  int dt_T1, dt_T2, dt_T3, dt_y;
-  size_t off_wt1, off_wt2, off_t1, off_t2, off_split, total, split_bytes;
+struct HeffLayout {
+  int dt_T1, dt_T2, dt_y;
+  size_t off_wt1, off_wt2, off_t1, off_t2, off_split;
 };
 
 static int validate_heff(const reno_heff_desc* d) {
@@ -134,18 +145,14 @@ static int validate_heff(const reno_heff_desc* d) {
   return RENO_OK;
 }
 
-static HeffPlan plan_heff(const reno_heff_desc* d) {
-  HeffPlan p{};
+static HeffLayout heff_layout(const reno_heff_desc* d) {
+  HeffLayout p{};
   const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wm = d->wm, wr = d->wr, d1 = d->d1, d2 = d->d2;
   p.dt_T1 = promote(d->env_dtype, d->psi_dtype);
-  p.dt_T2 = promote(p.dt_T1, d->mpo_dtype);
-  p.dt_T3 = p.dt_T2;
+  p.dt_T2 = d->nsite == 0 ? p.dt_T1 : promote(p.dt_T1, d->mpo_dtype);
   p.dt_y = promote(p.dt_T2, d->env_dtype);
-  size_t off = 0;
   int64_t n_wt1 = 0, n_wt2 = 0, n_t1 = 0, n_t2 = 0;
   if (d->nsite == 0) {
-    p.dt_T2 = p.dt_T1;
-    p.dt_y = p.dt_T1;
     n_t1 = ml * wl * mr;
   } else if (d->nsite == 1) {
     n_wt1 = d1 * wr * wl * d1;
@@ -157,6 +164,7 @@ static HeffPlan plan_heff(const reno_heff_desc* d) {
     n_t1 = std::max(ml * wl * d1 * d2 * mr, ml * d1 * d2 * wr * mr);  // T1, later reused for T3
     n_t2 = ml * d1 * wm * d2 * mr;
   }
+  size_t off = 0;
   p.off_wt1 = off;
   off = align256(off + n_wt1 * esz(d->mpo_dtype));
   p.off_wt2 = off;
@@ -166,16 +174,48 @@ static HeffPlan plan_heff(const reno_heff_desc* d) {
   p.off_t2 = off;
   off = align256(off + n_t2 * esz(p.dt_T2));
   p.off_split = off;
-  p.split_bytes = 0;
-  if (d->prec != RENO_PREC_FP64) {
-    // the split kernel stages operands of the largest GEMM in its own format
-    const int64_t big_a = std::max<int64_t>(ml * wl * ml, ml * d1 * std::max<int64_t>(d2, 1) * wr * mr);
-    const int64_t big_b = std::max<int64_t>(ml * d1 * std::max<int64_t>(d2, 1) * mr, wr * mr * mr);
-    p.split_bytes = split_gemm_workspace_bytes(big_a, big_b);
-    off = align256(off + p.split_bytes);
-  }
-  p.total = off;
   return p;
+}
+
+// the GEMM stages of hop_expr.py:57-103 with the reference's C-order strides
+static std::vector<Stage> heff_stages(const reno_heff_desc* d, const HeffLayout& lay, char* w, const void* L,
+                                      const void* R, const void* psi, void* y) {
+  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wm = d->wm, wr = d->wr, d1 = d->d1, d2 = d->d2;
+  const int ev = d->env_dtype, pv = d->psi_dtype, mv = d->mpo_dtype, pr = d->prec;
+  void* Wt1 = w + lay.off_wt1;
+  void* Wt2 = w + lay.off_wt2;
+  void* T1 = w + lay.off_t1;
+  void* T2 = w + lay.off_t2;
+  std::vector<Stage> s;
+  if (d->nsite == 0) {
+    s.push_back({gp(ml * wl, mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, mr), T1, mr, 1), pr});
+    s.push_back({gp(ml, mr, wl * mr, 1, opnd(T1, lay.dt_T1, wl * mr, 1), opnd(R, ev, wl * mr, 1), y, mr, 1), pr});
+  } else if (d->nsite == 1) {
+    s.push_back({gp(ml * wl, d1 * mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, d1 * mr), T1, d1 * mr, 1), pr});
+    s.push_back({gp(d1 * wr, mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1), opnd(T1, lay.dt_T1, 1, mr, wl * d1 * mr), T2,
+                    mr, 1, d1 * wr * mr),
+                 pr});
+    s.push_back({gp(ml * d1, mr, wr * mr, 1, opnd(T2, lay.dt_T2, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1), pr});
+  } else {
+    const int64_t n12 = d1 * d2 * mr;
+    void* T3 = T1;
+    s.push_back({gp(ml * wl, n12, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, n12), T1, n12, 1), pr});
+    s.push_back({gp(d1 * wm, d2 * mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1),
+                    opnd(T1, lay.dt_T1, 1, d2 * mr, wl * d1 * d2 * mr), T2, d2 * mr, 1, d1 * wm * d2 * mr),
+                 pr});
+    s.push_back({gp(d2 * wr, mr, wm * d2, ml * d1, opnd(Wt2, mv, wm * d2, 1), opnd(T2, lay.dt_T2, 1, mr, wm * d2 * mr),
+                    T3, mr, 1, d2 * wr * mr),
+                 pr});
+    s.push_back({gp(ml * d1 * d2, mr, wr * mr, 1, opnd(T3, lay.dt_T2, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1),
+                 pr});
+  }
+  return s;
+}
+
+static size_t heff_total(const reno_heff_desc* d) {
+  const HeffLayout lay = heff_layout(d);
+  char* nul = nullptr;
+  return lay.off_split + align256(split_need(heff_stages(d, lay, nul, nullptr, nullptr, nullptr, nullptr)));
 }
 
 }  // namespace reno
@@ -184,7 +224,7 @@ using namespace reno;
 
 extern "C" int reno_heff_workspace_bytes(const reno_heff_desc* d, size_t* bytes) {
   if (validate_heff(d) != RENO_OK || !bytes) return RENO_ERR_INVALID;
-  *bytes = plan_heff(d).total;
+  *bytes = heff_total(d);
   return RENO_OK;
 }
 
@@ -195,67 +235,31 @@ extern "C" int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* d, const voi
   if (validate_heff(d) != RENO_OK) return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply: invalid descriptor");
   if (!L || !R || !psi || !y || (d->nsite >= 1 && !W1) || (d->nsite == 2 && !W2))
     return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply: null tensor pointer");
-  const HeffPlan p = plan_heff(d);
-  if (ws_bytes < p.total || (p.total > 0 && !ws))
-    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heff_apply: workspace too small");
+  const HeffLayout lay = heff_layout(d);
   char* w = static_cast<char*>(ws);
-  void* Wt1 = w + p.off_wt1;
-  void* Wt2 = w + p.off_wt2;
-  void* T1 = w + p.off_t1;
-  void* T2 = w + p.off_t2;
-  void* sws = w + p.off_split;
+  const std::vector<Stage> stages = heff_stages(d, lay, w, L, R, psi, y);
+  const size_t need_split = split_need(stages);
+  if (ws_bytes < lay.off_split + need_split || !ws)
+    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heff_apply: workspace too small");
   cudaStream_t st = ctx->stream;
-  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wm = d->wm, wr = d->wr, d1 = d->d1, d2 = d->d2;
-  const int ev = d->env_dtype, pv = d->psi_dtype, mv = d->mpo_dtype;
   cudaError_t e = cudaSuccess;
-
-  if (d->nsite == 0) {
-    e = run_stage(gp(ml * wl, mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, mr), T1, mr, 1), d->prec, sws,
-                  p.split_bytes, st);
-    if (e == cudaSuccess)
-      e = run_stage(gp(ml, mr, wl * mr, 1, opnd(T1, p.dt_T1, wl * mr, 1), opnd(R, ev, wl * mr, 1), y, mr, 1),
-                    d->prec, sws, p.split_bytes, st);
-  } else if (d->nsite == 1) {
-    e = launch_wt(W1, Wt1, mv, wl, d1, wr, 0, st);
-    if (e == cudaSuccess)
-      e = run_stage(gp(ml * wl, d1 * mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, d1 * mr), T1, d1 * mr, 1),
-                    d->prec, sws, p.split_bytes, st);
-    if (e == cudaSuccess)
-      e = run_stage(gp(d1 * wr, mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1), opnd(T1, p.dt_T1, 1, mr, wl * d1 * mr),
-                       T2, mr, 1, d1 * wr * mr),
-                    RENO_PREC_FP64, sws, p.split_bytes, st);
-    if (e == cudaSuccess)
-      e = run_stage(gp(ml * d1, mr, wr * mr, 1, opnd(T2, p.dt_T2, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1),
-                    d->prec, sws, p.split_bytes, st);
-  } else {
-    e = launch_wt(W1, Wt1, mv, wl, d1, wm, 0, st);
-    if (e == cudaSuccess) e = launch_wt(W2, Wt2, mv, wm, d2, wr, 0, st);
-    const int64_t n12 = d1 * d2 * mr;
-    if (e == cudaSuccess)
-      e = run_stage(gp(ml * wl, n12, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, n12), T1, n12, 1), d->prec, sws,
-                    p.split_bytes, st);
-    if (e == cudaSuccess)
-      e = run_stage(gp(d1 * wm, d2 * mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1),
-                       opnd(T1, p.dt_T1, 1, d2 * mr, wl * d1 * d2 * mr), T2, d2 * mr, 1, d1 * wm * d2 * mr),
-                    RENO_PREC_FP64, sws, p.split_bytes, st);
-    void* T3 = T1;
-    if (e == cudaSuccess)
-      e = run_stage(gp(d2 * wr, mr, wm * d2, ml * d1, opnd(Wt2, mv, wm * d2, 1),
-                       opnd(T2, p.dt_T2, 1, mr, wm * d2 * mr), T3, mr, 1, d2 * wr * mr),
-                    RENO_PREC_FP64, sws, p.split_bytes, st);
-    if (e == cudaSuccess)
-      e = run_stage(gp(ml * d1 * d2, mr, wr * mr, 1, opnd(T3, p.dt_T3, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr,
-                       1),
-                    d->prec, sws, p.split_bytes, st);
+  if (d->nsite == 1) e = launch_wt(W1, w + lay.off_wt1, d->mpo_dtype, d->wl, d->d1, d->wr, 0, st);
+  if (d->nsite == 2) {
+    e = launch_wt(W1, w + lay.off_wt1, d->mpo_dtype, d->wl, d->d1, d->wm, 0, st);
+    if (e == cudaSuccess) e = launch_wt(W2, w + lay.off_wt2, d->mpo_dtype, d->wm, d->d2, d->wr, 0, st);
+  }
+  for (const Stage& s : stages) {
+    if (e != cudaSuccess) break;
+    e = run_stage(s, w + lay.off_split, need_split, st);
   }
   return check_cuda(ctx, e, "reno_heff_apply");
 }
 
 // ---------------------------------------------------------------- env update
 namespace reno {
-struct EnvPlan {
+struct EnvLayout {
   int dt_T1, dt_T2, dt_out;
-  size_t off_ketT, off_braT, off_wt, off_t1, off_t2, off_split, total, split_bytes;
+  size_t off_ketT, off_braT, off_wt, off_t1, off_t2, off_split;
 };
 
 static int validate_env(const reno_env_desc* d) {
@@ -270,8 +274,8 @@ static int validate_env(const reno_env_desc* d) {
   return RENO_OK;
 }
 
-static EnvPlan plan_env(const reno_env_desc* d) {
-  EnvPlan p{};
+static EnvLayout env_layout(const reno_env_desc* d) {
+  EnvLayout p{};
   const int64_t dd = d->d, wi = d->w_in, wo = d->w_out, ki = d->mk_in, ko = d->mk_out, bi = d->mb_in,
                 bo = d->mb_out;
   p.dt_T1 = promote(d->env_dtype, d->ket_dtype);
@@ -289,21 +293,42 @@ static EnvPlan plan_env(const reno_env_desc* d) {
   p.off_t2 = off;
   off = align256(off + bi * dd * wo * ko * esz(p.dt_T2));
   p.off_split = off;
-  p.split_bytes = 0;
-  if (d->prec != RENO_PREC_FP64) {
-    const int64_t big_a = std::max<int64_t>(bi * wi * ki, bo * bi * dd);
-    const int64_t big_b = std::max<int64_t>(ki * dd * ko, bi * dd * wo * ko);
-    p.split_bytes = split_gemm_workspace_bytes(big_a, big_b);
-    off = align256(off + p.split_bytes);
-  }
-  p.total = off;
   return p;
+}
+
+// lib.py:200-205 stage order on (possibly mirrored) bra/ket
+static std::vector<Stage> env_stages(const reno_env_desc* d, const EnvLayout& lay, char* w, const void* E,
+                                     const void* k_op, const void* b_op, int bra_dt, int conj_bra, void* out) {
+  const int64_t dd = d->d, wi = d->w_in, wo = d->w_out, ki = d->mk_in, ko = d->mk_out, bi = d->mb_in,
+                bo = d->mb_out;
+  void* Wt = w + lay.off_wt;
+  void* T1 = w + lay.off_t1;
+  void* T2 = w + lay.off_t2;
+  const int pr = d->prec;
+  std::vector<Stage> s;
+  s.push_back({gp(bi * wi, dd * ko, ki, 1, opnd(E, d->env_dtype, ki, 1), opnd(k_op, d->ket_dtype, 1, dd * ko), T1,
+                  dd * ko, 1),
+               pr});
+  s.push_back({gp(dd * wo, ko, wi * dd, bi, opnd(Wt, d->mpo_dtype, wi * dd, 1), opnd(T1, lay.dt_T1, 1, ko, wi * dd * ko),
+                  T2, ko, 1, dd * wo * ko),
+               pr});
+  s.push_back({gp(bo, wo * ko, bi * dd, 1, opnd(b_op, bra_dt, 1, bo, 0, conj_bra), opnd(T2, lay.dt_T2, 1, wo * ko), out,
+                  wo * ko, 1),
+               pr});
+  return s;
+}
+
+static size_t env_total(const reno_env_desc* d) {
+  const EnvLayout lay = env_layout(d);
+  char* nul = nullptr;
+  return lay.off_split +
+         align256(split_need(env_stages(d, lay, nul, nullptr, nullptr, nullptr, d->bra_dtype, 0, nullptr)));
 }
 }  // namespace reno
 
 extern "C" int reno_env_workspace_bytes(const reno_env_desc* d, size_t* bytes) {
   if (validate_env(d) != RENO_OK || !bytes) return RENO_ERR_INVALID;
-  *bytes = plan_env(d).total;
+  *bytes = env_total(d);
   return RENO_OK;
 }
 
@@ -314,44 +339,35 @@ extern "C" int reno_env_update(reno_ctx* ctx, const reno_env_desc* d, const void
   if (!E || !W || !ket || !out) return set_error(ctx, RENO_ERR_INVALID, "reno_env_update: null tensor pointer");
   if (!bra && (d->mb_in != d->mk_in || d->mb_out != d->mk_out))
     return set_error(ctx, RENO_ERR_INVALID, "reno_env_update: bra == NULL needs bra dims == ket dims");
-  const EnvPlan p = plan_env(d);
-  if (ws_bytes < p.total || !ws) return set_error(ctx, RENO_ERR_WORKSPACE, "reno_env_update: workspace too small");
+  const EnvLayout lay = env_layout(d);
   char* w = static_cast<char*>(ws);
   cudaStream_t st = ctx->stream;
   const int64_t dd = d->d, wi = d->w_in, wo = d->w_out, ki = d->mk_in, ko = d->mk_out, bi = d->mb_in,
                 bo = d->mb_out;
   const void* k_op = ket;
   const void* b_op = bra;
-  int bra_dt = bra ? d->bra_dtype : d->ket_dtype;
-  cudaError_t e = cudaSuccess;
+  const int bra_dt = bra ? d->bra_dtype : d->ket_dtype;
   if (d->side == 1) {
-    // mirror: ketT[c,e,h] = ket[h,e,c], braT[a,d,f] = bra[f,d,a]
-    e = launch_swap13(ket, w + p.off_ketT, d->ket_dtype, (int)ko, (int)dd, (int)ki, st);
-    k_op = w + p.off_ketT;
-    if (e == cudaSuccess && bra) {
-      e = launch_swap13(bra, w + p.off_braT, d->bra_dtype, (int)bo, (int)dd, (int)bi, st);
-      b_op = w + p.off_braT;
-    }
+    k_op = w + lay.off_ketT;
+    if (bra) b_op = w + lay.off_braT;
   }
   const int conj_bra = bra ? 0 : 1;
   if (!bra) b_op = k_op;
-  void* Wt = w + p.off_wt;
-  void* T1 = w + p.off_t1;
-  void* T2 = w + p.off_t2;
-  void* sws = w + p.off_split;
-  if (e == cudaSuccess) e = launch_wt(W, Wt, d->mpo_dtype, (int)wi, (int)dd, (int)wo, d->side == 1 ? 1 : 0, st);
-  if (e == cudaSuccess)
-    e = run_stage(gp(bi * wi, dd * ko, ki, 1, opnd(E, d->env_dtype, ki, 1), opnd(k_op, d->ket_dtype, 1, dd * ko), T1,
-                     dd * ko, 1),
-                  d->prec, sws, p.split_bytes, st);
-  if (e == cudaSuccess)
-    e = run_stage(gp(dd * wo, ko, wi * dd, bi, opnd(Wt, d->mpo_dtype, wi * dd, 1),
-                     opnd(T1, p.dt_T1, 1, ko, wi * dd * ko), T2, ko, 1, dd * wo * ko),
-                  RENO_PREC_FP64, sws, p.split_bytes, st);
-  if (e == cudaSuccess)
-    e = run_stage(gp(bo, wo * ko, bi * dd, 1, opnd(b_op, bra_dt, 1, bo, 0, conj_bra), opnd(T2, p.dt_T2, 1, wo * ko),
-                     out, wo * ko, 1),
-                  d->prec, sws, p.split_bytes, st);
+  const std::vector<Stage> stages = env_stages(d, lay, w, E, k_op, b_op, bra_dt, conj_bra, out);
+  const size_t need_split = split_need(stages);
+  if (ws_bytes < lay.off_split + need_split || !ws)
+    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_env_update: workspace too small");
+  cudaError_t e = cudaSuccess;
+  if (d->side == 1) {
+    // mirror: ketT[c,e,h] = ket[h,e,c], braT[a,d,f] = bra[f,d,a]
+    e = launch_swap13(ket, w + lay.off_ketT, d->ket_dtype, (int)ko, (int)dd, (int)ki, st);
+    if (e == cudaSuccess && bra) e = launch_swap13(bra, w + lay.off_braT, d->bra_dtype, (int)bo, (int)dd, (int)bi, st);
+  }
+  if (e == cudaSuccess) e = launch_wt(W, w + lay.off_wt, d->mpo_dtype, (int)wi, (int)dd, (int)wo, d->side == 1 ? 1 : 0, st);
+  for (const Stage& s : stages) {
+    if (e != cudaSuccess) break;
+    e = run_stage(s, w + lay.off_split, need_split, st);
+  }
   return check_cuda(ctx, e, "reno_env_update");
 }
 
@@ -432,15 +448,38 @@ extern "C" int reno_heff_diag(reno_ctx* ctx, const reno_heff_desc* d, const void
 }
 
 // ---------------------------------------------------------------- plain GEMM
+static GemmParams plain_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t a_dtype, int64_t a_rs,
+                             int64_t a_cs, int32_t a_conj, const void* B, int32_t b_dtype, int64_t b_rs, int64_t b_cs,
+                             int32_t b_conj, void* C, int64_t c_rs) {
+  return gp(M, N, K, 1, opnd(A, a_dtype, a_rs, a_cs, 0, a_conj), opnd(B, b_dtype, b_cs, b_rs, 0, b_conj), C, c_rs, 1);
+}
+
+extern "C" int reno_gemm_workspace_bytes(int32_t M, int32_t N, int32_t K, int32_t a_dtype, int32_t b_dtype,
+                                         int32_t prec, size_t* bytes) {
+  if (!bytes || M < 0 || N < 0 || K < 0 || prec < RENO_PREC_FP64 || prec > RENO_PREC_TF32X3) return RENO_ERR_INVALID;
+  const char* dummy = reinterpret_cast<const char*>(256);
+  GemmParams p = plain_gemm(M, N, K, dummy, a_dtype, K, 1, 0, dummy, b_dtype, N, 1, 0, (void*)dummy, N);
+  *bytes = split_gemm_required_bytes(p, prec);
+  return RENO_OK;
+}
+
 extern "C" int reno_gemm(reno_ctx* ctx, int32_t M, int32_t N, int32_t K, const void* A, int32_t a_dtype,
                          int64_t a_rs, int64_t a_cs, int32_t a_conj, const void* B, int32_t b_dtype, int64_t b_rs,
-                         int64_t b_cs, int32_t b_conj, void* C, int64_t c_rs, int32_t prec) {
+                         int64_t b_cs, int32_t b_conj, void* C, int64_t c_rs, int32_t prec, void* ws,
+                         size_t ws_bytes) {
   if (!ctx) return RENO_ERR_INVALID;
   if (M < 0 || N < 0 || K < 0 || !A || !B || !C || (a_dtype != RENO_F64 && a_dtype != RENO_C128) ||
-      (b_dtype != RENO_F64 && b_dtype != RENO_C128) || c_rs < N)
+      (b_dtype != RENO_F64 && b_dtype != RENO_C128) || c_rs < N || prec < RENO_PREC_FP64 || prec > RENO_PREC_TF32X3)
     return set_error(ctx, RENO_ERR_INVALID, "reno_gemm: bad arguments");
-  if (prec != RENO_PREC_FP64) return set_error(ctx, RENO_ERR_UNSUPPORTED, "reno_gemm: FP64 only");
-  GemmParams p = gp(M, N, K, 1, opnd(A, a_dtype, a_rs, a_cs, 0, a_conj), opnd(B, b_dtype, b_cs, b_rs, 0, b_conj), C,
-                    c_rs, 1);
-  return check_cuda(ctx, gemm_fp64(p, ctx->stream), "reno_gemm");
+  GemmParams p = plain_gemm(M, N, K, A, a_dtype, a_rs, a_cs, a_conj, B, b_dtype, b_rs, b_cs, b_conj, C, c_rs);
+  if (prec == RENO_PREC_FP64) return check_cuda(ctx, gemm_fp64(p, ctx->stream), "reno_gemm");
+  if (ws_bytes < split_gemm_required_bytes(p, prec) || !ws)
+    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_gemm: workspace too small");
+  return check_cuda(ctx, split_gemm(p, prec, ws, ws_bytes, ctx->stream), "reno_gemm");
+}
+
+extern "C" int reno_device_error(reno_ctx* ctx, int32_t* code) {
+  if (!ctx || !code) return RENO_ERR_INVALID;
+  *code = split_gemm_take_error();
+  return RENO_OK;
 }

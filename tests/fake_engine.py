@@ -64,7 +64,7 @@ class FakeEngine:
             r = torch.einsum("fda,abc,gdeb,hec->fgh", b, E.to(dt), W.to(dt), ket.to(dt))
         out.copy_(r)
 
-    def matmul(self, A, B, conj_a=False, conj_b=False):
+    def matmul(self, A, B, conj_a=False, conj_b=False, prec="fp64"):
         dt = torch.complex128 if (A.is_complex() or B.is_complex()) else torch.float64
         a, b = A.to(dt), B.to(dt)
         if conj_a:

@@ -1,0 +1,113 @@
+"""Split-precision tensor-core path (tcgen05 + TMA, BF16x3 / TF32x3 with FP32
+accumulation) against FP64 references.
+
+Tolerances (relative to max|C|): a BF16 hi/lo pair keeps ~17 significant
+bits of each operand, a TF32 pair ~22; with the dropped lo*lo term and FP32
+accumulation the products agree with FP64 to ~1e-5 (BF16x3) and ~1e-6
+(TF32x3).  The bounds below leave a 3-5x margin."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_cases, load_golden
+from oracle import reno_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"bf16x3": 5e-5, "tf32x3": 5e-6}
+HEFF = load_golden("heff_cases.npz")
+ENV = load_golden("env_cases.npz")
+
+
+def _eng():
+    from renormalizer_b200._native import Engine
+    return Engine.get(0)
+
+
+def _rand(shape, cplx, g):
+    if cplx:
+        return torch.complex(torch.randn(shape, dtype=torch.float64, device="cuda", generator=g),
+                             torch.randn(shape, dtype=torch.float64, device="cuda", generator=g))
+    return torch.randn(shape, dtype=torch.float64, device="cuda", generator=g)
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("ac,bc", [(False, False), (True, False), (False, True), (True, True)])
+@pytest.mark.parametrize("M,N,K", [(200, 300, 150), (7, 1000, 33), (1000, 9, 260)])
+def test_split_gemm_matches_fp64(prec, ac, bc, M, N, K):
+    eng = _eng()
+    g = torch.Generator(device="cuda").manual_seed(M + 7 * N + K)
+    A, B = _rand((M, K), ac, g), _rand((K, N), bc, g)
+    C = eng.matmul(A, B, prec=prec)
+    ref = A.to(C.dtype) @ B.to(C.dtype)
+    err = float((C - ref).abs().max() / ref.abs().max())
+    assert err < TOL[prec], err
+    assert eng.device_error() == 0
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+def test_split_gemm_strided_conj(prec):
+    eng = _eng()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    A = _rand((300, 129), True, g).transpose(0, 1)  # (129, 300) column-major view
+    B = _rand((300, 77), True, g)
+    C = eng.matmul(A, B, conj_a=True, prec=prec)
+    ref = A.conj() @ B
+    assert float((C - ref).abs().max() / ref.abs().max()) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("case", golden_cases(HEFF))
+def test_split_heff_matches_reference(prec, case):
+    from renormalizer_b200.hop_expr import HeffOperator
+    n = int(HEFF[f"{case}/nsite"])
+    Ws = [HEFF[f"{case}/W{i + 1}"] for i in range(n)]
+    psi = HEFF[f"{case}/psi"]
+    op = HeffOperator(HEFF[f"{case}/L"], HEFF[f"{case}/R"], Ws, psi.shape, prec=prec)
+    y = op(torch.from_numpy(psi).cuda()).cpu().numpy()
+    ref = HEFF[f"{case}/y"]
+    # a chain of 2-4 split GEMM stages
+    assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("case", golden_cases(ENV))
+def test_split_env_matches_reference(prec, case):
+    from renormalizer_b200.lib import contract_one_site
+    bra = ENV[f"{case}/bra"] if f"{case}/bra" in ENV.files else None
+    out = contract_one_site(ENV[f"{case}/E"], ENV[f"{case}/ms"], ENV[f"{case}/W"], str(ENV[f"{case}/domain"]),
+                            ms_conj=bra, prec=prec).cpu().numpy()
+    ref = ENV[f"{case}/out"]
+    assert np.abs(out - ref).max() / np.abs(ref).max() < 3 * TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+def test_split_heff_2site_holstein_block(prec):
+    """the config's 2-site block shape at reduced M (d1=16, d2=16, w=5)"""
+    from renormalizer_b200.hop_expr import HeffOperator
+    rng = np.random.default_rng(11)
+    ml, mr, d1, d2, w = 64, 48, 16, 16, 5
+    mk = lambda s: rng.standard_normal(s) + 1j * rng.standard_normal(s)
+    L, R, psi = mk((ml, w, ml)), mk((mr, w, mr)), mk((ml, d1, d2, mr))
+    W1, W2 = rng.standard_normal((w, d1, d1, w)), rng.standard_normal((w, d2, d2, w))
+    ref = O.hop(L, [W1, W2], R, psi)
+    y = HeffOperator(L, R, [W1, W2], psi.shape, prec=prec)(torch.from_numpy(psi).cuda()).cpu().numpy()
+    assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
+
+
+@pytest.mark.parametrize("prec,atol", [("bf16x3", 2e-5), ("tf32x3", 2e-6)])
+def test_split_tdvp_short_trajectory(prec, atol):
+    from renormalizer_b200 import EvolveConfig, EvolveMethod, backend
+    from test_gpu_tdvp import TDVP, engine_state
+    backend.prec = prec
+    try:
+        mps, mpo = engine_state("ps_hol4")
+        mps.evolve_config = EvolveConfig(EvolveMethod.tdvp_ps)
+        pops = [mps.e_occupations]
+        for _ in range(8):
+            mps = mps.evolve(mpo, float(TDVP["ps_hol4/dt"]))
+            pops.append(mps.e_occupations)
+    finally:
+        backend.prec = "fp64"
+    dev = np.abs(np.array(pops) - TDVP["ps_hol4/pops"]).max()
+    assert dev < atol, dev
