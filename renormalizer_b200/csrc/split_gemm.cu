@@ -33,7 +33,7 @@ constexpr int B_TILE = BN * KROW_BYTES;   // 32 KB
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr uint32_t TMEM_COLS = 256;
-constexpr long long WAIT_LIMIT = 200000000LL;  // bounded spin (~seconds)
+constexpr uint64_t WAIT_NS = 2000000000ull;  // bounded spin: 2 s of wall clock
 
 // device error word: 0 = ok; otherwise 1000 + site of the first timed-out wait
 __device__ int g_split_error = 0;
@@ -74,11 +74,21 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait: returns false (and raises the abort flag) on timeout
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait (WAIT_NS of wall clock): returns false and raises the abort flag on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int site) {
-  for (long long it = 0; it < WAIT_LIMIT; ++it) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0;; ++it) {
     if (mbar_try(bar, parity)) return true;
-    if (*abort_flag) return false;
+    if ((it & 255u) == 255u) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > WAIT_NS) break;
+    }
   }
   *abort_flag = 1;
   atomicCAS(&g_split_error, 0, 1000 + site);
