@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--prec", default=os.environ.get("RENO_BENCH_PREC", "fp64"),
+    ap.add_argument("--prec", default=os.environ.get("RENO_BENCH_PREC", "bf16x3"),
                     choices=["fp64", "bf16x3", "tf32x3"])
     ap.add_argument("--nmol", type=int, default=32)
     ap.add_argument("--nlev", type=int, default=16)
@@ -306,10 +306,11 @@ class PhaseTimer:
     def install(self):
         import importlib
         mps_mod = importlib.import_module("renormalizer_b200.mps")
+        lib_mod = importlib.import_module("renormalizer_b200.lib")
         self.wrap(mps_mod, "svd_truncate", "svd_truncate")
         self.wrap(mps_mod, "qr_split", "qr_split")
         self.wrap(mps_mod, "expm_krylov", "krylov_total")
-        self.wrap(mps_mod, "contract_one_site", "env_update")
+        self.wrap(lib_mod, "contract_one_site", "env_update")
         return self
 
     def uninstall(self):

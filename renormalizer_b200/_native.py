@@ -132,6 +132,18 @@ def ptr(t: Optional[torch.Tensor]):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def h2d(arr, device, dtype=None) -> torch.Tensor:
+    """Host array -> device tensor through pinned memory without a stream sync
+    (torch's caching host allocator keeps the staging block alive until the
+    copy has run)."""
+    import numpy as np
+    a = np.ascontiguousarray(arr if dtype is None else np.asarray(arr, dtype=dtype))
+    src = torch.from_numpy(a)
+    pinned = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+    pinned.copy_(src)
+    return pinned.to(device, non_blocking=True)
+
+
 def raw_view(t: torch.Tensor) -> torch.Tensor:
     """A tensor whose memory holds the values it denotes (no lazy conj/neg bit)."""
     if t.is_conj():

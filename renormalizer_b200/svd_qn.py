@@ -24,7 +24,7 @@ from typing import List, Optional
 import numpy as np
 import torch
 
-from ._native import Engine
+from ._native import Engine, h2d
 
 
 def add_outer(a: np.ndarray, b: np.ndarray) -> np.ndarray:
@@ -40,7 +40,9 @@ def get_qn_mask(qnmat: np.ndarray, qntot) -> np.ndarray:
 
 
 def _i64(x, device):
-    return torch.as_tensor(np.asarray(x, dtype=np.int64), device=device)
+    if device.type != "cuda":
+        return torch.as_tensor(np.asarray(x, dtype=np.int64), device=device)
+    return h2d(x, device, np.int64)
 
 
 @dataclass
@@ -146,7 +148,9 @@ def _scatter(eng: Engine, src: torch.Tensor, rows, scols, dcols, sigma, dst: tor
     if len(rows) == 0 or len(scols) == 0:
         return
     dev = dst.device
-    sig = None if sigma is None else torch.as_tensor(np.asarray(sigma, dtype=np.float64), device=dev)
+    sig = None
+    if sigma is not None:
+        sig = h2d(sigma, dev, np.float64) if dev.type == "cuda" else torch.as_tensor(np.asarray(sigma, np.float64))
     eng.qn_scatter(src, _i64(rows, dev), _i64(scols, dev), _i64(dcols, dev), sig, dst, dst_rs, dst_cs)
 
 
