@@ -116,6 +116,21 @@ int reno_gemm(reno_ctx* ctx, int32_t M, int32_t N, int32_t K, const void* A,
  * (the kernel then skipped its remaining work and freed its TMEM). */
 int reno_device_error(reno_ctx* ctx, int32_t* code);
 
+/* Allocation-free variant of reno_heff_apply.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory (hosts
+ * that own the whole GPU through their own pool, foreign-language hosts that
+ * cannot keep a device allocation alive) and pass only inputs and outputs.
+ * Its scratch is a fixed array inside the library, RENO_NOALLOC_SCRATCH_BYTES
+ * on every GPU that loads the library, held until the process exits; larger
+ * problems are rejected with RENO_ERR_WORKSPACE.  All calls share the array
+ * (calls that overlap on the GPU race, so serialise them); nothing in it has
+ * to start at zero.  The first call on a device looks up the array's address
+ * and should come before any stream capture. */
+#define RENO_NOALLOC_SCRATCH_BYTES (128u << 20)
+int reno_heff_apply_noalloc(reno_ctx* ctx, const reno_heff_desc* desc,
+                            const void* L, const void* W1, const void* W2,
+                            const void* R, const void* psi, void* y);
+
 /* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
  *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]
  *   nsite 2: hdiag[a,c,d,f] = sum L[a,b,a] W1[b,c,c,e] W2[e,d,d,g] R[f,g,f]

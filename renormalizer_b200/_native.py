@@ -50,6 +50,7 @@ _SIGS = {
     "reno_gemm": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _c_i64, _c_i64, _c_int, _vp, _c_int, _c_i64,
                            _c_i64, _c_int, _vp, _c_i64, _c_int, _vp, _c_sz]),
     "reno_device_error": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
     "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),
     "reno_env_workspace_bytes": (_c_int, [ctypes.POINTER(EnvDesc), ctypes.POINTER(_c_sz)]),
     "reno_env_update": (_c_int, [_vp, ctypes.POINTER(EnvDesc), _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
