@@ -335,6 +335,14 @@ class OMps:
         last = stop_idx if stop_idx is not None else (-1 if full else 0)
         return range(self.qnidx, last, -1)
 
+    def move_qnidx(self, dstidx):  # mp.py:159-172
+        n = len(self)
+        for idx in range(self.qnidx + 1, n + 1):
+            self.qn[idx] = self.qntot - self.qn[idx]
+        for idx in range(n, dstidx, -1):
+            self.qn[idx] = self.qntot - self.qn[idx]
+        self.qnidx = dstidx
+
     def _switch_direction(self):  # mp.py:297-306
         if self.to_right:
             self.qnidx = len(self) - 1
@@ -776,10 +784,20 @@ def optimize_mps(mps: OMps, mpo, procedure, method="2site", e_rtol=1e-6, e_atol=
 
     procedure: list of (max_bonddim, percent).  Returns (energies, mps)."""
     assert method in ("1site", "2site")
-    assert mps.to_right is False and mps.qnidx == len(mps) - 1, "oracle expects a left-canonical start"
     mps.qn = [q.copy() for q in mps.qn]
-    mps.to_right = False
-    env_dom = "L"
+    # gs.py:97-102: a left-canonical start is right-canonicalised first and
+    # the environment is built from the right; any other start the other way
+    # (ensure_*_canonical, mp.py:206-228, always re-canonicalising)
+    if mps.qnidx == len(mps) - 1:
+        mps.move_qnidx(len(mps) - 1)
+        mps.to_right = False
+        mps.canonicalise()
+        env_dom = "R"
+    else:
+        mps.move_qnidx(0)
+        mps.to_right = True
+        mps.canonicalise()
+        env_dom = "L"
     environ = OEnviron(mps, mpo, env_dom)
     energies = []
     opt_e_idx = None

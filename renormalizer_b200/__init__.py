@@ -17,8 +17,10 @@ from .lib import Environ, contract_one_site
 from .hop_expr import hop_expr
 from .krylov import expm_krylov
 from .svd_qn import svd_qn
+from .davidson import davidson
+from .gs import optimize_mps
 
 __all__ = ["backend", "CompressConfig", "CompressCriteria", "EvolveConfig", "EvolveMethod", "OptimizeConfig",
            "BasisHalfSpin", "BasisSHO", "BasisSimpleElectron", "HolsteinModel", "Model", "Mol", "Op", "Phonon",
            "Quantity", "SpectralDensityFunction", "SpinBosonModel", "Mpo", "Mps", "Environ", "contract_one_site",
-           "hop_expr", "expm_krylov", "svd_qn"]
+           "hop_expr", "expm_krylov", "svd_qn", "davidson", "optimize_mps"]

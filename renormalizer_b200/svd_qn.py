@@ -112,7 +112,11 @@ def qn_block_svd(coef: torch.Tensor, qnbigl, qnbigr, qntot, full_matrices=True, 
 
 def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
     """Per-block QR (system "L") or RQ (system "R"), economic (svd_qn.py:195-204).
-    RQ is formed from the QR of the conjugate transpose: A = R1^H Q1^H."""
+    RQ comes from the Householder QR of the reversed conjugate transpose:
+    (J A J)^H = Q1 R1 gives A = (J R1^H J)(J Q1^H J), with J R1^H J upper
+    triangular.  Householder QR processes the entries in the same order as
+    LAPACK's RQ (last row first, pivot on its last entry), so R and Q agree
+    with scipy.linalg.rq including the signs, not only up to a rotation."""
     eng = Engine.get(coef.device)
     rows = int(np.prod(qnbigl.shape[:-1]))
     cols = int(np.prod(qnbigr.shape[:-1]))
@@ -133,9 +137,9 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
             Q, R = torch.linalg.qr(blk, mode="reduced")
             blocks.append(QNBlock(nl, nr, lset, rset, Q, None, None, R))
         elif system == "R":
-            Q1, R1 = torch.linalg.qr(blk.mH, mode="reduced")
-            blocks.append(QNBlock(nl, nr, lset, rset, R1.mH.resolve_conj().contiguous(), None, None,
-                                  Q1.mH.resolve_conj().contiguous()))
+            Q1, R1 = torch.linalg.qr(blk.flip([0, 1]).mH, mode="reduced")
+            blocks.append(QNBlock(nl, nr, lset, rset, R1.mH.flip([0, 1]).resolve_conj().contiguous(), None, None,
+                                  Q1.mH.flip([0, 1]).resolve_conj().contiguous()))
         else:
             raise AssertionError("system must be L or R for QR")
     if not blocks:

@@ -1,0 +1,53 @@
+"""DMRG ground-state search (gs.optimize_mps) against the reference's own
+sweeps (tests/golden/dmrg_cases.npz): a 2-site Holstein chain (test_gs.py's
+model, procedure [[10,.4],[20,.2],[30,.1],[40,0],[40,0]]) and a 6-mode
+spin-boson chain, both from the reference's dumped random initial MPS.
+
+The per-sweep lowest energies must agree with the reference to 1e-9 relative
+(the reference itself moves by ~1e-13 between BLAS thread counts; Davidson
+stops at |de| < 1e-12 so iteration counts can differ by one), the number of
+sweeps before convergence must agree, and the Holstein energy must match the
+model's analytic ground state within test_gs.py's 1e-5."""
+import numpy as np
+import pytest
+
+from conftest import engine_chain, load_golden
+
+DMRG = load_golden("dmrg_cases.npz")
+PROC = {"hol_test_gs": ([[10, 0.4], [20, 0.2], [30, 0.1], [40, 0], [40, 0]], 1e-8),
+        "sbm6x4": ([[12, 0.4], [12, 0.2], [12, 0.1], [12, 0], [12, 0], [12, 0]], 1e-9)}
+
+
+def run_dmrg(tag, method="2site"):
+    from renormalizer_b200 import backend
+    from renormalizer_b200.gs import optimize_mps
+    backend.prec = "fp64"
+    mps, mpo = engine_chain(DMRG, tag)
+    proc, e_atol = PROC[tag]
+    mps.optimize_config.procedure = proc
+    mps.optimize_config.method = method
+    mps.optimize_config.e_atol = e_atol
+    energies, res = optimize_mps(mps, mpo)
+    return np.array(energies), res, mpo
+
+
+def check(tag, energies, res, mpo):
+    ref = DMRG[f"{tag}/energies"]
+    assert len(energies) == len(ref)
+    np.testing.assert_allclose(energies, ref, rtol=1e-9)
+    if tag == "hol_test_gs":
+        assert min(energies) == pytest.approx(float(DMRG["hol_test_gs/GS_E"]), rel=1e-5)
+    # the returned state is normalised, canonical and carries the energy
+    assert res.norm == pytest.approx(1.0, abs=1e-10)
+    assert np.real(res.expectation(mpo)) == pytest.approx(min(energies), rel=1e-7, abs=1e-9)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", ["hol_test_gs", "sbm6x4"])
+def test_dmrg_matches_reference(tag):
+    check(tag, *run_dmrg(tag))
+
+
+def test_dmrg_host_logic_matches_reference(cpu_engine):
+    """the sweep logic on the CPU stand-in engine, on the Holstein chain"""
+    check("hol_test_gs", *run_dmrg("hol_test_gs"))

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import load_golden
+from conftest import engine_chain, load_golden
 
 pytestmark = pytest.mark.gpu
 
@@ -18,25 +18,8 @@ TDVP = load_golden("tdvp_cases.npz")
 
 
 def engine_state(tag):
-    from renormalizer_b200 import CompressConfig, CompressCriteria, Mpo, Mps
-    from renormalizer_b200.model import BasisSHO, BasisSimpleElectron, Model
-    n = int(TDVP[f"{tag}/init/nsites"])
-    # a model carrying the local bases (dims + QN) of the dumped chain
-    basis = []
-    ie = 0
-    for i in range(n):
-        sq = TDVP[f"{tag}/init/sigmaqn_{i}"]
-        if sq.shape[0] == 2 and sq[1, 0] == 1:
-            basis.append(BasisSimpleElectron(ie))
-            ie += 1
-        else:
-            basis.append(BasisSHO(("ph", i), 1.0, int(sq.shape[0])))
-    model = Model(basis, [])
-    sites = [TDVP[f"{tag}/init/mt_{i}"] for i in range(n)]
-    qn = [TDVP[f"{tag}/init/qn_{i}"] for i in range(n + 1)]
-    mps = Mps.from_arrays(model, sites, qn, int(TDVP[f"{tag}/init/qnidx"]), TDVP[f"{tag}/init/qntot"],
-                          bool(TDVP[f"{tag}/init/to_right"]))
-    mpo = Mpo.from_tensors(model, [TDVP[f"{tag}/mpo/W_{i}"] for i in range(n)])
+    from renormalizer_b200 import CompressConfig, CompressCriteria
+    mps, mpo = engine_chain(TDVP, tag)
     mmax = int(TDVP[f"{tag}/mmax"])
     if mmax > 0:
         mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=mmax)
