@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--dt", type=float, default=0.025)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--heff-only", action="store_true",
+                    help="time only the workload's largest 2-site H_eff matvec (phonon-phonon block, M x 16 x 16 x M)")
     return ap.parse_args()
 
 
@@ -365,6 +367,9 @@ def run_engine(args, rank, world, dist):
     phases = PhaseTimer().install()
     barrier()
     l0 = launch_count()
+    import importlib
+    svdmod = importlib.import_module("renormalizer_b200.svd_qn")
+    sub0 = (svdmod.subspace.calls, svdmod.subspace.fallbacks)
     with ClockSampler(local) as clocks:
         s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s_ev.record()
@@ -373,6 +378,9 @@ def run_engine(args, rank, world, dist):
         e_ev.record()
         barrier()
     launches = launch_count() - l0
+    trunc = {"subspace_blocks": svdmod.subspace.calls - sub0[0], "fallbacks": svdmod.subspace.fallbacks - sub0[1],
+             "options": {"min_dim": svdmod.subspace.min_dim, "iters": svdmod.subspace.iters,
+                         "oversample": svdmod.subspace.oversample, "rtol": svdmod.subspace.rtol}}
     timer.uninstall()
     phases.uninstall()
     t_ms = s_ev.elapsed_time(e_ev)
@@ -455,14 +463,59 @@ def run_engine(args, rank, world, dist):
                            "dt": args.dt, "prec": args.prec, "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (MPS ~1.5 GB, environments ~1 GB resident in HBM)"},
                 "tflops_heff2": achieved, "heff2_ms": round(heff_ms, 1), "phase_ms": phases.result(),
-                "krylov": kry_timed, "bond_dims_max": max(mps.bond_dims),
+                "krylov": kry_timed, "bond_dims_max": max(mps.bond_dims), "truncation": trunc,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks.summary(), "fp64_engine": fp64}
         print(json.dumps(line), flush=True)
 
 
+def run_heff_only(args):
+    """--steps matvecs of the phonon-phonon block (ml = mr = M, d1 = d2 = nlev)
+    with the workload's own MPO tensors and seeded random complex L, R, psi.
+    Inputs (~1.6 GB incl. intermediates) exceed L2; each timed matvec reads
+    and writes them all."""
+    import torch
+    from renormalizer_b200 import Mpo, backend
+    from renormalizer_b200._native import launch_count
+    from renormalizer_b200.hop_expr import HeffOperator
+    torch.cuda.set_device(0)
+    backend.prec = args.prec
+    model = holstein_2mode(args.nmol, args.nlev)
+    mpo = Mpo(model)
+    i = next(k for k in range(1, len(mpo) - 1) if mpo[k].shape[1] == args.nlev and mpo[k + 1].shape[1] == args.nlev)
+    W1, W2 = mpo[i], mpo[i + 1]
+    wl, wm, wr = W1.shape[0], W1.shape[3], W2.shape[3]
+    M, d = args.M, args.nlev
+    g = torch.Generator(device="cuda").manual_seed(7)
+    cx = lambda *s: torch.complex(torch.randn(s, dtype=torch.float64, device="cuda", generator=g),
+                                  torch.randn(s, dtype=torch.float64, device="cuda", generator=g))
+    L, R, psi = cx(M, wl, M), cx(M, wr, M), cx(M, d, d, M)
+    op = HeffOperator(L, R, [W1, W2], psi.shape, prec=args.prec)
+    y = torch.empty_like(psi)
+    for _ in range(args.warmup):
+        op.apply(psi, y)
+    torch.cuda.synchronize()
+    l0 = launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s_ev, e_ev in evs:
+        s_ev.record()
+        op.apply(psi, y)
+        e_ev.record()
+    torch.cuda.synchronize()
+    ms = [s_ev.elapsed_time(e_ev) for s_ev, e_ev in evs]
+    fl = heff_flops(2, M, M, wl, wm, wr, d, d)
+    t = statistics.median(ms)
+    print(json.dumps({"metric": "2-site H_eff matvec (phonon-phonon block)", "value": fl / (t * 1e-3) / 1e12,
+                      "unit": "TFLOP/s", "ms_per_matvec": t, "ms_all": ms, "gflop": fl / 1e9, "prec": args.prec,
+                      "shape": {"M": M, "d1": d, "d2": d, "wl": wl, "wm": wm, "wr": wr},
+                      "gpu_launches_per_matvec": (launch_count() - l0) / args.steps}))
+
+
 def main():
     args = parse()
+    if args.heff_only:
+        run_heff_only(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

@@ -63,6 +63,14 @@ class CompressConfig:
         assert self.max_dims is not None
         return int(min(self.max_dims[idx + 1 if left else idx], len(sigma)))
 
+    def fixed_cap(self, idx: int, left: bool):
+        """The kept dimension's upper bound when the rule is ``fixed`` (the
+        same bond index as compute_m_trunc); None for threshold-based rules,
+        whose count depends on the whole spectrum."""
+        if self.criteria is not CompressCriteria.fixed or self.max_dims is None:
+            return None
+        return int(self.max_dims[idx + 1 if left else idx])
+
     def compute_m_trunc(self, sigma: np.ndarray, idx: int, left: bool) -> int:
         if self.criteria is CompressCriteria.threshold:
             return self._threshold_m_trunc(sigma)

@@ -148,7 +148,7 @@ template <int ESZ>
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                       const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, Epi epi,
-                      int num_k_tiles, int a_batched, int b_batched) {
+                      int num_k_tiles, int a_batched, int b_batched, int m_fast) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -158,7 +158,9 @@ __global__ void __launch_bounds__(THREADS, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int m_tile = blockIdx.y, n_tile = blockIdx.x, bz = blockIdx.z;
+  // m_fast: consecutive CTAs walk the M tiles of one N tile, so a large B
+  // operand streams from HBM once while the small A operand stays in L2
+  const int m_tile = m_fast ? blockIdx.x : blockIdx.y, n_tile = m_fast ? blockIdx.y : blockIdx.x, bz = blockIdx.z;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -322,6 +324,8 @@ struct PackArgs {
   void* lo;
   int64_t pitch;        // K' padded (elements)
   int64_t rows_out;     // rows per batch in the packed buffer
+  int64_t kused;        // K' actually written; [kused, pitch) is zeroed
+  int kblocks;          // blocks along K that copy data; the block column after them zeroes the padding
 };
 
 template <int ESZ>
@@ -343,14 +347,40 @@ __device__ __forceinline__ void split_store(void* hi, void* lo, int64_t idx, dou
   }
 }
 
+template <int ESZ>
+__device__ __forceinline__ void zero_store(void* hi, void* lo, int64_t idx) {
+  if constexpr (ESZ == 2) {
+    reinterpret_cast<__nv_bfloat16*>(hi)[idx] = __float2bfloat16(0.f);
+    reinterpret_cast<__nv_bfloat16*>(lo)[idx] = __float2bfloat16(0.f);
+  } else {
+    reinterpret_cast<float*>(hi)[idx] = 0.f;
+    reinterpret_cast<float*>(lo)[idx] = 0.f;
+  }
+}
+
 // one 32 x 32 (rows x K) source tile per block, staged through shared memory so
-// that both the strided FP64 reads and the K-contiguous packed writes coalesce
+// that both the strided FP64 reads and the K-contiguous packed writes coalesce;
+// the extra block column (blockIdx.x == kblocks) zeroes the K padding
+// [kused, pitch) of the packed rows of its 32 source rows
 template <int ESZ>
 __global__ void pack_kernel(PackArgs a) {
   __shared__ double2 tile[32][33];
   const int b = blockIdx.z;
   const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  if ((int)blockIdx.x >= a.kblocks) {
+    const int64_t base = (int64_t)b * a.rows_out * a.pitch;
+    const bool dbl = a.mode == P_DBL_CPLX || a.mode == P_DBL_SPLIT;
+    for (int i = ty; i < 32; i += 8) {
+      const int r = r0 + i;
+      if (r >= a.R) continue;
+      for (int rr = 0; rr < (dbl ? 2 : 1); ++rr) {
+        const int64_t row = base + (int64_t)(dbl ? 2 * r + rr : r) * a.pitch;
+        for (int64_t k = a.kused + tx; k < a.pitch; k += 32) zero_store<ESZ>(a.hi, a.lo, row + k);
+      }
+    }
+    return;
+  }
   const bool k_fast = (a.s_k == 1) || (a.s_r != 1);
   for (int i = ty; i < 32; i += 8) {
     const int r = k_fast ? r0 + i : r0 + tx;
@@ -403,23 +433,6 @@ __global__ void pack_kernel(PackArgs a) {
           split_store<ESZ>(a.hi, a.lo, r2 + a.pitch + k, v.y);
         }
         break;
-    }
-  }
-}
-
-// zero the K padding [kp_used, pitch) of every packed row
-template <int ESZ>
-__global__ void pad_kernel(void* hi, void* lo, int64_t rows, int64_t pitch, int64_t kused) {
-  const int64_t w = pitch - kused;
-  const int64_t total = rows * w;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = i / w, k = kused + i % w;
-    if constexpr (ESZ == 2) {
-      reinterpret_cast<__nv_bfloat16*>(hi)[r * pitch + k] = __float2bfloat16(0.f);
-      reinterpret_cast<__nv_bfloat16*>(lo)[r * pitch + k] = __float2bfloat16(0.f);
-    } else {
-      reinterpret_cast<float*>(hi)[r * pitch + k] = 0.f;
-      reinterpret_cast<float*>(lo)[r * pitch + k] = 0.f;
     }
   }
 }
@@ -534,16 +547,11 @@ static cudaError_t run_pack(const GemmOperand& op, int R, int K, int nb, int mod
   a.lo = lo;
   a.pitch = pitch;
   a.rows_out = rows_out;
-  dim3 grid((unsigned)ceil_div(K, 32), (unsigned)ceil_div(R, 32), (unsigned)nb);
+  a.kused = kused;
+  a.kblocks = (int)ceil_div(K, 32);
+  dim3 grid((unsigned)(a.kblocks + (pitch > kused ? 1 : 0)), (unsigned)ceil_div(R, 32), (unsigned)nb);
   count_launch();
   pack_kernel<ESZ><<<grid, dim3(32, 8), 0, st>>>(a);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || pitch == kused) return e;
-  const int64_t prow = rows_out * nb;
-  int64_t g = ceil_div(prow * (pitch - kused), 256);
-  if (g > 148 * 16) g = 148 * 16;
-  count_launch();
-  pad_kernel<ESZ><<<(unsigned)std::max<int64_t>(g, 1), 256, 0, st>>>(hi, lo, prow, pitch, kused);
   return cudaGetLastError();
 }
 
@@ -574,10 +582,13 @@ static cudaError_t run_split(const GemmParams& p, const Plan& q, char* ws, cudaS
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  dim3 grid((unsigned)ceil_div(q.rowsB, BN), (unsigned)ceil_div(q.rowsA, BM), (unsigned)p.batch);
+  const int64_t mt = ceil_div(q.rowsA, BM), nt = ceil_div(q.rowsB, BN);
+  // walk the smaller operand's tiles fastest (packed rows per batch decide)
+  const int m_fast = (q.rowsA <= q.rowsB && mt > 1 && nt <= 65535) ? 1 : 0;
+  dim3 grid((unsigned)(m_fast ? mt : nt), (unsigned)(m_fast ? nt : mt), (unsigned)p.batch);
   count_launch();
   split_gemm_kernel<ESZ><<<grid, THREADS, SMEM_BYTES, st>>>(tAh, tAl, tBh, tBl, epi, (int)(q.pitch / q.kstep),
-                                                            q.nbA > 1 ? 1 : 0, q.nbB > 1 ? 1 : 0);
+                                                            q.nbA > 1 ? 1 : 0, q.nbB > 1 ? 1 : 0, m_fast);
   return cudaGetLastError();
 }
 

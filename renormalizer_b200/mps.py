@@ -37,7 +37,7 @@ from .krylov import expm_krylov
 from .lib import Environ, contract_one_site
 from .model import Model, Op
 from .mpo import Mpo
-from .svd_qn import add_outer, get_qn_mask, qr_split, select_basis_indices, svd_truncate
+from .svd_qn import qn_sectors, add_outer, get_qn_mask, qr_split, select_basis_indices, svd_truncate
 
 logger = logging.getLogger(__name__)
 
@@ -96,7 +96,7 @@ class Mps:
         for imps in range(model.nsite - 1):
             qnbig = add_outer(qn[imps], model.basis[imps].sigmaqn).reshape(-1, qn_size)
             u_blocks, s_set, qnset = [], [], []
-            for iblock in set(tuple(t) for t in qnbig):
+            for iblock in qn_sectors(qnbig):
                 if np.all(np.array(qntot) < np.array(iblock)):
                     continue
                 indices = [i for i, x in enumerate(qnbig) if tuple(x) == iblock]
@@ -325,8 +325,11 @@ class Mps:
             self.qnidx = 0
             self.to_right = True
 
-    def _get_big_qn(self, cidx: List[int]):
-        """mp.py:308-352"""
+    def _get_big_qn(self, cidx: List[int], with_mat: bool = True):
+        """mp.py:308-352.  ``with_mat=False`` skips the (rows x cols x qn_size)
+        outer sum qnmat (None is returned in its place): the truncation only
+        needs the row and column labels, and at M = 256 with two 16-level
+        sites qnmat has 16.7 M entries per bond."""
         if len(cidx) == 2:
             cidx = sorted(cidx)
             assert cidx[0] + 1 == cidx[1]
@@ -341,7 +344,7 @@ class Mps:
                 qnbigl, qnbigr = qnl, add_outer(sig[0], qnr)
         else:
             qnbigl, qnbigr = add_outer(qnl, sig[0]), add_outer(sig[1], qnr)
-        return qnbigl, qnbigr, add_outer(qnbigl, qnbigr)
+        return qnbigl, qnbigr, (add_outer(qnbigl, qnbigr) if with_mat else None)
 
     @property
     def is_left_canonical(self):
@@ -399,7 +402,7 @@ class Mps:
     def _push_cano(self, idx):
         """mp.py:890-908 with _update_ms (245-295, sigma=None)"""
         mt = self._mp[idx]
-        qnbigl, qnbigr, _ = self._get_big_qn([idx])
+        qnbigl, qnbigr, _ = self._get_big_qn([idx], with_mat=False)
         system = "L" if self.to_right else "R"
         u, qnlset, vt, qnrset = qr_split(mt, qnbigl, qnbigr, self.qntot, system)
         m_trunc = u.shape[1]
@@ -437,7 +440,7 @@ class Mps:
             self.compress_config.set_bonddim(len(self) + 1)
         for idx in self.iter_idx_list(full=False):
             mt = self._mp[idx]
-            qnbigl, qnbigr, _ = self._get_big_qn([idx])
+            qnbigl, qnbigr, _ = self._get_big_qn([idx], with_mat=False)
             left = self.to_right
 
             def m_fn(sigma, idx=idx, left=left):
@@ -449,8 +452,14 @@ class Mps:
                     m = temp_m_trunc
                 return min(int(m), len(sigma))
 
+            if temp_m_trunc is None:
+                kcap = self.compress_config.fixed_cap(idx, left)
+            elif isinstance(temp_m_trunc, (list, tuple, np.ndarray)):
+                kcap = int(temp_m_trunc[idx + 1 if left else idx])
+            else:
+                kcap = int(temp_m_trunc)
             res = svd_truncate(mt, qnbigl, qnbigr, self.qntot, keep_left=left, m_trunc_fn=m_fn,
-                               full_matrices=False)
+                               full_matrices=False, kcap=kcap)
             pd = list(mt.shape[1:-1])
             if left:
                 self._absorb_right(idx, res.right)
@@ -474,7 +483,7 @@ class Mps:
         bond_site = cidx[0] if left else cidx[-1]
         res = svd_truncate(cstruct, qnbigl, qnbigr, self.qntot, keep_left=left,
                            m_trunc_fn=lambda s: self.compress_config.compute_m_trunc(s, bond_site, left),
-                           percent=percent)
+                           percent=percent, kcap=self.compress_config.fixed_cap(bond_site, left))
         ldims = list(qnbigl.shape[:-1])
         rdims = list(qnbigr.shape[:-1])
         lmat = res.left.reshape(ldims + [res.mdim])
@@ -703,7 +712,7 @@ class Mps:
                 mps_t, j = self._krylov(hop, -1j * evolve_dt / 2, mps[imps])
                 local_steps.append(j)
                 mps_t = mps_t.reshape(shape)
-                qnbigl, qnbigr, _ = mps._get_big_qn([imps])
+                qnbigl, qnbigr, _ = mps._get_big_qn([imps], with_mat=False)
                 u, qnlset, vt, qnrset = qr_split(mps_t, qnbigl, qnbigr, mps.qntot, system)
                 if not mps.to_right and imps != 0:
                     mps[imps] = vt.reshape([-1] + shape[1:])
@@ -756,7 +765,7 @@ class Mps:
                 mps_t, j = self._krylov(hop, -1j * evolve_dt / 2, ms2)
                 local_steps.append(j)
                 mps_t = mps_t.reshape(shape2)
-                qnbigl, qnbigr, _ = mps._get_big_qn([cidx0, cidx1])
+                qnbigl, qnbigr, _ = mps._get_big_qn([cidx0, cidx1], with_mat=False)
                 mps._update_mps(mps_t, [cidx0, cidx1], qnbigl, qnbigr)
                 if imps == last_idx:
                     continue

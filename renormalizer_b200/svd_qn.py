@@ -18,6 +18,7 @@ them.
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass
 from typing import List, Optional
 
@@ -32,6 +33,17 @@ def add_outer(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     assert a.shape[-1] == b.shape[-1]
     out = np.array([np.add.outer(a[..., i], b[..., i]) for i in range(a.shape[-1])])
     return out.transpose(list(range(1, out.ndim)) + [0])
+
+
+def qn_sectors(labels: np.ndarray) -> set:
+    """set(tuple(row) for row in labels) -- the reference's sector loop order
+    (svd_qn.py:183-184) -- built from the distinct rows in first-occurrence
+    order, which leaves the set, and so its iteration order, unchanged."""
+    labels = np.asarray(labels)
+    if labels.shape[0] == 0:
+        return set()
+    _, first = np.unique(labels, axis=0, return_index=True)
+    return set(tuple(int(v) for v in labels[i]) for i in np.sort(first))
 
 
 def get_qn_mask(qnmat: np.ndarray, qntot) -> np.ndarray:
@@ -89,7 +101,7 @@ def qn_block_svd(coef: torch.Tensor, qnbigl, qnbigr, qntot, full_matrices=True, 
     lq = qnbigl.reshape(-1, qs)
     rq = qnbigr.reshape(-1, qs)
     blocks: List[QNBlock] = []
-    for nl in set(tuple(t) for t in lq):
+    for nl in qn_sectors(lq):
         nr = tuple(qntot - np.array(nl))
         rset = np.where(get_qn_mask(rq, nr))[0]
         if len(rset) == 0:
@@ -126,7 +138,7 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
     lq = qnbigl.reshape(-1, qs)
     rq = qnbigr.reshape(-1, qs)
     blocks = []
-    for nl in set(tuple(t) for t in lq):
+    for nl in qn_sectors(lq):
         nr = tuple(qntot - np.array(nl))
         rset = np.where(get_qn_mask(rq, nr))[0]
         if len(rset) == 0:
@@ -212,8 +224,121 @@ class TruncatedSplit:
         self.sigma = sigma
 
 
+class SubspaceOptions:
+    """Top-k truncation of large QN blocks by block subspace iteration.
+
+    A block X whose smaller side has at least ``min_dim`` rows, when the
+    bond's cap k on the kept dimension is known (``fixed`` criteria), needs
+    only its leading k singular triplets: the selection takes at most k from
+    any one block and the fixed rule reads only min(k, len(sigma)).  They
+    come from ``iters`` + 1 products with X X^H (two FP64 GEMMs each,
+    Householder QR in between) on kk = k + oversample columns, a
+    Rayleigh-Ritz step on the kk x kk projection and the norms of the
+    projected rows.  Acceptance uses the excess discarded weight the Ritz
+    basis can carry, estimated from the residuals
+    r_i = ||X X^H u_i - lambda_i u_i|| of the leading k as
+    sum_i r_i^2 / max(lambda_i - lambda_kk, r_i): it must stay below
+    ``rtol`` * ||X||_F^2, otherwise the block falls back to the full Gram
+    eigendecomposition.  ``min_dim = 0`` disables the path.  Defaults can be
+    overridden by RENO_SUBSPACE="min_dim,iters,oversample,rtol"."""
+
+    def __init__(self, min_dim=1024, iters=3, oversample=64, rtol=1e-13):
+        env = os.environ.get("RENO_SUBSPACE")
+        if env:
+            a, b, c, d = env.split(",")
+            min_dim, iters, oversample, rtol = int(a), int(b), int(c), float(d)
+        self.min_dim = min_dim
+        self.iters = iters
+        self.oversample = oversample
+        self.rtol = rtol
+        self.calls = 0
+        self.fallbacks = 0
+
+
+subspace = SubspaceOptions()
+_OMEGA = {}
+
+
+def _omega(rows, kk, dtype, device):
+    """a fixed seeded Gaussian start block per shape (deterministic runs)"""
+    key = (rows, kk, dtype, str(device))
+    om = _OMEGA.get(key)
+    if om is None:
+        if len(_OMEGA) > 64:
+            _OMEGA.clear()
+        g = torch.Generator(device=device).manual_seed(0x5EED + 7919 * rows + kk)
+        om = torch.randn((rows, kk), dtype=torch.float64, device=device, generator=g)
+        if dtype.is_complex:
+            om = torch.complex(om, torch.randn((rows, kk), dtype=torch.float64, device=device, generator=g))
+        _OMEGA[key] = om
+    return om
+
+
+def _topk_kept_side(eng: Engine, A: torch.Tensor, k: int, opts: SubspaceOptions):
+    """Leading k left singular vectors of A (r x c, any 2-D view) by block
+    subspace iteration.  Returns K (r x k, descending), P = K^H A (k x c),
+    S (k, device: row norms of P) and a device pair (excess-weight estimate,
+    ||A||_F^2) for the acceptance test."""
+    r = A.shape[0]
+    kk = min(k + opts.oversample, r)
+    Q = _omega(r, kk, A.dtype, A.device)
+    for _ in range(opts.iters + 1):
+        Y = eng.matmul(A, eng.matmul(A.transpose(0, 1), Q, conj_a=True))
+        Q, _ = torch.linalg.qr(Y, mode="reduced")
+    B = eng.matmul(Q.transpose(0, 1), A, conj_a=True)          # kk x c
+    T = eng.matmul(B, B.transpose(0, 1), conj_b=True)          # kk x kk
+    w, W = torch.linalg.eigh(T)                                 # ascending
+    Wk = torch.flip(W[:, kk - k:], dims=[1])
+    lam = torch.flip(w[kk - k:], dims=[0])
+    K = eng.matmul(Q, Wk)                                       # r x k
+    P = eng.matmul(Wk.transpose(0, 1), B, conj_a=True)         # k x c
+    AP = eng.matmul(A, P.transpose(0, 1), conj_b=True)          # A A^H K
+    res = torch.linalg.vector_norm(AP - K * lam.to(K.dtype), dim=0)
+    gap = torch.maximum(lam - w[0], res)
+    excess = torch.sum(res * res / torch.clamp(gap, min=1e-300))
+    fro2 = torch.linalg.vector_norm(A) ** 2
+    S = torch.linalg.vector_norm(P, dim=1)
+    return K, P, S, torch.stack([excess, fro2])
+
+
+def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool) -> dict:
+    """Kept-side basis K, projection P and sigma S of one block from the full
+    Gram eigendecomposition of its smaller side (all min(m, n) triplets)."""
+    m, n = X.shape
+    dim = min(m, n)
+    if keep_left and m <= n:
+        G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
+        _, K = torch.linalg.eigh(G)
+        K = torch.flip(K, dims=[1])
+        P = eng.matmul(K[:, :dim].transpose(0, 1), X, conj_a=True)
+        S = torch.linalg.vector_norm(P, dim=1)
+    elif keep_left:
+        G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
+        _, V = torch.linalg.eigh(G)
+        V = torch.flip(V, dims=[1])
+        Us = eng.matmul(X, V)
+        S = torch.linalg.vector_norm(Us, dim=0)
+        K, _ = torch.linalg.qr(Us, mode="reduced")
+        P = eng.matmul(K.transpose(0, 1), X, conj_a=True)
+    elif n <= m:
+        G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
+        _, K = torch.linalg.eigh(G)
+        K = torch.flip(K, dims=[1])
+        P = eng.matmul(X, K[:, :dim])
+        S = torch.linalg.vector_norm(P, dim=0)
+    else:
+        G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
+        _, U = torch.linalg.eigh(G)
+        U = torch.flip(U, dims=[1])
+        Vs = eng.matmul(X.transpose(0, 1), U, conj_a=True)
+        S = torch.linalg.vector_norm(Vs, dim=0)
+        K, _ = torch.linalg.qr(Vs, mode="reduced")
+        P = eng.matmul(X, K)
+    return dict(K=K, P=P, S=S, dim=dim)
+
+
 def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_trunc_fn, percent=0,
-                 full_matrices=True):
+                 full_matrices=True, kcap: Optional[int] = None):
     """Fused svd_qn + compute_m_trunc + select_basis of mp.py:693-778.
 
     keep_left=True keeps U (left-to-right sweep: left = U, right = sigma Vh);
@@ -223,7 +348,13 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
     zero-sigma completion columns the reference appends with
     full_matrices=True (svd_qn.py:12-86).  The singular values used for
     ordering and truncation are the norms of the projected rows/columns
-    (||u_j^H X|| or ||X v_j||), which stay accurate far below sqrt(eps)."""
+    (||u_j^H X|| or ||X v_j||), which stay accurate far below sqrt(eps).
+
+    ``kcap`` (the bond's fixed cap on the kept dimension, None when the rule
+    is threshold-based) lets large blocks use the top-k subspace solver
+    (``subspace`` options); its residual norms come to the host with the
+    singular values and a block whose Ritz pairs miss the tolerance is redone
+    with the full decomposition."""
     eng = Engine.get(coef.device)
     rows = int(np.prod(qnbigl.shape[:-1]))
     cols = int(np.prod(qnbigr.shape[:-1]))
@@ -233,7 +364,7 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
     lq = qnbigl.reshape(-1, qs)
     rq = qnbigr.reshape(-1, qs)
     blocks = []
-    for nl in set(tuple(t) for t in lq):
+    for nl in qn_sectors(lq):
         nr = tuple(qntot - np.array(nl))
         rset = np.where(get_qn_mask(rq, nr))[0]
         if len(rset) == 0:
@@ -243,46 +374,41 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         m, n = X.shape
         dim = min(m, n)
         upad, vpad = _pad_counts(m, n, full_matrices)
-        if keep_left and m <= n:
-            # kept side is the small side: its Gram eigenbasis is the kept basis
-            G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-            _, K = torch.linalg.eigh(G)
-            K = torch.flip(K, dims=[1])                       # descending eigenvalues
-            P = eng.matmul(K[:, :dim].transpose(0, 1), X, conj_a=True)   # (dim, n) = sigma Vh
-            S = torch.linalg.vector_norm(P, dim=1)
-        elif keep_left:
-            # m > n: eigen-solve the small side, orthonormalise X v_j (QR keeps the
-            # column order) and project X onto it
-            G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-            _, V = torch.linalg.eigh(G)
-            V = torch.flip(V, dims=[1])
-            Us = eng.matmul(X, V)                              # (m, dim) = U sigma
-            S = torch.linalg.vector_norm(Us, dim=0)
-            K, _ = torch.linalg.qr(Us, mode="reduced")
-            P = eng.matmul(K.transpose(0, 1), X, conj_a=True)  # (dim, n)
-        elif n <= m:
-            G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-            _, K = torch.linalg.eigh(G)
-            K = torch.flip(K, dims=[1])
-            P = eng.matmul(X, K[:, :dim])                     # (m, dim) = U sigma
-            S = torch.linalg.vector_norm(P, dim=0)
-        else:
-            G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-            _, U = torch.linalg.eigh(G)
-            U = torch.flip(U, dims=[1])
-            Vs = eng.matmul(X.transpose(0, 1), U, conj_a=True)  # (n, dim): column j = sigma_j v_j
-            S = torch.linalg.vector_norm(Vs, dim=0)
-            K, _ = torch.linalg.qr(Vs, mode="reduced")
-            P = eng.matmul(X, K)                               # (m, dim)
+        ksub = min(kcap, dim) if kcap is not None else 0
+        if (subspace.min_dim and kcap is not None and dim >= subspace.min_dim
+                and dim >= 2 * (ksub + subspace.oversample)):
+            subspace.calls += 1
+            if keep_left:
+                K, P, S, res = _topk_kept_side(eng, X, ksub, subspace)
+            else:
+                K, Ph, S, res = _topk_kept_side(eng, X.transpose(0, 1).conj(), ksub, subspace)
+                P = Ph.transpose(0, 1).conj().resolve_conj()     # (m, k) = U sigma
+            npad = upad if keep_left else vpad
+            blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=ksub, npad=npad, res=res,
+                               X=X))
+            continue
+        full = _full_kept_side(eng, X, keep_left)
+        K, P, S = full["K"], full["P"], full["S"]
         npad = upad if keep_left else vpad
         blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=dim, npad=npad))
     if not blocks:
         raise ValueError("Invalid quantum number")
-    Sh = torch.cat([b["S"] for b in blocks]).cpu().numpy()
+    sub = [b for b in blocks if "res" in b]
+    host = torch.cat([b["S"] for b in blocks] + [b["res"] for b in sub]).cpu().numpy()
     off = 0
     for b in blocks:
-        b["Sh"] = Sh[off:off + b["dim"]]
+        b["Sh"] = host[off:off + b["dim"]]
         off += b["dim"]
+    for b in sub:
+        excess, fro2 = host[off], host[off + 1]
+        off += 2
+        if not (np.isfinite(excess) and excess <= subspace.rtol * fro2):
+            # Ritz pairs not converged to the tolerance: full decomposition of this block
+            subspace.fallbacks += 1
+            full = _full_kept_side(eng, b["X"], keep_left)
+            b.update(full)
+            b["Sh"] = b["S"].cpu().numpy()
+        b.pop("X", None)
     # the reference's concatenated order: nonzero parts block by block, then
     # the zero-sigma paddings block by block (svd_qn.py:222-230)
     sig, qns, where = [], [], []

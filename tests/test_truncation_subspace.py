@@ -1,0 +1,102 @@
+"""The top-k subspace path of svd_truncate against its full Gram
+eigendecomposition path on the same QN-blocked coefficient.
+
+Both keep the bond's cap k = kcap; with a decaying spectrum (ratio of the
+k-th to the (k + oversample)-th singular value well above one) the kept
+singular values must agree to 1e-12 relative to sigma_1, the truncated
+coefficients left @ right to 1e-10 relative to its norm, the QN labels and
+selection exactly, and the kept side must be orthonormal to 1e-12.  A zero
+residual tolerance forces the fallback, which must reproduce the full path
+bit for bit.  CPU cases run on the test stand-in engine with a lowered size
+threshold; the GPU case uses the workload's block size (2048 per QN sector,
+k = 256)."""
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+
+def _case(dev, nblk, decay, seed=3):
+    """two QN sectors of nblk x nblk each: rows/cols labelled 0/1 with qntot 1"""
+    g = torch.Generator(device=dev).manual_seed(seed)
+    n = 2 * nblk
+    ql = np.array([0] * nblk + [1] * nblk).reshape(n, 1)
+    qr = np.array([1] * nblk + [0] * nblk).reshape(n, 1)
+    coef = torch.zeros((n, n), dtype=torch.complex128, device=dev)
+    for b, sl in enumerate((slice(0, nblk), slice(nblk, n))):
+        X = torch.complex(torch.randn(nblk, nblk, dtype=torch.float64, device=dev, generator=g),
+                          torch.randn(nblk, nblk, dtype=torch.float64, device=dev, generator=g))
+        U, _ = torch.linalg.qr(X)
+        V, _ = torch.linalg.qr(X.mT)
+        s = torch.exp(-torch.arange(nblk, dtype=torch.float64, device=dev) / decay) * (1.0 + 0.5 * b)
+        coef[sl, sl] = (U * s) @ V.mH
+    # rows of sector 0 pair with columns of sector 0 (labels 0 + 1 = qntot)
+    return coef, ql, qr
+
+
+def _run(coef, ql, qr, keep_left, kcap, percent=0.0):
+    from renormalizer_b200.svd_qn import svd_truncate
+    return svd_truncate(coef, ql, qr, np.array([1]), keep_left, lambda s: min(kcap, len(s)), percent=percent,
+                        kcap=kcap)
+
+
+def _compare(coef, ql, qr, keep_left, kcap, percent=0.0):
+    svd_qn = importlib.import_module("renormalizer_b200.svd_qn")
+    saved = svd_qn.subspace.min_dim
+    try:
+        svd_qn.subspace.min_dim = 0
+        from renormalizer_b200.svd_qn import svd_truncate
+        full = svd_truncate(coef, ql, qr, np.array([1]), keep_left, lambda s: min(kcap, len(s)), percent=percent)
+    finally:
+        svd_qn.subspace.min_dim = saved
+    sub = _run(coef, ql, qr, keep_left, kcap, percent)
+    assert sub.mdim == full.mdim == kcap
+    np.testing.assert_array_equal(np.asarray(sub.qn), np.asarray(full.qn))
+    np.testing.assert_allclose(sub.sigma, full.sigma, rtol=0, atol=1e-12 * full.sigma.max())
+    a = (sub.left @ sub.right)
+    b = (full.left @ full.right)
+    assert float((a - b).abs().max() / b.abs().max()) < 1e-10
+    kept = sub.left if keep_left else sub.right.mH
+    eye = torch.eye(kcap, dtype=kept.dtype, device=kept.device)
+    assert float((kept.mH @ kept - eye).abs().max()) < 1e-12
+    return sub, full
+
+
+@pytest.mark.parametrize("keep_left", [True, False])
+def test_subspace_matches_full_path_cpu(cpu_engine, keep_left):
+    svd_qn = importlib.import_module("renormalizer_b200.svd_qn")
+    saved = (svd_qn.subspace.min_dim, svd_qn.subspace.oversample)
+    svd_qn.subspace.min_dim, svd_qn.subspace.oversample = 64, 16
+    c0, f0 = svd_qn.subspace.calls, svd_qn.subspace.fallbacks
+    try:
+        coef, ql, qr = _case("cpu", 160, 6.0)
+        _compare(coef, ql, qr, keep_left, 24)
+        _compare(coef, ql, qr, keep_left, 24, percent=0.4)
+        assert svd_qn.subspace.calls - c0 == 4 and svd_qn.subspace.fallbacks == f0
+    finally:
+        svd_qn.subspace.min_dim, svd_qn.subspace.oversample = saved
+
+
+def test_subspace_fallback_reproduces_full_path_cpu(cpu_engine):
+    svd_qn = importlib.import_module("renormalizer_b200.svd_qn")
+    saved = (svd_qn.subspace.min_dim, svd_qn.subspace.oversample, svd_qn.subspace.rtol)
+    svd_qn.subspace.min_dim, svd_qn.subspace.oversample, svd_qn.subspace.rtol = 64, 16, 0.0
+    f0 = svd_qn.subspace.fallbacks
+    try:
+        coef, ql, qr = _case("cpu", 160, 6.0)
+        sub, full = _compare(coef, ql, qr, True, 24)
+        assert svd_qn.subspace.fallbacks - f0 == 2
+        assert torch.equal(sub.left, full.left) and torch.equal(sub.right, full.right)
+    finally:
+        svd_qn.subspace.min_dim, svd_qn.subspace.oversample, svd_qn.subspace.rtol = saved
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("keep_left", [True, False])
+def test_subspace_matches_full_path_gpu(keep_left):
+    svd_qn = importlib.import_module("renormalizer_b200.svd_qn")
+    f0 = svd_qn.subspace.fallbacks
+    coef, ql, qr = _case("cuda", 2048, 45.0)
+    _compare(coef, ql, qr, keep_left, 256)
+    assert svd_qn.subspace.fallbacks == f0
