@@ -59,6 +59,11 @@ def parse():
     ap.add_argument("--dt", type=float, default=0.025)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
+                    help="run STEPS steps with --prec and with plain FP64 from the same start and report the "
+                         "largest site-population difference after every step (no timing)")
+    ap.add_argument("--truncation", default="subspace", choices=["subspace", "exact"],
+                    help="exact: every QN block uses the full Gram eigendecomposition")
     ap.add_argument("--heff-only", action="store_true",
                     help="time only the workload's largest 2-site H_eff matvec (phonon-phonon block, M x 16 x 16 x M)")
     return ap.parse_args()
@@ -369,7 +374,7 @@ def run_engine(args, rank, world, dist):
     l0 = launch_count()
     import importlib
     svdmod = importlib.import_module("renormalizer_b200.svd_qn")
-    sub0 = (svdmod.subspace.calls, svdmod.subspace.fallbacks)
+    sub0 = (svdmod.subspace.calls, svdmod.subspace.fallbacks, svdmod.subspace.retries)
     with ClockSampler(local) as clocks:
         s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s_ev.record()
@@ -378,7 +383,8 @@ def run_engine(args, rank, world, dist):
         e_ev.record()
         barrier()
     launches = launch_count() - l0
-    trunc = {"subspace_blocks": svdmod.subspace.calls - sub0[0], "fallbacks": svdmod.subspace.fallbacks - sub0[1],
+    trunc = {"subspace_blocks": svdmod.subspace.calls - sub0[0], "retries": svdmod.subspace.retries - sub0[2],
+             "fallbacks": svdmod.subspace.fallbacks - sub0[1],
              "options": {"min_dim": svdmod.subspace.min_dim, "iters": svdmod.subspace.iters,
                          "oversample": svdmod.subspace.oversample, "rtol": svdmod.subspace.rtol}}
     timer.uninstall()
@@ -511,8 +517,37 @@ def run_heff_only(args):
                       "gpu_launches_per_matvec": (launch_count() - l0) / args.steps}))
 
 
+def run_accuracy(args):
+    """|population(prec) - population(FP64)| over --accuracy steps."""
+    import torch
+    from renormalizer_b200 import Mpo, backend
+    torch.cuda.set_device(0)
+    model = holstein_2mode(args.nmol, args.nlev)
+    mpo = Mpo(model)
+    mps0 = initial_state(model, args.M)
+    a, b = mps0, mps0
+    dev = []
+    for step in range(args.accuracy):
+        backend.prec = args.prec
+        a = a.evolve(mpo, args.dt)
+        backend.prec = "fp64"
+        b = b.evolve(mpo, args.dt)
+        dev.append(float(np.abs(a.e_occupations - b.e_occupations).max()))
+        print(json.dumps({"step": step + 1, "max_abs_dpop": dev[-1]}), flush=True)
+    print(json.dumps({"metric": f"max |population({args.prec}) - population(fp64)| per step",
+                      "workload": WORKLOAD, "M": args.M, "nmol": args.nmol, "dt": args.dt,
+                      "truncation": args.truncation, "steps": args.accuracy, "per_step": dev,
+                      "max": max(dev) if dev else None}), flush=True)
+
+
 def main():
     args = parse()
+    if args.truncation == "exact":
+        import importlib
+        importlib.import_module("renormalizer_b200.svd_qn").subspace.min_dim = 0
+    if args.accuracy:
+        run_accuracy(args)
+        return
     if args.heff_only:
         run_heff_only(args)
         return

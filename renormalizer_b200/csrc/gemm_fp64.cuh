@@ -20,6 +20,7 @@ struct GemmOperand {
   int64_t s_batch = 0;
   int is_complex = 0;
   int conj = 0;
+  int is_f32 = 0;       // elements are float / float2 (split-precision intermediates only)
 };
 
 struct GemmParams {
@@ -28,6 +29,7 @@ struct GemmParams {
   void* C = nullptr;
   int64_t sCm = 0, sCn = 0, sCb = 0;
   int accumulate = 0;
+  int c_f32 = 0;        // C is float / float2 (split-precision intermediates only)
 };
 
 namespace fp64gemm {
@@ -232,6 +234,8 @@ inline cudaError_t launch_t(const GemmParams& p, cudaStream_t st) {
 // Launch the FP64 GEMM; returns a CUDA error code.
 inline cudaError_t gemm_fp64(const GemmParams& p, cudaStream_t st) {
   if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return cudaSuccess;
+  // FP32 operands / outputs exist only between split-precision stages
+  if (p.A.is_f32 || p.B.is_f32 || p.c_f32) return cudaErrorInvalidValue;
   const bool ac = p.A.is_complex, bc = p.B.is_complex;
   if (ac && bc) return fp64gemm::launch_t<true, true>(p, st);
   if (ac) return fp64gemm::launch_t<true, false>(p, st);

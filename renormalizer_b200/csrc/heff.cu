@@ -82,7 +82,8 @@ static cudaError_t launch_swap13(const void* in, void* out, int dt, int n0, int 
   return cudaGetLastError();
 }
 
-static GemmOperand opnd(const void* p, int dt, int64_t s_outer, int64_t s_k, int64_t s_b = 0, int conj = 0) {
+static GemmOperand opnd(const void* p, int dt, int64_t s_outer, int64_t s_k, int64_t s_b = 0, int conj = 0,
+                        int f32 = 0) {
   GemmOperand o;
   o.ptr = p;
   o.is_complex = dt == RENO_C128;
@@ -90,7 +91,18 @@ static GemmOperand opnd(const void* p, int dt, int64_t s_outer, int64_t s_k, int
   o.s_k = s_k;
   o.s_batch = s_b;
   o.conj = conj;
+  o.is_f32 = f32;
   return o;
+}
+
+// an intermediate operand: FP32 storage between split-precision stages
+static GemmOperand iopnd(const void* p, int dt, int f32, int64_t s_outer, int64_t s_k, int64_t s_b = 0) {
+  return opnd(p, dt, s_outer, s_k, s_b, 0, f32);
+}
+
+static GemmParams to_f32(GemmParams p, int f32) {
+  p.c_f32 = f32;
+  return p;
 }
 
 static GemmParams gp(int M, int N, int K, int batch, GemmOperand A, GemmOperand B, void* C, int64_t sCm,
@@ -127,8 +139,10 @@ static size_t split_need(const std::vector<Stage>& stages) {
 }
 
 // ---------------------------------------------------------------- heff
+// Intermediates (T1, T2, T3) are FP64 on the FP64 path and FP32 between
+// split-precision stages, whose tensor-core accumulators are FP32 anyway.
 struct HeffLayout {
-  int dt_T1, dt_T2, dt_y;
+  int dt_T1, dt_T2, dt_y, t32;
   size_t off_wt1, off_wt2, off_t1, off_t2, off_split;
 };
 
@@ -151,6 +165,7 @@ static HeffLayout heff_layout(const reno_heff_desc* d) {
   p.dt_T1 = promote(d->env_dtype, d->psi_dtype);
   p.dt_T2 = d->nsite == 0 ? p.dt_T1 : promote(p.dt_T1, d->mpo_dtype);
   p.dt_y = promote(p.dt_T2, d->env_dtype);
+  p.t32 = d->prec != RENO_PREC_FP64;
   int64_t n_wt1 = 0, n_wt2 = 0, n_t1 = 0, n_t2 = 0;
   if (d->nsite == 0) {
     n_t1 = ml * wl * mr;
@@ -169,10 +184,11 @@ static HeffLayout heff_layout(const reno_heff_desc* d) {
   off = align256(off + n_wt1 * esz(d->mpo_dtype));
   p.off_wt2 = off;
   off = align256(off + n_wt2 * esz(d->mpo_dtype));
+  const int64_t tsz = esz(p.dt_T2) / (p.t32 ? 2 : 1);
   p.off_t1 = off;
-  off = align256(off + n_t1 * esz(p.dt_T2));
+  off = align256(off + n_t1 * tsz);
   p.off_t2 = off;
-  off = align256(off + n_t2 * esz(p.dt_T2));
+  off = align256(off + n_t2 * tsz);
   p.off_split = off;
   return p;
 }
@@ -186,34 +202,149 @@ static std::vector<Stage> heff_stages(const reno_heff_desc* d, const HeffLayout&
   void* Wt2 = w + lay.off_wt2;
   void* T1 = w + lay.off_t1;
   void* T2 = w + lay.off_t2;
+  const int f = lay.t32;
   std::vector<Stage> s;
   if (d->nsite == 0) {
-    s.push_back({gp(ml * wl, mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, mr), T1, mr, 1), pr});
-    s.push_back({gp(ml, mr, wl * mr, 1, opnd(T1, lay.dt_T1, wl * mr, 1), opnd(R, ev, wl * mr, 1), y, mr, 1), pr});
+    s.push_back({to_f32(gp(ml * wl, mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, mr), T1, mr, 1), f), pr});
+    s.push_back({gp(ml, mr, wl * mr, 1, iopnd(T1, lay.dt_T1, f, wl * mr, 1), opnd(R, ev, wl * mr, 1), y, mr, 1), pr});
   } else if (d->nsite == 1) {
-    s.push_back({gp(ml * wl, d1 * mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, d1 * mr), T1, d1 * mr, 1), pr});
-    s.push_back({gp(d1 * wr, mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1), opnd(T1, lay.dt_T1, 1, mr, wl * d1 * mr), T2,
-                    mr, 1, d1 * wr * mr),
+    s.push_back(
+        {to_f32(gp(ml * wl, d1 * mr, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, d1 * mr), T1, d1 * mr, 1), f), pr});
+    s.push_back({to_f32(gp(d1 * wr, mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1),
+                           iopnd(T1, lay.dt_T1, f, 1, mr, wl * d1 * mr), T2, mr, 1, d1 * wr * mr),
+                        f),
                  pr});
-    s.push_back({gp(ml * d1, mr, wr * mr, 1, opnd(T2, lay.dt_T2, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1), pr});
+    s.push_back(
+        {gp(ml * d1, mr, wr * mr, 1, iopnd(T2, lay.dt_T2, f, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1), pr});
   } else {
     const int64_t n12 = d1 * d2 * mr;
     void* T3 = T1;
-    s.push_back({gp(ml * wl, n12, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, n12), T1, n12, 1), pr});
-    s.push_back({gp(d1 * wm, d2 * mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1),
-                    opnd(T1, lay.dt_T1, 1, d2 * mr, wl * d1 * d2 * mr), T2, d2 * mr, 1, d1 * wm * d2 * mr),
+    s.push_back({to_f32(gp(ml * wl, n12, ml, 1, opnd(L, ev, ml, 1), opnd(psi, pv, 1, n12), T1, n12, 1), f), pr});
+    s.push_back({to_f32(gp(d1 * wm, d2 * mr, wl * d1, ml, opnd(Wt1, mv, wl * d1, 1),
+                           iopnd(T1, lay.dt_T1, f, 1, d2 * mr, wl * d1 * d2 * mr), T2, d2 * mr, 1, d1 * wm * d2 * mr),
+                        f),
                  pr});
-    s.push_back({gp(d2 * wr, mr, wm * d2, ml * d1, opnd(Wt2, mv, wm * d2, 1), opnd(T2, lay.dt_T2, 1, mr, wm * d2 * mr),
-                    T3, mr, 1, d2 * wr * mr),
+    s.push_back({to_f32(gp(d2 * wr, mr, wm * d2, ml * d1, opnd(Wt2, mv, wm * d2, 1),
+                           iopnd(T2, lay.dt_T2, f, 1, mr, wm * d2 * mr), T3, mr, 1, d2 * wr * mr),
+                        f),
                  pr});
-    s.push_back({gp(ml * d1 * d2, mr, wr * mr, 1, opnd(T3, lay.dt_T2, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1),
+    s.push_back({gp(ml * d1 * d2, mr, wr * mr, 1, iopnd(T3, lay.dt_T2, f, wr * mr, 1), opnd(R, ev, wr * mr, 1), y, mr, 1),
                  pr});
   }
   return s;
 }
 
+// ---------------------------------------------------------------- fused split 2-site matvec
+// The four stages of the 2-site matvec with every intermediate written by the
+// producing GEMM's epilogue straight into the consumer's packed hi/lo operand
+// (no FP64/FP32 intermediate, no separate pack pass):
+//   S1  T1 = L . psi      N order (k, h, e): e runs along the consumer's K
+//   S2  T2 = Wt1 . T1[a]  written as S3's B, N order (k, h): h along K
+//   S3  T3 = Wt2 . T2[ad] written as S4's A ([re | im] along K = (w, k))
+//   S4  y  = T3 . R^T     FP64 output
+// Used for complex L, R, psi with a real MPO (TDVP) and for all-real
+// operands (DMRG); other combinations take the staged path.
+struct Fused2 {
+  SplitPacked s1a, s1b, s2a, s2b, s3a, s3b, s4a, s4b;
+  size_t bytes;
+};
+
+static bool fused2_eligible(const reno_heff_desc* d) {
+  if (d->nsite != 2 || d->prec == RENO_PREC_FP64 || d->mpo_dtype != RENO_F64) return false;
+  const bool allc = d->env_dtype == RENO_C128 && d->psi_dtype == RENO_C128;
+  const bool allr = d->env_dtype == RENO_F64 && d->psi_dtype == RENO_F64;
+  // grid.z of S2 / S3 is the batch (ml, ml * d1)
+  return (allc || allr) && (int64_t)d->ml * d->d1 <= 65535;
+}
+
+static Fused2 fused2_layout(const reno_heff_desc* d, char* base) {
+  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wm = d->wm, wr = d->wr, d1 = d->d1, d2 = d->d2;
+  const bool c = d->env_dtype == RENO_C128;
+  const int pr = d->prec;
+  const int64_t x2 = c ? 2 : 1;
+  // (rows, kext, nb, mode) of each packed operand
+  struct Spec { int64_t rows, kext, nb; int mode; };
+  const Spec s1a{x2 * ml * wl, x2 * ml, 1, c ? SPLIT_DBL_CPLX : SPLIT_REAL};
+  const Spec s1b{d1 * d2 * mr, x2 * ml, 1, c ? SPLIT_CAT : SPLIT_REAL};
+  const Spec s2a{d1 * wm, wl * d1, 1, SPLIT_REAL};
+  const Spec s2b{x2 * d2 * mr, wl * d1, ml, c ? SPLIT_DBL_SPLIT : SPLIT_REAL};
+  const Spec s3a{d2 * wr, wm * d2, 1, SPLIT_REAL};
+  const Spec s3b{x2 * mr, wm * d2, ml * d1, c ? SPLIT_DBL_SPLIT : SPLIT_REAL};
+  const Spec s4a{ml * d1 * d2, x2 * wr * mr, 1, c ? SPLIT_CAT : SPLIT_REAL};
+  const Spec s4b{x2 * mr, x2 * wr * mr, 1, c ? SPLIT_DBL_CPLX : SPLIT_REAL};
+  auto sz = [&](const Spec& q) { return split_packed_bytes(q.rows, q.kext, q.nb, pr); };
+  auto at = [&](size_t off, const Spec& q) {
+    return split_packed_at(base ? base + off : nullptr, q.rows, q.kext, q.nb, q.mode, pr);
+  };
+  Fused2 f{};
+  size_t off = 0;
+  f.s1a = at(off, s1a);
+  off = align256(off + sz(s1a));
+  f.s2a = at(off, s2a);
+  off = align256(off + sz(s2a));
+  f.s3a = at(off, s3a);
+  off = align256(off + sz(s3a));
+  f.s4b = at(off, s4b);
+  off = align256(off + sz(s4b));
+  // region P: psi packed (S1's B), later S3's B; region Q: S2's B, later S4's A
+  const size_t P = off;
+  off = align256(off + std::max(sz(s1b), sz(s3b)));
+  const size_t Q = off;
+  off = align256(off + std::max(sz(s2b), sz(s4a)));
+  f.s1b = at(P, s1b);
+  f.s3b = at(P, s3b);
+  f.s2b = at(Q, s2b);
+  f.s4a = at(Q, s4a);
+  f.bytes = off;
+  return f;
+}
+
+static cudaError_t fused2_run(const reno_heff_desc* d, const Fused2& f, const void* L, const void* Wt1,
+                              const void* Wt2, const void* R, const void* psi, void* y, cudaStream_t st) {
+  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wm = d->wm, wr = d->wr, d1 = d->d1, d2 = d->d2;
+  const int ev = d->env_dtype, pv = d->psi_dtype, pr = d->prec;
+  const bool c = ev == RENO_C128;
+  const int64_t x2 = c ? 2 : 1;
+  cudaError_t e = split_pack(opnd(L, ev, ml, 1), (int)(ml * wl), (int)ml, 1, SplitRows{}, f.s1a, pr, st);
+  // psi rows in (k, h, e) order: e at stride d2*mr, h at mr, k at 1; K = c at d1*d2*mr
+  SplitRows khe;
+  khe.D0 = (int)d1;
+  khe.D1 = (int)d2;
+  khe.s_r1 = mr;
+  khe.s_r2 = 1;
+  if (e == cudaSuccess)
+    e = split_pack(opnd(psi, pv, d2 * mr, d1 * d2 * mr), (int)(d1 * d2 * mr), (int)ml, 1, khe, f.s1b, pr, st);
+  if (e == cudaSuccess)
+    e = split_pack(opnd(Wt1, RENO_F64, wl * d1, 1), (int)(d1 * wm), (int)(wl * d1), 1, SplitRows{}, f.s2a, pr, st);
+  if (e == cudaSuccess)
+    e = split_pack(opnd(Wt2, RENO_F64, wm * d2, 1), (int)(d2 * wr), (int)(wm * d2), 1, SplitRows{}, f.s3a, pr, st);
+  if (e == cudaSuccess)
+    e = split_pack(opnd(R, ev, wr * mr, 1), (int)mr, (int)(wr * mr), 1, SplitRows{}, f.s4b, pr, st);
+  if (e != cudaSuccess) return e;
+  // S1: rows (a, b) of L, columns (k, h, e) -> S2's B[a][(k, h) re/im][(b, e)]
+  SplitPackOut o1{f.s2b.hi, f.s2b.lo, 0, f.s2b.rows * f.s2b.pitch, d1, x2 * f.s2b.pitch, 1, f.s2b.pitch,
+                  (int)wl, (int)d1};
+  e = split_run(f.s1a, f.s1b, (int)(ml * wl), (int)(d1 * d2 * mr), 1, nullptr, &o1, pr, st);
+  // S2 (batch a): rows (d', w), columns (k, h) -> S3's B[(a, d')][k re/im][(w, h)]
+  SplitPackOut o2{f.s3b.hi, f.s3b.lo, d1 * f.s3b.rows * f.s3b.pitch, f.s3b.rows * f.s3b.pitch, d2,
+                  x2 * f.s3b.pitch, 1, f.s3b.pitch, (int)wm, (int)d2};
+  if (e == cudaSuccess) e = split_run(f.s2a, f.s2b, (int)(d1 * wm), (int)(d2 * mr), (int)ml, nullptr, &o2, pr, st);
+  // S3 (batch (a, d')): rows (h', w2), columns k -> S4's A[(a, d', h')][re/im | (w2, k)]
+  SplitPackOut o3{f.s4a.hi, f.s4a.lo, d2 * f.s4a.pitch, f.s4a.pitch, mr, 0, 1, wr * mr, (int)wr, (int)mr};
+  if (e == cudaSuccess) e = split_run(f.s3a, f.s3b, (int)(d2 * wr), (int)mr, (int)(ml * d1), nullptr, &o3, pr, st);
+  // S4: y[(a, d', h'), l] = T3 . R^T
+  GemmParams out;
+  out.C = y;
+  out.sCm = mr;
+  out.sCn = 1;
+  if (e == cudaSuccess) e = split_run(f.s4a, f.s4b, (int)(ml * d1 * d2), (int)mr, 1, &out, nullptr, pr, st);
+  (void)x2;
+  return e;
+}
+
 static size_t heff_total(const reno_heff_desc* d) {
   const HeffLayout lay = heff_layout(d);
+  if (fused2_eligible(d)) return lay.off_t1 + fused2_layout(d, nullptr).bytes;
   char* nul = nullptr;
   return lay.off_split + align256(split_need(heff_stages(d, lay, nul, nullptr, nullptr, nullptr, nullptr)));
 }
@@ -237,6 +368,16 @@ extern "C" int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* d, const voi
     return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply: null tensor pointer");
   const HeffLayout lay = heff_layout(d);
   char* w = static_cast<char*>(ws);
+  if (fused2_eligible(d)) {
+    const Fused2 f = fused2_layout(d, w ? w + lay.off_t1 : nullptr);
+    if (ws_bytes < lay.off_t1 + f.bytes || !ws)
+      return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heff_apply: workspace too small");
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = launch_wt(W1, w + lay.off_wt1, d->mpo_dtype, d->wl, d->d1, d->wm, 0, st);
+    if (e == cudaSuccess) e = launch_wt(W2, w + lay.off_wt2, d->mpo_dtype, d->wm, d->d2, d->wr, 0, st);
+    if (e == cudaSuccess) e = fused2_run(d, f, L, w + lay.off_wt1, w + lay.off_wt2, R, psi, y, st);
+    return check_cuda(ctx, e, "reno_heff_apply");
+  }
   const std::vector<Stage> stages = heff_stages(d, lay, w, L, R, psi, y);
   const size_t need_split = split_need(stages);
   if (ws_bytes < lay.off_split + need_split || !ws)
@@ -258,7 +399,7 @@ extern "C" int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* d, const voi
 // ---------------------------------------------------------------- env update
 namespace reno {
 struct EnvLayout {
-  int dt_T1, dt_T2, dt_out;
+  int dt_T1, dt_T2, dt_out, t32;
   size_t off_ketT, off_braT, off_wt, off_t1, off_t2, off_split;
 };
 
@@ -281,6 +422,8 @@ static EnvLayout env_layout(const reno_env_desc* d) {
   p.dt_T1 = promote(d->env_dtype, d->ket_dtype);
   p.dt_T2 = promote(p.dt_T1, d->mpo_dtype);
   p.dt_out = promote(p.dt_T2, d->bra_dtype);
+  p.t32 = d->prec != RENO_PREC_FP64;
+  const int64_t div = p.t32 ? 2 : 1;
   size_t off = 0;
   p.off_ketT = off;
   if (d->side == 1) off = align256(off + ki * dd * ko * esz(d->ket_dtype));
@@ -289,9 +432,9 @@ static EnvLayout env_layout(const reno_env_desc* d) {
   p.off_wt = off;
   off = align256(off + dd * wo * wi * dd * esz(d->mpo_dtype));
   p.off_t1 = off;
-  off = align256(off + bi * wi * dd * ko * esz(p.dt_T1));
+  off = align256(off + bi * wi * dd * ko * esz(p.dt_T1) / div);
   p.off_t2 = off;
-  off = align256(off + bi * dd * wo * ko * esz(p.dt_T2));
+  off = align256(off + bi * dd * wo * ko * esz(p.dt_T2) / div);
   p.off_split = off;
   return p;
 }
@@ -304,16 +447,18 @@ static std::vector<Stage> env_stages(const reno_env_desc* d, const EnvLayout& la
   void* Wt = w + lay.off_wt;
   void* T1 = w + lay.off_t1;
   void* T2 = w + lay.off_t2;
-  const int pr = d->prec;
+  const int pr = d->prec, f = lay.t32;
   std::vector<Stage> s;
-  s.push_back({gp(bi * wi, dd * ko, ki, 1, opnd(E, d->env_dtype, ki, 1), opnd(k_op, d->ket_dtype, 1, dd * ko), T1,
-                  dd * ko, 1),
+  s.push_back({to_f32(gp(bi * wi, dd * ko, ki, 1, opnd(E, d->env_dtype, ki, 1), opnd(k_op, d->ket_dtype, 1, dd * ko),
+                         T1, dd * ko, 1),
+                      f),
                pr});
-  s.push_back({gp(dd * wo, ko, wi * dd, bi, opnd(Wt, d->mpo_dtype, wi * dd, 1), opnd(T1, lay.dt_T1, 1, ko, wi * dd * ko),
-                  T2, ko, 1, dd * wo * ko),
+  s.push_back({to_f32(gp(dd * wo, ko, wi * dd, bi, opnd(Wt, d->mpo_dtype, wi * dd, 1),
+                         iopnd(T1, lay.dt_T1, f, 1, ko, wi * dd * ko), T2, ko, 1, dd * wo * ko),
+                      f),
                pr});
-  s.push_back({gp(bo, wo * ko, bi * dd, 1, opnd(b_op, bra_dt, 1, bo, 0, conj_bra), opnd(T2, lay.dt_T2, 1, wo * ko), out,
-                  wo * ko, 1),
+  s.push_back({gp(bo, wo * ko, bi * dd, 1, opnd(b_op, bra_dt, 1, bo, 0, conj_bra), iopnd(T2, lay.dt_T2, f, 1, wo * ko),
+                  out, wo * ko, 1),
                pr});
   return s;
 }

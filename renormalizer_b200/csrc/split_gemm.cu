@@ -1,7 +1,7 @@
 // Split-precision complex GEMM on the 5th-generation tensor cores (sm_100a).
 //
-// C (FP64, real or complex) = opA(A) opB(B) with A, B FP64 (real or complex,
-// any strides), computed as
+// C (real or complex) = opA(A) opB(B) with A, B real or complex with any
+// strides, computed as
 //     A ~ A_hi + A_lo,  B ~ B_hi + B_lo    (BF16 or TF32 pairs)
 //     C ~ A_hi B_hi + A_hi B_lo + A_lo B_hi   (FP32 accumulation in TMEM)
 // Complex operands use the real embedding: the smaller operand is "doubled"
@@ -14,8 +14,11 @@
 //              128-byte swizzled K-major boxes, mbarrier complete_tx
 //   warp 1     TMEM allocator + single-thread tcgen05.mma issuer: 3 products
 //              per stage, tcgen05.commit frees the stage
-//   warps 2-5  epilogue: tcgen05.ld 32x32b from TMEM, FP32 -> FP64, strided
-//              writes of the (interleaved complex) output
+//   warps 2-5  epilogue: tcgen05.ld 32x32b from TMEM, strided writes of the
+//              (interleaved complex) output as FP64, or as FP32 when the
+//              output only feeds the next split stage (the accumulator is
+//              FP32, so nothing is lost) -- the operands A, B are FP64 or
+//              such FP32 intermediates
 // Every mbarrier wait is bounded; on timeout the kernel records the site in
 // a device error word, skips the remaining work and still frees its TMEM.
 #include <cuda.h>
@@ -38,7 +41,7 @@ constexpr uint64_t WAIT_NS = 2000000000ull;  // bounded spin: 2 s of wall clock
 // device error word: 0 = ok; otherwise 1000 + site of the first timed-out wait
 __device__ int g_split_error = 0;
 
-enum OutMode { OUT_REAL = 0, OUT_COLS_CPLX = 1, OUT_ROWS_CPLX = 2 };
+enum OutMode { OUT_REAL = 0, OUT_COLS_CPLX = 1, OUT_ROWS_CPLX = 2, OUT_PACK = 3 };
 
 struct Epi {
   void* C;
@@ -47,7 +50,104 @@ struct Epi {
   int mode;
   int accumulate;
   int rows_p, cols_p;     // rows / cols of the real product C' actually present
+  int c_f32;              // C holds float (complex: float2) instead of double
+  // OUT_PACK: the tile is written as the next split stage's packed operand.
+  // Output element (m, n, ri) of the real product (ri: re/im component, from
+  // the row interleave when A was doubled, inter = 1, or the column interleave
+  // when B was doubled, inter = 2) goes to hi/lo element
+  //   bz*s_b + (m / Dm)*s_m1 + (m % Dm)*s_m0 + (n / Dn)*s_n1 + (n % Dn)*s_n0 + ri*s_ri
+  void* phi;
+  void* plo;
+  int64_t s_b, s_m1, s_m0, s_n1, s_n0, s_ri;
+  int Dm, Dn, inter;
 };
+
+template <typename T>
+__device__ __forceinline__ void st_real(void* C, int64_t i, float v, int acc) {
+  T* p = reinterpret_cast<T*>(C) + i;
+  *p = (acc ? *p : T(0)) + (T)v;
+}
+
+template <typename T2>
+__device__ __forceinline__ void st_cplx(void* C, int64_t i, float re, float im, int acc) {
+  T2* p = reinterpret_cast<T2*>(C) + i;
+  T2 o = acc ? *p : T2{0, 0};
+  o.x += re;
+  o.y += im;
+  *p = o;
+}
+
+// x = hi + lo in the split format: bits of hi and lo (BF16 in the low 16 bits, or TF32)
+template <int ESZ>
+__device__ __forceinline__ void split_bits(float x, uint32_t& hb, uint32_t& lb) {
+  if constexpr (ESZ == 2) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+    hb = __bfloat16_as_ushort(h);
+    lb = __bfloat16_as_ushort(l);
+  } else {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(x));
+    const float rem = x - __uint_as_float(hb);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lb) : "f"(rem));
+  }
+}
+
+template <int ESZ>
+__device__ __forceinline__ void split_store_bits(void* hi, void* lo, int64_t idx, uint32_t hb, uint32_t lb) {
+  if constexpr (ESZ == 2) {
+    reinterpret_cast<unsigned short*>(hi)[idx] = (unsigned short)hb;
+    reinterpret_cast<unsigned short*>(lo)[idx] = (unsigned short)lb;
+  } else {
+    reinterpret_cast<uint32_t*>(hi)[idx] = hb;
+    reinterpret_cast<uint32_t*>(lo)[idx] = lb;
+  }
+}
+
+// 16 output values v[t*STRIDE + OFF] (t = 0..15) of one (m, ri) for columns
+// n0 .. n0+15 into the packed planes: one 32-byte (BF16) or 64-byte (TF32)
+// vector store per plane when the run is contiguous and aligned, scalar
+// stores otherwise
+template <int ESZ, int STRIDE, int OFF>
+__device__ __forceinline__ void pack_run(const float* v, const Epi& e, int64_t mbase, int n0, int ri) {
+  const int64_t rbase = mbase + (int64_t)ri * e.s_ri;
+  const int64_t idx0 = rbase + (int64_t)(n0 / e.Dn) * e.s_n1 + (int64_t)(n0 % e.Dn) * e.s_n0;
+  const bool vec = e.s_n0 == 1 && n0 + 16 <= e.N && (n0 % e.Dn) + 16 <= e.Dn && (idx0 % (16 / ESZ)) == 0;
+  if (vec) {
+    uint32_t hb[16], lb[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) split_bits<ESZ>(v[t * STRIDE + OFF], hb[t], lb[t]);
+    if constexpr (ESZ == 2) {
+      uint4* ph = reinterpret_cast<uint4*>(reinterpret_cast<unsigned short*>(e.phi) + idx0);
+      uint4* pl = reinterpret_cast<uint4*>(reinterpret_cast<unsigned short*>(e.plo) + idx0);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        ph[q] = make_uint4(hb[8 * q] | (hb[8 * q + 1] << 16), hb[8 * q + 2] | (hb[8 * q + 3] << 16),
+                           hb[8 * q + 4] | (hb[8 * q + 5] << 16), hb[8 * q + 6] | (hb[8 * q + 7] << 16));
+        pl[q] = make_uint4(lb[8 * q] | (lb[8 * q + 1] << 16), lb[8 * q + 2] | (lb[8 * q + 3] << 16),
+                           lb[8 * q + 4] | (lb[8 * q + 5] << 16), lb[8 * q + 6] | (lb[8 * q + 7] << 16));
+      }
+    } else {
+      uint4* ph = reinterpret_cast<uint4*>(reinterpret_cast<uint32_t*>(e.phi) + idx0);
+      uint4* pl = reinterpret_cast<uint4*>(reinterpret_cast<uint32_t*>(e.plo) + idx0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        ph[q] = make_uint4(hb[4 * q], hb[4 * q + 1], hb[4 * q + 2], hb[4 * q + 3]);
+        pl[q] = make_uint4(lb[4 * q], lb[4 * q + 1], lb[4 * q + 2], lb[4 * q + 3]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const int n = n0 + t;
+      if (n < e.N) {
+        uint32_t hb, lb;
+        split_bits<ESZ>(v[t * STRIDE + OFF], hb, lb);
+        split_store_bits<ESZ>(e.phi, e.plo, rbase + (int64_t)(n / e.Dn) * e.s_n1 + (int64_t)(n % e.Dn) * e.s_n0,
+                              hb, lb);
+      }
+    }
+  }
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -148,7 +248,7 @@ template <int ESZ>
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                       const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, Epi epi,
-                      int num_k_tiles, int a_batched, int b_batched, int m_fast) {
+                      int num_k_tiles, int k_elems, int a_batched, int b_batched, int m_fast) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -213,13 +313,19 @@ __global__ void __launch_bounds__(THREADS, 1)
       const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
       const uint64_t dah = sdesc(base), dal = sdesc(base + A_TILE);
       const uint64_t dbh = sdesc(base + 2 * A_TILE), dbl = sdesc(base + 2 * A_TILE + B_TILE);
+      // K beyond k_elems is TMA zero fill: skip the sub-steps that only see it
+      constexpr int SUB = (KROW_BYTES / ESZ) / 4;  // elements per 32-byte instruction step
+      const int rem = k_elems - kt * (KROW_BYTES / ESZ);
+      const int nsub = rem >= 4 * SUB ? 4 : (rem + SUB - 1) / SUB;
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk) {
-        const uint64_t adv = (uint64_t)((kk * 32) >> 4);  // 32 bytes of K per instruction
-        const uint32_t first = (kt == 0 && kk == 0) ? 0u : 1u;
-        umma<ESZ>(tmem, dah + adv, dbh + adv, idesc, first);
-        umma<ESZ>(tmem, dah + adv, dbl + adv, idesc, 1u);
-        umma<ESZ>(tmem, dal + adv, dbh + adv, idesc, 1u);
+        if (kk < nsub) {
+          const uint64_t adv = (uint64_t)((kk * 32) >> 4);  // 32 bytes of K per instruction
+          const uint32_t first = (kt == 0 && kk == 0) ? 0u : 1u;
+          umma<ESZ>(tmem, dah + adv, dbh + adv, idesc, first);
+          umma<ESZ>(tmem, dah + adv, dbl + adv, idesc, 1u);
+          umma<ESZ>(tmem, dal + adv, dbh + adv, idesc, 1u);
+        }
       }
       umma_commit(&empty[s]);
     }
@@ -241,30 +347,45 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
         for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
         const int cp = n_tile * BN + c0;  // product column of v[0]
-        if (epi.mode == OUT_REAL) {
+        if (epi.mode == OUT_PACK) {
+          const int m = epi.inter == 1 ? (rp >> 1) : rp;
+          if (m < epi.M) {
+            const int64_t mbase =
+                (int64_t)bz * epi.s_b + (int64_t)(m / epi.Dm) * epi.s_m1 + (int64_t)(m % epi.Dm) * epi.s_m0;
+            if (epi.inter == 2) {
+              pack_run<ESZ, 2, 0>(v, epi, mbase, cp / 2, 0);
+              pack_run<ESZ, 2, 1>(v, epi, mbase, cp / 2, 1);
+            } else {
+              const int ri = epi.inter == 1 ? (rp & 1) : 0;
+              pack_run<ESZ, 1, 0>(v, epi, mbase, cp, ri);
+              pack_run<ESZ, 1, 16>(v, epi, mbase, cp + 16, ri);
+            }
+          }
+        } else if (epi.mode == OUT_REAL) {
           if (rp < epi.M) {
-            double* C = reinterpret_cast<double*>(epi.C) + (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
+            const int64_t base = (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
               const int n = cp + j;
               if (n < epi.N) {
-                double* p = C + (int64_t)n * epi.sCn;
-                *p = (epi.accumulate ? *p : 0.0) + (double)v[j];
+                if (epi.c_f32)
+                  st_real<float>(epi.C, base + (int64_t)n * epi.sCn, v[j], epi.accumulate);
+                else
+                  st_real<double>(epi.C, base + (int64_t)n * epi.sCn, v[j], epi.accumulate);
               }
             }
           }
         } else if (epi.mode == OUT_COLS_CPLX) {
           if (rp < epi.M) {
-            double2* C = reinterpret_cast<double2*>(epi.C) + (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
+            const int64_t base = (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const int n = cp / 2 + j;
               if (n < epi.N) {
-                double2* p = C + (int64_t)n * epi.sCn;
-                double2 o = epi.accumulate ? *p : make_double2(0.0, 0.0);
-                o.x += (double)v[2 * j];
-                o.y += (double)v[2 * j + 1];
-                *p = o;
+                if (epi.c_f32)
+                  st_cplx<float2>(epi.C, base + (int64_t)n * epi.sCn, v[2 * j], v[2 * j + 1], epi.accumulate);
+                else
+                  st_cplx<double2>(epi.C, base + (int64_t)n * epi.sCn, v[2 * j], v[2 * j + 1], epi.accumulate);
               }
             }
           }
@@ -280,17 +401,17 @@ __global__ void __launch_bounds__(THREADS, 1)
           }
           const int m = rp >> 1;
           if (m < epi.M) {
-            double2* C = reinterpret_cast<double2*>(epi.C) + (int64_t)bz * epi.sCb + (int64_t)m * epi.sCm;
+            const int64_t base = (int64_t)bz * epi.sCb + (int64_t)m * epi.sCm;
             const int nb = cp + (even ? 0 : 16);
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const int n = nb + j;
               if (n < epi.N) {
-                double2* p = C + (int64_t)n * epi.sCn;
-                double2 o = epi.accumulate ? *p : make_double2(0.0, 0.0);
-                o.x += (double)(even ? mine[j] : got[j]);
-                o.y += (double)(even ? got[j] : mine[j]);
-                *p = o;
+                const float re = even ? mine[j] : got[j], im = even ? got[j] : mine[j];
+                if (epi.c_f32)
+                  st_cplx<float2>(epi.C, base + (int64_t)n * epi.sCn, re, im, epi.accumulate);
+                else
+                  st_cplx<double2>(epi.C, base + (int64_t)n * epi.sCn, re, im, epi.accumulate);
               }
             }
           }
@@ -317,15 +438,17 @@ enum PackMode {
 
 struct PackArgs {
   const void* src;
-  int src_complex, conj;
+  int src_complex, conj, src_f32;
   int64_t s_r, s_k, s_b;  // element strides of rows, K and batch
+  // row r = (r2 * D1 + r1) * D0 + r0 sits at r0*s_r + r1*s_r1 + r2*s_r2
+  // (a single-strided row index has D0 >= R)
+  int D0, D1;
+  int64_t s_r1, s_r2;
   int R, K, nbatch, mode;
   void* hi;
   void* lo;
-  int64_t pitch;        // K' padded (elements)
+  int64_t pitch;        // row pitch of the packed buffer (elements, 16-byte multiple)
   int64_t rows_out;     // rows per batch in the packed buffer
-  int64_t kused;        // K' actually written; [kused, pitch) is zeroed
-  int kblocks;          // blocks along K that copy data; the block column after them zeroes the padding
 };
 
 template <int ESZ>
@@ -347,52 +470,36 @@ __device__ __forceinline__ void split_store(void* hi, void* lo, int64_t idx, dou
   }
 }
 
-template <int ESZ>
-__device__ __forceinline__ void zero_store(void* hi, void* lo, int64_t idx) {
-  if constexpr (ESZ == 2) {
-    reinterpret_cast<__nv_bfloat16*>(hi)[idx] = __float2bfloat16(0.f);
-    reinterpret_cast<__nv_bfloat16*>(lo)[idx] = __float2bfloat16(0.f);
-  } else {
-    reinterpret_cast<float*>(hi)[idx] = 0.f;
-    reinterpret_cast<float*>(lo)[idx] = 0.f;
-  }
-}
-
 // one 32 x 32 (rows x K) source tile per block, staged through shared memory so
-// that both the strided FP64 reads and the K-contiguous packed writes coalesce;
-// the extra block column (blockIdx.x == kblocks) zeroes the K padding
-// [kused, pitch) of the packed rows of its 32 source rows
+// that both the strided reads (FP64, or FP32 intermediates) and the
+// K-contiguous packed writes coalesce.  Packed rows hold K' elements at a
+// 16-byte pitch; the tensor maps end at K', so the TMA loads zero-fill the
+// rest of the last 128-byte K tile and no padding is ever written.
 template <int ESZ>
 __global__ void pack_kernel(PackArgs a) {
   __shared__ double2 tile[32][33];
   const int b = blockIdx.z;
   const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  if ((int)blockIdx.x >= a.kblocks) {
-    const int64_t base = (int64_t)b * a.rows_out * a.pitch;
-    const bool dbl = a.mode == P_DBL_CPLX || a.mode == P_DBL_SPLIT;
-    for (int i = ty; i < 32; i += 8) {
-      const int r = r0 + i;
-      if (r >= a.R) continue;
-      for (int rr = 0; rr < (dbl ? 2 : 1); ++rr) {
-        const int64_t row = base + (int64_t)(dbl ? 2 * r + rr : r) * a.pitch;
-        for (int64_t k = a.kused + tx; k < a.pitch; k += 32) zero_store<ESZ>(a.hi, a.lo, row + k);
-      }
-    }
-    return;
-  }
   const bool k_fast = (a.s_k == 1) || (a.s_r != 1);
   for (int i = ty; i < 32; i += 8) {
     const int r = k_fast ? r0 + i : r0 + tx;
     const int k = k_fast ? k0 + tx : k0 + i;
     double2 v = make_double2(0.0, 0.0);
     if (r < a.R && k < a.K) {
-      const int64_t off = (int64_t)b * a.s_b + (int64_t)r * a.s_r + (int64_t)k * a.s_k;
+      const int r0 = r % a.D0, rq = r / a.D0;
+      const int64_t roff = (int64_t)r0 * a.s_r + (int64_t)(rq % a.D1) * a.s_r1 + (int64_t)(rq / a.D1) * a.s_r2;
+      const int64_t off = (int64_t)b * a.s_b + roff + (int64_t)k * a.s_k;
       if (a.src_complex) {
-        v = reinterpret_cast<const double2*>(a.src)[off];
+        if (a.src_f32) {
+          const float2 f = reinterpret_cast<const float2*>(a.src)[off];
+          v = make_double2(f.x, f.y);
+        } else {
+          v = reinterpret_cast<const double2*>(a.src)[off];
+        }
         if (a.conj) v.y = -v.y;
       } else {
-        v.x = reinterpret_cast<const double*>(a.src)[off];
+        v.x = a.src_f32 ? (double)reinterpret_cast<const float*>(a.src)[off] : reinterpret_cast<const double*>(a.src)[off];
       }
     }
     if (k_fast)
@@ -456,10 +563,13 @@ static EncodeTiledFn encoder() {
   return fn;
 }
 
-static bool make_map(CUtensorMap* tm, void* base, int esz, int64_t pitch, int64_t rows, int64_t nb, int box_rows) {
+// 3-D map (K', rows, batch) over a packed buffer of row pitch `pitch`; loads
+// past K' read zeros
+static bool make_map(CUtensorMap* tm, void* base, int esz, int64_t kext, int64_t pitch, int64_t rows, int64_t nb,
+                     int box_rows) {
   EncodeTiledFn enc = encoder();
   if (!enc) return false;
-  cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)rows, (cuuint64_t)nb};
+  cuuint64_t dims[3] = {(cuuint64_t)kext, (cuuint64_t)rows, (cuuint64_t)nb};
   cuuint64_t strides[2] = {(cuuint64_t)(pitch * esz), (cuuint64_t)(pitch * esz * rows)};
   cuuint32_t box[3] = {(cuuint32_t)(KROW_BYTES / esz), (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -473,7 +583,7 @@ struct Plan {
   int esz, kstep;        // element size, elements per 128-byte K row
   int modeA, modeB, out;
   int64_t KA;            // logical K' (after re/im concatenation)
-  int64_t pitch;         // K' padded to 128-byte rows
+  int64_t pitch;         // packed row pitch: K' rounded up to 16 bytes
   int64_t rowsA, rowsB;  // packed rows per batch
   int64_t nbA, nbB;      // packed batches
   size_t offAh, offAl, offBh, offBl, total;
@@ -514,7 +624,8 @@ static Plan make_plan(const GemmParams& p, int prec) {
     q.out = OUT_REAL;
   }
   q.KA = kf * p.K;
-  q.pitch = ((q.KA + q.kstep - 1) / q.kstep) * q.kstep;
+  const int64_t align = 16 / q.esz;  // TMA row strides are 16-byte multiples
+  q.pitch = ((q.KA + align - 1) / align) * align;
   q.rowsA = (q.modeA == P_DBL_CPLX || q.modeA == P_DBL_SPLIT) ? 2 * (int64_t)p.M : p.M;
   q.rowsB = (q.modeB == P_DBL_CPLX || q.modeB == P_DBL_SPLIT) ? 2 * (int64_t)p.N : p.N;
   q.nbA = p.A.s_batch ? p.batch : 1;
@@ -530,15 +641,20 @@ static Plan make_plan(const GemmParams& p, int prec) {
 }
 
 template <int ESZ>
-static cudaError_t run_pack(const GemmOperand& op, int R, int K, int nb, int mode, void* hi, void* lo, int64_t pitch,
-                            int64_t rows_out, int64_t kused, cudaStream_t st) {
+static cudaError_t run_pack(const GemmOperand& op, int R, int K, int nb, int mode, const SplitRows& rs, void* hi,
+                            void* lo, int64_t pitch, int64_t rows_out, cudaStream_t st) {
   PackArgs a;
   a.src = op.ptr;
   a.src_complex = op.is_complex;
   a.conj = op.conj;
+  a.src_f32 = op.is_f32;
   a.s_r = op.s_outer;
   a.s_k = op.s_k;
   a.s_b = op.s_batch;
+  a.D0 = rs.D0 > 0 ? rs.D0 : std::max(R, 1);
+  a.D1 = rs.D0 > 0 ? std::max(rs.D1, 1) : 1;
+  a.s_r1 = rs.D0 > 0 ? rs.s_r1 : 0;
+  a.s_r2 = rs.D0 > 0 ? rs.s_r2 : 0;
   a.R = R;
   a.K = K;
   a.nbatch = nb;
@@ -547,49 +663,84 @@ static cudaError_t run_pack(const GemmOperand& op, int R, int K, int nb, int mod
   a.lo = lo;
   a.pitch = pitch;
   a.rows_out = rows_out;
-  a.kused = kused;
-  a.kblocks = (int)ceil_div(K, 32);
-  dim3 grid((unsigned)(a.kblocks + (pitch > kused ? 1 : 0)), (unsigned)ceil_div(R, 32), (unsigned)nb);
+  dim3 grid((unsigned)ceil_div(K, 32), (unsigned)ceil_div(R, 32), (unsigned)nb);
   count_launch();
   pack_kernel<ESZ><<<grid, dim3(32, 8), 0, st>>>(a);
   return cudaGetLastError();
 }
 
+static int inter_of(int modeA, int modeB) {
+  if (modeA == P_DBL_CPLX || modeA == P_DBL_SPLIT) return 1;
+  if (modeB == P_DBL_CPLX || modeB == P_DBL_SPLIT) return 2;
+  return 0;
+}
+
+// C' = A' B'^T over packed operands; the epilogue writes FP64/FP32 C (c != null)
+// or the next stage's packed operand (po != null)
 template <int ESZ>
-static cudaError_t run_split(const GemmParams& p, const Plan& q, char* ws, cudaStream_t st) {
-  void *Ah = ws + q.offAh, *Al = ws + q.offAl, *Bh = ws + q.offBh, *Bl = ws + q.offBl;
-  cudaError_t e = run_pack<ESZ>(p.A, p.M, p.K, (int)q.nbA, q.modeA, Ah, Al, q.pitch, q.rowsA, q.KA, st);
-  if (e == cudaSuccess) e = run_pack<ESZ>(p.B, p.N, p.K, (int)q.nbB, q.modeB, Bh, Bl, q.pitch, q.rowsB, q.KA, st);
-  if (e != cudaSuccess) return e;
+static cudaError_t launch_split(const SplitPacked& A, const SplitPacked& B, int M, int N, int batch,
+                                const GemmParams* c, const SplitPackOut* po, cudaStream_t st) {
   CUtensorMap tAh, tAl, tBh, tBl;
-  if (!make_map(&tAh, Ah, ESZ, q.pitch, q.rowsA, q.nbA, BM) || !make_map(&tAl, Al, ESZ, q.pitch, q.rowsA, q.nbA, BM) ||
-      !make_map(&tBh, Bh, ESZ, q.pitch, q.rowsB, q.nbB, BN) || !make_map(&tBl, Bl, ESZ, q.pitch, q.rowsB, q.nbB, BN))
+  if (A.kext != B.kext) return cudaErrorInvalidValue;
+  if (!make_map(&tAh, A.hi, ESZ, A.kext, A.pitch, A.rows, A.nb, BM) ||
+      !make_map(&tAl, A.lo, ESZ, A.kext, A.pitch, A.rows, A.nb, BM) ||
+      !make_map(&tBh, B.hi, ESZ, B.kext, B.pitch, B.rows, B.nb, BN) ||
+      !make_map(&tBl, B.lo, ESZ, B.kext, B.pitch, B.rows, B.nb, BN))
     return cudaErrorInvalidValue;
-  Epi epi;
-  epi.C = p.C;
-  epi.sCm = p.sCm;
-  epi.sCn = p.sCn;
-  epi.sCb = p.sCb;
-  epi.M = p.M;
-  epi.N = p.N;
-  epi.mode = q.out;
-  epi.accumulate = p.accumulate;
-  epi.rows_p = (int)q.rowsA;
-  epi.cols_p = (int)q.rowsB;
+  const int inter = inter_of(A.mode, B.mode);
+  Epi epi{};
+  epi.M = M;
+  epi.N = N;
+  epi.rows_p = (int)A.rows;
+  epi.cols_p = (int)B.rows;
+  if (po) {
+    epi.mode = OUT_PACK;
+    epi.phi = po->hi;
+    epi.plo = po->lo;
+    epi.s_b = po->s_b;
+    epi.s_m1 = po->s_m1;
+    epi.s_m0 = po->s_m0;
+    epi.s_n1 = po->s_n1;
+    epi.s_n0 = po->s_n0;
+    epi.s_ri = po->s_ri;
+    epi.Dm = po->Dm > 0 ? po->Dm : 1 << 30;
+    epi.Dn = po->Dn > 0 ? po->Dn : 1 << 30;
+    epi.inter = inter;
+  } else {
+    epi.mode = inter == 1 ? OUT_ROWS_CPLX : inter == 2 ? OUT_COLS_CPLX : OUT_REAL;
+    epi.C = c->C;
+    epi.sCm = c->sCm;
+    epi.sCn = c->sCn;
+    epi.sCb = c->sCb;
+    epi.accumulate = c->accumulate;
+    epi.c_f32 = c->c_f32;
+  }
   static bool attr_set = false;
   if (!attr_set) {
-    e = cudaFuncSetAttribute(split_gemm_kernel<ESZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaError_t e = cudaFuncSetAttribute(split_gemm_kernel<ESZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  const int64_t mt = ceil_div(q.rowsA, BM), nt = ceil_div(q.rowsB, BN);
+  const int64_t kstep = KROW_BYTES / ESZ;
+  const int64_t mt = ceil_div(A.rows, BM), nt = ceil_div(B.rows, BN);
   // walk the smaller operand's tiles fastest (packed rows per batch decide)
-  const int m_fast = (q.rowsA <= q.rowsB && mt > 1 && nt <= 65535) ? 1 : 0;
-  dim3 grid((unsigned)(m_fast ? mt : nt), (unsigned)(m_fast ? nt : mt), (unsigned)p.batch);
+  const int m_fast = (A.rows <= B.rows && mt > 1 && nt <= 65535) ? 1 : 0;
+  if ((m_fast ? mt : nt) > 0x7fffffff || (m_fast ? nt : mt) > 65535 || batch > 65535) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)(m_fast ? mt : nt), (unsigned)(m_fast ? nt : mt), (unsigned)batch);
   count_launch();
-  split_gemm_kernel<ESZ><<<grid, THREADS, SMEM_BYTES, st>>>(tAh, tAl, tBh, tBl, epi, (int)(q.pitch / q.kstep),
-                                                            q.nbA > 1 ? 1 : 0, q.nbB > 1 ? 1 : 0, m_fast);
+  split_gemm_kernel<ESZ><<<grid, THREADS, SMEM_BYTES, st>>>(tAh, tAl, tBh, tBl, epi, (int)ceil_div(A.kext, kstep),
+                                                            (int)A.kext, A.nb > 1 ? 1 : 0, B.nb > 1 ? 1 : 0, m_fast);
   return cudaGetLastError();
+}
+
+template <int ESZ>
+static cudaError_t run_split(const GemmParams& p, const Plan& q, char* ws, cudaStream_t st) {
+  SplitPacked A{ws + q.offAh, ws + q.offAl, q.pitch, q.rowsA, q.nbA, q.KA, q.modeA};
+  SplitPacked B{ws + q.offBh, ws + q.offBl, q.pitch, q.rowsB, q.nbB, q.KA, q.modeB};
+  cudaError_t e = run_pack<ESZ>(p.A, p.M, p.K, (int)q.nbA, q.modeA, SplitRows{}, A.hi, A.lo, q.pitch, q.rowsA, st);
+  if (e == cudaSuccess) e = run_pack<ESZ>(p.B, p.N, p.K, (int)q.nbB, q.modeB, SplitRows{}, B.hi, B.lo, q.pitch, q.rowsB, st);
+  if (e != cudaSuccess) return e;
+  return launch_split<ESZ>(A, B, p.M, p.N, p.batch, &p, nullptr, st);
 }
 
 }  // namespace split
@@ -606,11 +757,43 @@ size_t split_gemm_workspace_bytes(int64_t a_elems, int64_t b_elems) {
 
 cudaError_t split_gemm(const GemmParams& p, int prec, void* ws, size_t ws_bytes, cudaStream_t st) {
   if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return cudaSuccess;
-  if (p.K <= 0) return gemm_fp64(p, st);
+  if (p.K <= 0) return (p.A.is_f32 || p.B.is_f32 || p.c_f32) ? cudaErrorInvalidValue : gemm_fp64(p, st);
   const split::Plan q = split::make_plan(p, prec);
   if (q.total > ws_bytes || !ws) return cudaErrorInvalidValue;
   if (q.esz == 2) return split::run_split<2>(p, q, static_cast<char*>(ws), st);
   return split::run_split<4>(p, q, static_cast<char*>(ws), st);
+}
+
+int split_esz(int prec) { return prec == RENO_PREC_BF16X3 ? 2 : 4; }
+
+int64_t split_pitch(int64_t kext, int prec) {
+  const int64_t align = 16 / split_esz(prec);
+  return ((kext + align - 1) / align) * align;
+}
+
+size_t split_packed_bytes(int64_t rows, int64_t kext, int64_t nb, int prec) {
+  return 2 * split::al((size_t)rows * split_pitch(kext, prec) * nb * split_esz(prec));
+}
+
+SplitPacked split_packed_at(void* base, int64_t rows, int64_t kext, int64_t nb, int mode, int prec) {
+  const size_t plane = split::al((size_t)rows * split_pitch(kext, prec) * nb * split_esz(prec));
+  return SplitPacked{base, static_cast<char*>(base) + plane, split_pitch(kext, prec), rows, nb, kext, mode};
+}
+
+cudaError_t split_pack(const GemmOperand& op, int R, int K, int nb, const SplitRows& rs, const SplitPacked& dst,
+                       int prec, cudaStream_t st) {
+  if (R <= 0 || K <= 0 || nb <= 0) return cudaSuccess;
+  if (split_esz(prec) == 2)
+    return split::run_pack<2>(op, R, K, nb, dst.mode, rs, dst.hi, dst.lo, dst.pitch, dst.rows, st);
+  return split::run_pack<4>(op, R, K, nb, dst.mode, rs, dst.hi, dst.lo, dst.pitch, dst.rows, st);
+}
+
+cudaError_t split_run(const SplitPacked& A, const SplitPacked& B, int M, int N, int batch, const GemmParams* c,
+                      const SplitPackOut* po, int prec, cudaStream_t st) {
+  if (M <= 0 || N <= 0 || batch <= 0) return cudaSuccess;
+  if ((c == nullptr) == (po == nullptr)) return cudaErrorInvalidValue;
+  if (split_esz(prec) == 2) return split::launch_split<2>(A, B, M, N, batch, c, po, st);
+  return split::launch_split<4>(A, B, M, N, batch, c, po, st);
 }
 
 int split_gemm_take_error() {

@@ -231,27 +231,41 @@ class SubspaceOptions:
     bond's cap k on the kept dimension is known (``fixed`` criteria), needs
     only its leading k singular triplets: the selection takes at most k from
     any one block and the fixed rule reads only min(k, len(sigma)).  They
-    come from ``iters`` + 1 products with X X^H (two FP64 GEMMs each,
-    Householder QR in between) on kk = k + oversample columns, a
+    come from ``iters`` + 1 products with X X^H (two FP64 GEMMs each, an
+    orthonormalisation in between) on kk = k + oversample columns, a
     Rayleigh-Ritz step on the kk x kk projection and the norms of the
     projected rows.  Acceptance uses the excess discarded weight the Ritz
     basis can carry, estimated from the residuals
     r_i = ||X X^H u_i - lambda_i u_i|| of the leading k as
     sum_i r_i^2 / max(lambda_i - lambda_kk, r_i): it must stay below
-    ``rtol`` * ||X||_F^2, otherwise the block falls back to the full Gram
-    eigendecomposition.  ``min_dim = 0`` disables the path.  Defaults can be
-    overridden by RENO_SUBSPACE="min_dim,iters,oversample,rtol"."""
+    ``rtol`` * ||X||_F^2.  A block that misses it runs ``iters`` + 1 more
+    products from its current basis and is checked again; if it still
+    misses, it falls back to the full Gram eigendecomposition.
+    Off by default (``min_dim = 0``): on the two-site TDVP workload (96 sites,
+    M = 256) the Ritz vectors near the cut differ between runs that differ
+    only in rounding, and split-precision and FP64 trajectories drifted apart
+    by 1.2e-5 in the populations over 8 steps (2e-7 with the full
+    decomposition), with 40 % of the blocks needing a retry or the fallback.
+    ``orth`` picks the orthonormalisation
+    ("householder", or "cholqr": shifted CholeskyQR3, which needs full column
+    rank and so fails -- and falls back -- on rank-deficient blocks).
+    RENO_SUBSPACE=
+    "min_dim,iters,oversample,rtol[,orth]" overrides the defaults."""
 
-    def __init__(self, min_dim=1024, iters=3, oversample=64, rtol=1e-13):
+    def __init__(self, min_dim=0, iters=3, oversample=64, rtol=1e-13, orth="householder"):
         env = os.environ.get("RENO_SUBSPACE")
         if env:
-            a, b, c, d = env.split(",")
-            min_dim, iters, oversample, rtol = int(a), int(b), int(c), float(d)
+            parts = env.split(",")
+            min_dim, iters, oversample, rtol = int(parts[0]), int(parts[1]), int(parts[2]), float(parts[3])
+            if len(parts) > 4:
+                orth = parts[4]
+        self.orth = orth
         self.min_dim = min_dim
         self.iters = iters
         self.oversample = oversample
         self.rtol = rtol
         self.calls = 0
+        self.retries = 0
         self.fallbacks = 0
 
 
@@ -274,17 +288,44 @@ def _omega(rows, kk, dtype, device):
     return om
 
 
-def _topk_kept_side(eng: Engine, A: torch.Tensor, k: int, opts: SubspaceOptions):
+def _orthonormalise(eng: Engine, Y: torch.Tensor, method: str) -> torch.Tensor:
+    """An orthonormal basis of the columns of Y (r x kk, r >= kk).
+
+    "householder": torch.linalg.qr.  "cholqr": shifted CholeskyQR3 (Fukaya,
+    Kannan, Nakatsukasa, Yamamoto, Yanagisawa, SIAM J. Sci. Comput. 2020): one
+    Cholesky QR of the Gram matrix shifted by 11 (r kk + kk (kk + 1)) u tr(G),
+    which keeps it positive definite for any column rank, then two plain
+    Cholesky QR passes that restore orthonormality to rounding level -- three
+    kk x kk Gram GEMMs, Cholesky factorisations and triangular solves, with no
+    host synchronisation."""
+    if method == "householder":
+        return torch.linalg.qr(Y, mode="reduced")[0]
+    r, kk = Y.shape
+    u = np.finfo(np.float64).eps / 2
+    for shifted in (True, False, False):
+        G = eng.matmul(Y.transpose(0, 1), Y, conj_a=True)
+        if shifted:
+            tr = torch.diagonal(G).real.sum()
+            G.diagonal().add_((11.0 * (r * kk + kk * (kk + 1)) * u * tr).to(G.dtype))
+        Lc, _ = torch.linalg.cholesky_ex(G)
+        Y = torch.linalg.solve_triangular(Lc.transpose(0, 1).conj(), Y, upper=True, left=False)
+    return Y
+
+
+def _topk_kept_side(eng: Engine, A: torch.Tensor, k: int, opts: SubspaceOptions, Q=None, iters=None):
     """Leading k left singular vectors of A (r x c, any 2-D view) by block
-    subspace iteration.  Returns K (r x k, descending), P = K^H A (k x c),
-    S (k, device: row norms of P) and a device pair (excess-weight estimate,
-    ||A||_F^2) for the acceptance test."""
+    subspace iteration, from the seeded Gaussian block or from a previous
+    call's basis Q.  Returns K (r x k, descending), P = K^H A (k x c),
+    S (k, device: row norms of P), a device pair (excess-weight estimate,
+    ||A||_F^2) for the acceptance test, and the iterated basis Q."""
     r = A.shape[0]
     kk = min(k + opts.oversample, r)
-    Q = _omega(r, kk, A.dtype, A.device)
-    for _ in range(opts.iters + 1):
+    if Q is None:
+        Q = _omega(r, kk, A.dtype, A.device)
+        iters = opts.iters + 1
+    for _ in range(iters):
         Y = eng.matmul(A, eng.matmul(A.transpose(0, 1), Q, conj_a=True))
-        Q, _ = torch.linalg.qr(Y, mode="reduced")
+        Q = _orthonormalise(eng, Y, opts.orth)
     B = eng.matmul(Q.transpose(0, 1), A, conj_a=True)          # kk x c
     T = eng.matmul(B, B.transpose(0, 1), conj_b=True)          # kk x kk
     w, W = torch.linalg.eigh(T)                                 # ascending
@@ -298,7 +339,16 @@ def _topk_kept_side(eng: Engine, A: torch.Tensor, k: int, opts: SubspaceOptions)
     excess = torch.sum(res * res / torch.clamp(gap, min=1e-300))
     fro2 = torch.linalg.vector_norm(A) ** 2
     S = torch.linalg.vector_norm(P, dim=1)
-    return K, P, S, torch.stack([excess, fro2])
+    return K, P, S, torch.stack([excess, fro2]), Q
+
+
+def _subspace_block(eng, X, keep_left, k, opts, Q=None, iters=None):
+    """_topk_kept_side on the kept side of block X: (K, P, S, check, Q) with
+    P = sigma Vh (keep_left) or U sigma (keep right)."""
+    if keep_left:
+        return _topk_kept_side(eng, X, k, opts, Q, iters)
+    K, Ph, S, chk, Q = _topk_kept_side(eng, X.transpose(0, 1).conj(), k, opts, Q, iters)
+    return K, Ph.transpose(0, 1).conj().resolve_conj(), S, chk, Q
 
 
 def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool) -> dict:
@@ -378,14 +428,10 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         if (subspace.min_dim and kcap is not None and dim >= subspace.min_dim
                 and dim >= 2 * (ksub + subspace.oversample)):
             subspace.calls += 1
-            if keep_left:
-                K, P, S, res = _topk_kept_side(eng, X, ksub, subspace)
-            else:
-                K, Ph, S, res = _topk_kept_side(eng, X.transpose(0, 1).conj(), ksub, subspace)
-                P = Ph.transpose(0, 1).conj().resolve_conj()     # (m, k) = U sigma
+            K, P, S, chk, Q = _subspace_block(eng, X, keep_left, ksub, subspace)
             npad = upad if keep_left else vpad
-            blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=ksub, npad=npad, res=res,
-                               X=X))
+            blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=ksub, npad=npad, res=chk,
+                               X=X, Q=Q))
             continue
         full = _full_kept_side(eng, X, keep_left)
         K, P, S = full["K"], full["P"], full["S"]
@@ -399,16 +445,32 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
     for b in blocks:
         b["Sh"] = host[off:off + b["dim"]]
         off += b["dim"]
+    ok = lambda e, f: bool(np.isfinite(e) and e <= subspace.rtol * f)
+    retry = []
     for b in sub:
-        excess, fro2 = host[off], host[off + 1]
+        if not ok(host[off], host[off + 1]):
+            retry.append(b)
         off += 2
-        if not (np.isfinite(excess) and excess <= subspace.rtol * fro2):
-            # Ritz pairs not converged to the tolerance: full decomposition of this block
-            subspace.fallbacks += 1
-            full = _full_kept_side(eng, b["X"], keep_left)
-            b.update(full)
-            b["Sh"] = b["S"].cpu().numpy()
+    if retry:
+        # continue those blocks' iteration from their current basis, check once
+        # more, then fall back to the full decomposition
+        for b in retry:
+            subspace.retries += 1
+            b["K"], b["P"], b["S"], b["res"], b["Q"] = _subspace_block(eng, b["X"], keep_left, b["dim"], subspace,
+                                                                       b["Q"], subspace.iters + 1)
+        host2 = torch.cat([t for b in retry for t in (b["S"], b["res"])]).cpu().numpy()
+        off = 0
+        for b in retry:
+            b["Sh"] = host2[off:off + b["dim"]]
+            e, f = host2[off + b["dim"]], host2[off + b["dim"] + 1]
+            off += b["dim"] + 2
+            if not ok(e, f):
+                subspace.fallbacks += 1
+                b.update(_full_kept_side(eng, b["X"], keep_left))
+                b["Sh"] = b["S"].cpu().numpy()
+    for b in sub:
         b.pop("X", None)
+        b.pop("Q", None)
     # the reference's concatenated order: nonzero parts block by block, then
     # the zero-sigma paddings block by block (svd_qn.py:222-230)
     sig, qns, where = [], [], []

@@ -95,6 +95,26 @@ def test_split_heff_2site_holstein_block(prec):
     assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
 
 
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("cplx", [True, False])
+@pytest.mark.parametrize("ml,mr,d1,d2,wl,wm,wr", [(64, 48, 2, 16, 5, 5, 4), (48, 40, 16, 2, 4, 5, 5),
+                                                   (33, 17, 3, 5, 3, 4, 2), (128, 128, 16, 16, 5, 5, 4)])
+def test_split_heff_2site_fused_shapes(prec, cplx, ml, mr, d1, d2, wl, wm, wr):
+    """the fused 2-site chain (epilogues writing the next stage's packed
+    operand): electron-phonon and phonon-electron blocks (runs along K of 2
+    elements take the scalar stores), ragged bonds, the real (DMRG) form"""
+    from renormalizer_b200.hop_expr import HeffOperator
+    rng = np.random.default_rng(ml + d1)
+    mk = lambda s: rng.standard_normal(s) + (1j * rng.standard_normal(s) if cplx else 0)
+    L, R, psi = mk((ml, wl, ml)), mk((mr, wr, mr)), mk((ml, d1, d2, mr))
+    W1, W2 = rng.standard_normal((wl, d1, d1, wm)), rng.standard_normal((wm, d2, d2, wr))
+    ref = O.hop(L, [W1, W2], R, psi)
+    op = HeffOperator(L, R, [W1, W2], psi.shape, prec=prec)
+    y = op(torch.from_numpy(psi).cuda()).cpu().numpy()
+    assert y.dtype == ref.dtype
+    assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
+
+
 @pytest.mark.parametrize("prec,atol", [("bf16x3", 2e-5), ("tf32x3", 2e-6)])
 def test_split_tdvp_short_trajectory(prec, atol):
     from renormalizer_b200 import EvolveConfig, EvolveMethod, backend

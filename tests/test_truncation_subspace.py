@@ -43,13 +43,8 @@ def _run(coef, ql, qr, keep_left, kcap, percent=0.0):
 
 def _compare(coef, ql, qr, keep_left, kcap, percent=0.0):
     svd_qn = importlib.import_module("renormalizer_b200.svd_qn")
-    saved = svd_qn.subspace.min_dim
-    try:
-        svd_qn.subspace.min_dim = 0
-        from renormalizer_b200.svd_qn import svd_truncate
-        full = svd_truncate(coef, ql, qr, np.array([1]), keep_left, lambda s: min(kcap, len(s)), percent=percent)
-    finally:
-        svd_qn.subspace.min_dim = saved
+    from renormalizer_b200.svd_qn import svd_truncate
+    full = svd_truncate(coef, ql, qr, np.array([1]), keep_left, lambda s: min(kcap, len(s)), percent=percent)
     sub = _run(coef, ql, qr, keep_left, kcap, percent)
     assert sub.mdim == full.mdim == kcap
     np.testing.assert_array_equal(np.asarray(sub.qn), np.asarray(full.qn))
@@ -96,7 +91,12 @@ def test_subspace_fallback_reproduces_full_path_cpu(cpu_engine):
 @pytest.mark.parametrize("keep_left", [True, False])
 def test_subspace_matches_full_path_gpu(keep_left):
     svd_qn = importlib.import_module("renormalizer_b200.svd_qn")
+    saved = svd_qn.subspace.min_dim
+    svd_qn.subspace.min_dim = 1024
     f0 = svd_qn.subspace.fallbacks
-    coef, ql, qr = _case("cuda", 2048, 45.0)
-    _compare(coef, ql, qr, keep_left, 256)
-    assert svd_qn.subspace.fallbacks == f0
+    try:
+        coef, ql, qr = _case("cuda", 2048, 45.0)
+        _compare(coef, ql, qr, keep_left, 256)
+        assert svd_qn.subspace.fallbacks == f0
+    finally:
+        svd_qn.subspace.min_dim = saved
