@@ -35,7 +35,7 @@ constexpr int A_TILE = BM * KROW_BYTES;   // 16 KB
 constexpr int B_TILE = BN * KROW_BYTES;   // 32 KB
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t TMEM_COLS = 256;  // one accumulator buffer (two are allocated)
 constexpr uint64_t WAIT_NS = 2000000000ull;  // bounded spin: 2 s of wall clock
 
 // device error word: 0 = ok; otherwise 1000 + site of the first timed-out wait
@@ -244,36 +244,169 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
         "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])     \
       : "r"(taddr))
 
+// Epilogue of one output tile: TMEM columns [tacc, tacc + BN) -> registers
+// (32 columns at a time) -> the output in the Epi mode.  Warp w reads TMEM
+// lane quarter q = w % 4, i.e. tile rows q*32 .. q*32+31.
+template <int ESZ>
+__device__ __forceinline__ void epilogue_tile(const Epi& epi, uint32_t tacc, int q, int lane, int m_tile, int n_tile,
+                                              int bz) {
+  const int row = q * 32 + lane;  // tile row of this thread
+  const int rp = m_tile * BM + row;
+  for (int c0 = 0; c0 < BN; c0 += 32) {
+    uint32_t r[32];
+    const uint32_t taddr = tacc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+    TMEM_LD32(taddr, r);
+    asm volatile("tcgen05.wait::ld.sync.aligned;");
+    float v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+    const int cp = n_tile * BN + c0;  // product column of v[0]
+    if (epi.mode == OUT_PACK) {
+      const int m = epi.inter == 1 ? (rp >> 1) : rp;
+      if (m < epi.M) {
+        const int64_t mbase =
+            (int64_t)bz * epi.s_b + (int64_t)(m / epi.Dm) * epi.s_m1 + (int64_t)(m % epi.Dm) * epi.s_m0;
+        if (epi.inter == 2) {
+          pack_run<ESZ, 2, 0>(v, epi, mbase, cp / 2, 0);
+          pack_run<ESZ, 2, 1>(v, epi, mbase, cp / 2, 1);
+        } else {
+          const int ri = epi.inter == 1 ? (rp & 1) : 0;
+          pack_run<ESZ, 1, 0>(v, epi, mbase, cp, ri);
+          pack_run<ESZ, 1, 16>(v, epi, mbase, cp + 16, ri);
+        }
+      }
+    } else if (epi.mode == OUT_REAL) {
+      if (rp < epi.M) {
+        const int64_t base = (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int n = cp + j;
+          if (n < epi.N) {
+            if (epi.c_f32)
+              st_real<float>(epi.C, base + (int64_t)n * epi.sCn, v[j], epi.accumulate);
+            else
+              st_real<double>(epi.C, base + (int64_t)n * epi.sCn, v[j], epi.accumulate);
+          }
+        }
+      }
+    } else if (epi.mode == OUT_COLS_CPLX) {
+      if (rp < epi.M) {
+        const int64_t base = (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = cp / 2 + j;
+          if (n < epi.N) {
+            if (epi.c_f32)
+              st_cplx<float2>(epi.C, base + (int64_t)n * epi.sCn, v[2 * j], v[2 * j + 1], epi.accumulate);
+            else
+              st_cplx<double2>(epi.C, base + (int64_t)n * epi.sCn, v[2 * j], v[2 * j + 1], epi.accumulate);
+          }
+        }
+      }
+    } else {
+      // rows interleave re/im: lanes (2i, 2i+1) hold (re, im) of complex row rp/2
+      const bool even = (lane & 1) == 0;
+      float mine[16], got[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const float send = even ? v[16 + j] : v[j];
+        got[j] = __shfl_xor_sync(0xffffffffu, send, 1);
+        mine[j] = even ? v[j] : v[16 + j];
+      }
+      const int m = rp >> 1;
+      if (m < epi.M) {
+        const int64_t base = (int64_t)bz * epi.sCb + (int64_t)m * epi.sCm;
+        const int nb = cp + (even ? 0 : 16);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = nb + j;
+          if (n < epi.N) {
+            const float re = even ? mine[j] : got[j], im = even ? got[j] : mine[j];
+            if (epi.c_f32)
+              st_cplx<float2>(epi.C, base + (int64_t)n * epi.sCn, re, im, epi.accumulate);
+            else
+              st_cplx<double2>(epi.C, base + (int64_t)n * epi.sCn, re, im, epi.accumulate);
+          }
+        }
+      }
+    }
+  }
+}
+
+// tile t of the (bz, slow, fast) raster: M tiles fastest when m_fast
+__device__ __forceinline__ void tile_coords(int t, int mt, int nt, int m_fast, int& m_tile, int& n_tile, int& bz) {
+  const int per = mt * nt;
+  bz = t / per;
+  const int r = t - bz * per;
+  if (m_fast) {
+    m_tile = r % mt;
+    n_tile = r / mt;
+  } else {
+    n_tile = r % nt;
+    m_tile = r / nt;
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// bounded wait that ignores the abort flag: used only to drain the CTA's own
+// copies and MMAs in flight before it frees TMEM and exits
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_try(bar, parity)) return;
+    if ((it & 255u) == 255u && global_ns() - t0 > WAIT_NS) {
+      atomicCAS(&g_split_error, 0, 1009);
+      return;
+    }
+  }
+}
+
+// Persistent kernel: one CTA per SM walks output tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... in the raster above.  TMEM holds two BN-column
+// FP32 accumulators; the MMA thread fills buffer (i & 1) for the CTA's i-th
+// tile while the epilogue warps drain the other, so each tile's epilogue
+// overlaps the next tile's TMA + MMA mainloop.  The smem stage ring runs on
+// across tiles.  Barriers: full / empty (TMA <-> MMA, per stage), tmem_full
+// (MMA -> epilogue, per buffer, tcgen05.commit), tmem_empty (epilogue -> MMA,
+// per buffer, one arrive per epilogue warp), drain (the MMA thread's last
+// commit, waited for before TMEM is freed).
 template <int ESZ>
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                       const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, Epi epi,
-                      int num_k_tiles, int k_elems, int a_batched, int b_batched, int m_fast) {
+                      int num_k_tiles, int k_elems, int a_batched, int b_batched, int m_fast, int mt, int nt,
+                      int ntiles) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
   uint64_t* empty = full + STAGES;
-  uint64_t* tmem_full = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tmem_full + 1);
+  uint64_t* tmem_full = empty + STAGES;  // [2]
+  uint64_t* tmem_empty = tmem_full + 2;  // [2]
+  uint64_t* drain = tmem_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  // m_fast: consecutive CTAs walk the M tiles of one N tile, so a large B
-  // operand streams from HBM once while the small A operand stays in L2
-  const int m_tile = m_fast ? blockIdx.x : blockIdx.y, n_tile = m_fast ? blockIdx.y : blockIdx.x, bz = blockIdx.z;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(tmem_full, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tmem_full[b], 1);
+      mbar_init(&tmem_empty[b], 4);
+    }
+    mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS));
+                 "r"(2 * TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -283,147 +416,103 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   if (warp == 0 && lane == 0) {
     // ---------------- TMA producer
-    const int za = a_batched ? bz : 0, zb = b_batched ? bz : 0;
-    for (int kt = 0; kt < num_k_tiles; ++kt) {
-      const int s = kt % STAGES;
-      const uint32_t ph = (kt / STAGES) & 1;
-      if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, 1)) break;
-      unsigned char* st = smem + s * STAGE_BYTES;
-      mbar_expect_tx(&full[s], STAGE_BYTES);
-      const int kx = kt * (KROW_BYTES / ESZ);
-      tma_load_3d(st, &tmAh, &full[s], kx, m_tile * BM, za);
-      tma_load_3d(st + A_TILE, &tmAl, &full[s], kx, m_tile * BM, za);
-      tma_load_3d(st + 2 * A_TILE, &tmBh, &full[s], kx, n_tile * BN, zb);
-      tma_load_3d(st + 2 * A_TILE + B_TILE, &tmBl, &full[s], kx, n_tile * BN, zb);
+    uint32_t g = 0;  // k tiles issued by this CTA
+    bool ok = true;
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+      int m_tile, n_tile, bz;
+      tile_coords(t, mt, nt, m_fast, m_tile, n_tile, bz);
+      const int za = a_batched ? bz : 0, zb = b_batched ? bz : 0;
+      for (int kt = 0; kt < num_k_tiles; ++kt) {
+        const int s = g % STAGES;
+        const uint32_t ph = (g / STAGES) & 1;
+        if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, 1)) {
+          ok = false;
+          break;
+        }
+        unsigned char* st = smem + s * STAGE_BYTES;
+        mbar_expect_tx(&full[s], STAGE_BYTES);
+        const int kx = kt * (KROW_BYTES / ESZ);
+        tma_load_3d(st, &tmAh, &full[s], kx, m_tile * BM, za);
+        tma_load_3d(st + A_TILE, &tmAl, &full[s], kx, m_tile * BM, za);
+        tma_load_3d(st + 2 * A_TILE, &tmBh, &full[s], kx, n_tile * BN, zb);
+        tma_load_3d(st + 2 * A_TILE + B_TILE, &tmBl, &full[s], kx, n_tile * BN, zb);
+        ++g;
+      }
     }
+    // land every copy this CTA issued before it can exit (immediate for the
+    // ones the MMA thread already consumed)
+    for (uint32_t j = (g > (uint32_t)STAGES ? g - STAGES : 0u); j < g; ++j)
+      mbar_drain(&full[j % STAGES], (j / STAGES) & 1);
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
     constexpr uint32_t fmt = ESZ == 2 ? 1u : 2u;  // BF16 : TF32
     const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
                            ((uint32_t)(BM >> 4) << 24);
+    uint32_t g = 0;
     bool ok = true;
-    for (int kt = 0; kt < num_k_tiles && ok; ++kt) {
-      const int s = kt % STAGES;
-      const uint32_t ph = (kt / STAGES) & 1;
-      if (!mbar_wait(&full[s], ph, abort_flag, 2)) {
-        ok = false;
-        break;
-      }
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      const uint32_t use = (uint32_t)(i >> 1);
+      if (!mbar_wait(&tmem_empty[b], (use & 1) ^ 1, abort_flag, 4)) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
-      const uint64_t dah = sdesc(base), dal = sdesc(base + A_TILE);
-      const uint64_t dbh = sdesc(base + 2 * A_TILE), dbl = sdesc(base + 2 * A_TILE + B_TILE);
-      // K beyond k_elems is TMA zero fill: skip the sub-steps that only see it
-      constexpr int SUB = (KROW_BYTES / ESZ) / 4;  // elements per 32-byte instruction step
-      const int rem = k_elems - kt * (KROW_BYTES / ESZ);
-      const int nsub = rem >= 4 * SUB ? 4 : (rem + SUB - 1) / SUB;
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        if (kk < nsub) {
-          const uint64_t adv = (uint64_t)((kk * 32) >> 4);  // 32 bytes of K per instruction
-          const uint32_t first = (kt == 0 && kk == 0) ? 0u : 1u;
-          umma<ESZ>(tmem, dah + adv, dbh + adv, idesc, first);
-          umma<ESZ>(tmem, dah + adv, dbl + adv, idesc, 1u);
-          umma<ESZ>(tmem, dal + adv, dbh + adv, idesc, 1u);
+      const uint32_t tacc = tmem + (uint32_t)(b * TMEM_COLS);
+      for (int kt = 0; kt < num_k_tiles; ++kt) {
+        const int s = g % STAGES;
+        const uint32_t ph = (g / STAGES) & 1;
+        if (!mbar_wait(&full[s], ph, abort_flag, 2)) {
+          ok = false;
+          break;
         }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+        const uint64_t dah = sdesc(base), dal = sdesc(base + A_TILE);
+        const uint64_t dbh = sdesc(base + 2 * A_TILE), dbl = sdesc(base + 2 * A_TILE + B_TILE);
+        // K beyond k_elems is TMA zero fill: skip the sub-steps that only see it
+        constexpr int SUB = (KROW_BYTES / ESZ) / 4;  // elements per 32-byte instruction step
+        const int rem = k_elems - kt * (KROW_BYTES / ESZ);
+        const int nsub = rem >= 4 * SUB ? 4 : (rem + SUB - 1) / SUB;
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          if (kk < nsub) {
+            const uint64_t adv = (uint64_t)((kk * 32) >> 4);  // 32 bytes of K per instruction
+            const uint32_t first = (kt == 0 && kk == 0) ? 0u : 1u;
+            umma<ESZ>(tacc, dah + adv, dbh + adv, idesc, first);
+            umma<ESZ>(tacc, dah + adv, dbl + adv, idesc, 1u);
+            umma<ESZ>(tacc, dal + adv, dbh + adv, idesc, 1u);
+          }
+        }
+        umma_commit(&empty[s]);
+        ++g;
       }
-      umma_commit(&empty[s]);
+      if (ok) umma_commit(&tmem_full[b]);
     }
-    umma_commit(tmem_full);
+    // every MMA this thread issued completes before TMEM is freed
+    umma_commit(drain);
+    mbar_drain(drain, 0);
   } else if (warp >= 2) {
     // ---------------- epilogue
     const int q = warp % 4;  // TMEM lane quarter this warp may access
-    const bool ok = mbar_wait(tmem_full, 0, abort_flag, 3);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (ok && !*abort_flag) {
-      const int row = q * 32 + lane;  // tile row of this thread
-      const int rp = m_tile * BM + row;
-      for (int c0 = 0; c0 < BN; c0 += 32) {
-        uint32_t r[32];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
-        TMEM_LD32(taddr, r);
-        asm volatile("tcgen05.wait::ld.sync.aligned;");
-        float v[32];
-#pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-        const int cp = n_tile * BN + c0;  // product column of v[0]
-        if (epi.mode == OUT_PACK) {
-          const int m = epi.inter == 1 ? (rp >> 1) : rp;
-          if (m < epi.M) {
-            const int64_t mbase =
-                (int64_t)bz * epi.s_b + (int64_t)(m / epi.Dm) * epi.s_m1 + (int64_t)(m % epi.Dm) * epi.s_m0;
-            if (epi.inter == 2) {
-              pack_run<ESZ, 2, 0>(v, epi, mbase, cp / 2, 0);
-              pack_run<ESZ, 2, 1>(v, epi, mbase, cp / 2, 1);
-            } else {
-              const int ri = epi.inter == 1 ? (rp & 1) : 0;
-              pack_run<ESZ, 1, 0>(v, epi, mbase, cp, ri);
-              pack_run<ESZ, 1, 16>(v, epi, mbase, cp + 16, ri);
-            }
-          }
-        } else if (epi.mode == OUT_REAL) {
-          if (rp < epi.M) {
-            const int64_t base = (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const int n = cp + j;
-              if (n < epi.N) {
-                if (epi.c_f32)
-                  st_real<float>(epi.C, base + (int64_t)n * epi.sCn, v[j], epi.accumulate);
-                else
-                  st_real<double>(epi.C, base + (int64_t)n * epi.sCn, v[j], epi.accumulate);
-              }
-            }
-          }
-        } else if (epi.mode == OUT_COLS_CPLX) {
-          if (rp < epi.M) {
-            const int64_t base = (int64_t)bz * epi.sCb + (int64_t)rp * epi.sCm;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int n = cp / 2 + j;
-              if (n < epi.N) {
-                if (epi.c_f32)
-                  st_cplx<float2>(epi.C, base + (int64_t)n * epi.sCn, v[2 * j], v[2 * j + 1], epi.accumulate);
-                else
-                  st_cplx<double2>(epi.C, base + (int64_t)n * epi.sCn, v[2 * j], v[2 * j + 1], epi.accumulate);
-              }
-            }
-          }
-        } else {
-          // rows interleave re/im: lanes (2i, 2i+1) hold (re, im) of complex row rp/2
-          const bool even = (lane & 1) == 0;
-          float mine[16], got[16];
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const float send = even ? v[16 + j] : v[j];
-            got[j] = __shfl_xor_sync(0xffffffffu, send, 1);
-            mine[j] = even ? v[j] : v[16 + j];
-          }
-          const int m = rp >> 1;
-          if (m < epi.M) {
-            const int64_t base = (int64_t)bz * epi.sCb + (int64_t)m * epi.sCm;
-            const int nb = cp + (even ? 0 : 16);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int n = nb + j;
-              if (n < epi.N) {
-                const float re = even ? mine[j] : got[j], im = even ? got[j] : mine[j];
-                if (epi.c_f32)
-                  st_cplx<float2>(epi.C, base + (int64_t)n * epi.sCn, re, im, epi.accumulate);
-                else
-                  st_cplx<double2>(epi.C, base + (int64_t)n * epi.sCn, re, im, epi.accumulate);
-              }
-            }
-          }
-        }
-      }
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      const uint32_t use = (uint32_t)(i >> 1);
+      if (!mbar_wait(&tmem_full[b], use & 1, abort_flag, 3)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      if (*abort_flag) break;
+      int m_tile, n_tile, bz;
+      tile_coords(t, mt, nt, m_fast, m_tile, n_tile, bz);
+      epilogue_tile<ESZ>(epi, tmem + (uint32_t)(b * TMEM_COLS), q, lane, m_tile, n_tile, bz);
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tmem_empty[b]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TMEM_COLS));
   }
 }
 
@@ -724,12 +813,20 @@ static cudaError_t launch_split(const SplitPacked& A, const SplitPacked& B, int 
   const int64_t kstep = KROW_BYTES / ESZ;
   const int64_t mt = ceil_div(A.rows, BM), nt = ceil_div(B.rows, BN);
   // walk the smaller operand's tiles fastest (packed rows per batch decide)
-  const int m_fast = (A.rows <= B.rows && mt > 1 && nt <= 65535) ? 1 : 0;
-  if ((m_fast ? mt : nt) > 0x7fffffff || (m_fast ? nt : mt) > 65535 || batch > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)(m_fast ? mt : nt), (unsigned)(m_fast ? nt : mt), (unsigned)batch);
+  const int m_fast = (A.rows <= B.rows && mt > 1) ? 1 : 0;
+  const int64_t ntiles = mt * nt * (int64_t)batch;
+  if (ntiles > 0x7fffffff) return cudaErrorInvalidValue;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  const int grid = (int)std::min<int64_t>(ntiles, sms);  // one persistent CTA per SM
   count_launch();
   split_gemm_kernel<ESZ><<<grid, THREADS, SMEM_BYTES, st>>>(tAh, tAl, tBh, tBl, epi, (int)ceil_div(A.kext, kstep),
-                                                            (int)A.kext, A.nb > 1 ? 1 : 0, B.nb > 1 ? 1 : 0, m_fast);
+                                                            (int)A.kext, A.nb > 1 ? 1 : 0, B.nb > 1 ? 1 : 0, m_fast,
+                                                            (int)mt, (int)nt, (int)ntiles);
   return cudaGetLastError();
 }
 
