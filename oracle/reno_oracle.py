@@ -650,6 +650,71 @@ def site_expectations(mps: OMps, site_ops: dict):
     return out
 
 
+def calc_1site_rdm(mps: OMps):
+    """mps.py:1547-1598: rho_i[p, q] = sum L[a, a'] conj(ms[a, p, b]) R[b, b'] ms[a', q, b']
+    with the overlap (identity-MPO) environments on both sides."""
+    n = len(mps)
+    conj = [m.conj() for m in mps.ms]
+    eye = [np.eye(m.shape[1]).reshape(1, m.shape[1], m.shape[1], 1) for m in mps.ms]
+    left = [np.ones((1, 1, 1))]
+    for i in range(n - 1):
+        left.append(contract_one_site(left[-1], mps.ms[i], eye[i], "L", ms_conj=conj[i]))
+    right = [None] * (n + 1)
+    right[n] = np.ones((1, 1, 1))
+    for i in range(n - 1, 0, -1):
+        right[i] = contract_one_site(right[i + 1], mps.ms[i], eye[i], "R", ms_conj=conj[i])
+    rdm = {}
+    for i, ms in enumerate(mps.ms):
+        lt = left[i].reshape(left[i].shape[0], left[i].shape[-1])
+        rt = right[i + 1].reshape(right[i + 1].shape[0], right[i + 1].shape[-1])
+        t = np.tensordot(lt, ms.conj(), ([0], [0]))
+        t = np.tensordot(t, rt, ([-1], [0]))
+        rdm[i] = np.tensordot(t, ms, ([0, -1], [0, -1]))
+    return rdm
+
+
+def calc_bond_singular_values(mps: OMps):
+    """mps.py:1759-1772 with compress(temp_m_trunc=inf, ret_s=True) (mp.py:437-511):
+    right-canonicalise a copy, then an untruncated SVD sweep to the right with
+    sigma moved into the next site; the per-bond sigma lists (globally sorted,
+    svd_qn.py:231-239) padded with zeros to a rectangle."""
+    m = mps.copy()
+    m.move_qnidx(len(m) - 1)
+    m.to_right = False
+    m.canonicalise()
+    s_list = []
+    for idx in m.iter_idx_list(full=False):
+        qnbigl, qnbigr, _ = m._get_big_qn([idx])
+        u, sigma, qnlset, v, _, qnrset = svd_qn(m.ms[idx], qnbigl, qnbigr, m.qntot, system="L", full_matrices=False)
+        s_list.append(np.asarray(sigma))
+        vt = np.einsum("i,ij->ij", sigma, v.T)
+        m._update_ms(idx, u, vt, qnlset=qnlset, qnrset=qnrset)
+    m._switch_direction()
+    width = max(len(x) for x in s_list)
+    return np.array([np.pad(x, (0, width - len(x))) for x in s_list])
+
+
+def calc_vn_entropy(p):
+    """utils/utils.py:41-48"""
+    p = np.asarray(p, dtype=float)
+    p = p / p.sum()
+    p = p[p > 0]
+    return float(-(p * np.log(p)).sum())
+
+
+def calc_bond_entropy(mps: OMps, s_array=None):
+    """mps.py:1774-1793"""
+    if s_array is None:
+        s_array = calc_bond_singular_values(mps)
+    return np.array([calc_vn_entropy(sig ** 2) for sig in s_array])
+
+
+def expectations(mps: OMps, mpos):
+    """mps.py:527-575 with opt=False: one R-environment sweep per operator."""
+    res = np.array([expectation(mps, m) for m in mpos], dtype=complex)
+    return res.real if np.allclose(res.imag, 0) else res
+
+
 # --------------------------------------------------------------------------
 # lib/davidson/davidson.py:154-476 -- Davidson, one root (pyscf-derived)
 # --------------------------------------------------------------------------

@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import logging
 import os
+from collections import Counter
 from typing import Dict, List, Optional, Union
 
 import numpy as np
@@ -430,14 +431,17 @@ class Mps:
             self._switch_direction()
         return self
 
-    def compress(self, temp_m_trunc=None):
-        """mp.py:437-511 (SVD sweep, full_matrices=False, sigma to the next site)."""
+    def compress(self, temp_m_trunc=None, ret_s=False):
+        """mp.py:437-511 (SVD sweep, full_matrices=False, sigma to the next site).
+        ``ret_s`` also returns the per-bond singular values (all of them,
+        descending), zero-padded to a rectangle."""
         if self.to_right:
             assert self.qnidx == 0
         else:
             assert self.qnidx == self.site_num - 1
         if self.compress_config.bonddim_should_set:
             self.compress_config.set_bonddim(len(self) + 1)
+        s_list = []
         for idx in self.iter_idx_list(full=False):
             mt = self._mp[idx]
             qnbigl, qnbigr, _ = self._get_big_qn([idx], with_mat=False)
@@ -450,16 +454,18 @@ class Mps:
                     m = temp_m_trunc[idx + 1 if left else idx]
                 else:
                     m = temp_m_trunc
-                return min(int(m), len(sigma))
+                return len(sigma) if not np.isfinite(m) else min(int(m), len(sigma))
 
             if temp_m_trunc is None:
                 kcap = self.compress_config.fixed_cap(idx, left)
             elif isinstance(temp_m_trunc, (list, tuple, np.ndarray)):
-                kcap = int(temp_m_trunc[idx + 1 if left else idx])
+                kcap = temp_m_trunc[idx + 1 if left else idx]
             else:
-                kcap = int(temp_m_trunc)
+                kcap = temp_m_trunc
+            kcap = int(kcap) if kcap is not None and np.isfinite(kcap) else None
             res = svd_truncate(mt, qnbigl, qnbigr, self.qntot, keep_left=left, m_trunc_fn=m_fn,
                                full_matrices=False, kcap=kcap)
+            s_list.append(np.asarray(res.sigma))
             pd = list(mt.shape[1:-1])
             if left:
                 self._absorb_right(idx, res.right)
@@ -472,7 +478,10 @@ class Mps:
                 self.qn[idx] = res.qn
                 self.qnidx = idx - 1
         self._switch_direction()
-        return self
+        if not ret_s:
+            return self
+        width = max(len(x) for x in s_list)
+        return self, np.array([np.pad(x, (0, width - len(x))) for x in s_list])
 
     def _update_mps(self, cstruct: torch.Tensor, cidx: List[int], qnbigl, qnbigr, percent=0):
         """mp.py:651-888, one root, no OFS: QN-blocked SVD truncation of the
@@ -609,15 +618,75 @@ class Mps:
             return float(val.real)
         return val
 
-    def expectations(self, mpos: List[Mpo], self_conj: "Mps" = None) -> np.ndarray:
-        res = np.array([self.expectation(m, self_conj) for m in mpos])
-        if np.allclose(np.imag(res), 0):
-            return np.real(res)
-        return res
+    def expectations(self, mpos: List[Mpo], self_conj: "Mps" = None, opt: bool = True) -> np.ndarray:
+        """mps.py:527-575.  With ``opt`` the left and right environments of the
+        site-tensor sequences that several operators share (prefixes from the
+        left, suffixes from the right) are contracted once
+        (_construct_freq_environ / _get_freq_environ, mps.py:2103-2169; site
+        tensors are identified by content, not by a hash of it); every operator
+        then contracts only its own middle sites.  One host transfer for all
+        results."""
+        if not opt:
+            res = np.array([self.expectation(m, self_conj) for m in mpos])
+            return np.real(res) if np.allclose(np.imag(res), 0) else res
+        n = len(self)
+        conj = self_conj._mp if self_conj is not None else [t.conj().resolve_conj() for t in self._mp]
+        key_of, tensor_of = {}, {}
+        seqs = []
+        for mpo in mpos:
+            seq = []
+            for i in range(n):
+                a = np.ascontiguousarray(mpo.numpy(i))
+                k = (a.shape, a.dtype.str, a.tobytes())
+                if k not in key_of:
+                    key_of[k] = len(key_of)
+                    tensor_of[key_of[k]] = mpo[i]
+                seq.append(key_of[k])
+            seqs.append(seq)
 
-    def site_expectations(self, site_ops: Dict[int, np.ndarray]) -> Dict[int, float]:
-        """<psi|O_i|psi> for one-site operators, with left/right overlap
-        environments shared by all sites (the quantity e_occupations returns)."""
+        def freq_environ(domain):
+            counter = Counter()
+            for seq in seqs:
+                for i in range(1, len(seq) + 1):
+                    counter.update([tuple(seq[:i]) if domain == "L" else tuple(reversed(seq[-i:]))])
+            common = sorted(counter.items(), key=lambda x: (-x[1], len(x[0])))
+            chosen = []
+            for keys, cnt in common:
+                if cnt == 1 or n < len(chosen):
+                    break
+                chosen.append(keys)
+            out = {(): torch.ones((1, 1, 1), dtype=torch.float64, device=self._mp[0].device)}
+            for keys in chosen:
+                idx = len(keys) - 1 if domain == "L" else n - len(keys)
+                out[keys] = contract_one_site(out[keys[:-1]], self._mp[idx], tensor_of[keys[-1]], domain,
+                                              ms_conj=conj[idx], prec="fp64")
+            return out
+
+        def lookup(env, seq, domain, max_len):
+            it = seq if domain == "L" else list(reversed(seq))
+            keys = []
+            for k in it:
+                keys.append(k)
+                if tuple(keys) not in env or max_len < len(keys):
+                    keys.pop()
+                    break
+            i = len(keys) - 1 if domain == "L" else n - len(keys)
+            return env[tuple(keys)], i
+
+        l_env, r_env = freq_environ("L"), freq_environ("R")
+        vals = []
+        for mpo, seq in zip(mpos, seqs):
+            left, li = lookup(l_env, seq, "L", np.inf)
+            right, ri = lookup(r_env, seq, "R", n - li - 1)
+            for i in range(li + 1, ri):
+                left = contract_one_site(left, self._mp[i], mpo[i], "L", ms_conj=conj[i], prec="fp64")
+            vals.append((left.reshape(-1).to(torch.complex128) * right.reshape(-1).to(torch.complex128)).sum())
+        res = torch.stack(vals).cpu().numpy()
+        return np.real(res) if np.allclose(np.imag(res), 0) else res
+
+    def _overlap_environs(self):
+        """conj sites and the left / right environments of <psi|psi> (identity
+        MPO) at every bond: left[i] covers sites < i, right[i] sites >= i."""
         n = len(self)
         dev = self._mp[0].device
         conj = [t.conj().resolve_conj().contiguous() for t in self._mp]
@@ -630,6 +699,61 @@ class Mps:
         right[n] = torch.ones((1, 1, 1), dtype=torch.float64, device=dev)
         for i in range(n - 1, 0, -1):
             right[i] = contract_one_site(right[i + 1], self._mp[i], eye[i], "R", ms_conj=conj[i], prec="fp64")
+        return conj, left, right
+
+    def calc_1site_rdm(self, idx=None) -> Dict[int, np.ndarray]:
+        """mps.py:1547-1598: rho_i[p, q] = sum L[a, a'] conj(ms[a, p, b])
+        R[b, b'] ms[a', q, b'] from the overlap environments, three engine
+        GEMMs per site; one host transfer."""
+        n = len(self)
+        if idx is None:
+            idx = list(range(n))
+        elif isinstance(idx, (int, np.integer)):
+            idx = [int(idx)]
+        elif isinstance(idx, (list, tuple)):
+            idx = list(idx)
+        else:
+            raise AssertionError("idx must be None, an int, a list or a tuple")
+        eng = Engine.get(self._mp[0].device)
+        conj, left, right = self._overlap_environs()
+        out = []
+        for i in idx:
+            ms = self._mp[i]
+            mb, d, mk = ms.shape
+            L2 = left[i].reshape(left[i].shape[0], left[i].shape[-1])
+            R2 = right[i + 1].reshape(right[i + 1].shape[0], right[i + 1].shape[-1])
+            U = eng.matmul(L2, ms.reshape(mb, d * mk))                               # (a, (q, b'))
+            V = eng.matmul(U.reshape(L2.shape[0] * d, mk), R2.transpose(0, 1))       # ((a, q), b)
+            X = conj[i].permute(1, 0, 2).reshape(d, -1).contiguous()                 # (p, (a, b))
+            Y = V.reshape(L2.shape[0], d, R2.shape[0]).permute(1, 0, 2).reshape(d, -1).contiguous()
+            out.append(eng.matmul(X, Y.transpose(0, 1)))                             # (p, q)
+        host = [t.cpu().numpy() for t in out]
+        return {i: h for i, h in zip(idx, host)}
+
+    def calc_bond_singular_values(self) -> np.ndarray:
+        """mps.py:1759-1772: sigma at every bond from an untruncated SVD sweep
+        of a right-canonical copy, zero-padded to a rectangle."""
+        mps = self.copy()
+        mps.ensure_right_canonical()
+        _, s_array = mps.compress(temp_m_trunc=np.inf, ret_s=True)
+        return s_array
+
+    def calc_bond_entropy(self, s_array: np.ndarray = None) -> np.ndarray:
+        """mps.py:1774-1793: von Neumann entropy -sum p ln p, p = sigma^2 / sum sigma^2."""
+        if s_array is None:
+            s_array = self.calc_bond_singular_values()
+        res = []
+        for sig in s_array:
+            p = np.asarray(sig, dtype=float) ** 2
+            p = p / p.sum()
+            p = p[p > 0]
+            res.append(float(-(p * np.log(p)).sum()))
+        return np.array(res)
+
+    def site_expectations(self, site_ops: Dict[int, np.ndarray]) -> Dict[int, float]:
+        """<psi|O_i|psi> for one-site operators, with left/right overlap
+        environments shared by all sites (the quantity e_occupations returns)."""
+        conj, left, right = self._overlap_environs()
         out = {}
         vals = []
         for i, op in site_ops.items():

@@ -43,28 +43,29 @@ def mpo_from_golden(d, prefix, n):
     return [d[f"{prefix}/W_{i}"] for i in range(n)]
 
 
-def engine_chain(d, tag):
-    """The engine's Mps / Mpo from a dumped reference chain ``{tag}/init`` and
-    ``{tag}/mpo``: a model with the same local dimensions and QNs (electron
-    sites carry QN (0, 1), the others QN 0) and the dumped tensors."""
+def engine_chain(d, tag, mps_key="init", mpo_key="mpo"):
+    """The engine's Mps / Mpo from a dumped reference chain ``{tag}/{mps_key}``
+    and ``{tag}/{mpo_key}`` (None: no Mpo): a model with the same local
+    dimensions and QNs (electron sites carry QN (0, 1), the others QN 0) and
+    the dumped tensors."""
     from renormalizer_b200 import Mpo, Mps
     from renormalizer_b200.model import BasisSHO, BasisSimpleElectron, Model
-    n = int(d[f"{tag}/init/nsites"])
+    pre = f"{tag}/{mps_key}"
+    n = int(d[f"{pre}/nsites"])
     basis = []
     ie = 0
     for i in range(n):
-        sq = d[f"{tag}/init/sigmaqn_{i}"]
+        sq = d[f"{pre}/sigmaqn_{i}"]
         if sq.shape[0] == 2 and sq[1, 0] == 1:
             basis.append(BasisSimpleElectron(ie))
             ie += 1
         else:
             basis.append(BasisSHO(("ph", i), 1.0, int(sq.shape[0])))
     model = Model(basis, [])
-    sites = [d[f"{tag}/init/mt_{i}"] for i in range(n)]
-    qn = [d[f"{tag}/init/qn_{i}"] for i in range(n + 1)]
-    mps = Mps.from_arrays(model, sites, qn, int(d[f"{tag}/init/qnidx"]), d[f"{tag}/init/qntot"],
-                          bool(d[f"{tag}/init/to_right"]))
-    mpo = Mpo.from_tensors(model, [d[f"{tag}/mpo/W_{i}"] for i in range(n)])
+    sites = [d[f"{pre}/mt_{i}"] for i in range(n)]
+    qn = [d[f"{pre}/qn_{i}"] for i in range(n + 1)]
+    mps = Mps.from_arrays(model, sites, qn, int(d[f"{pre}/qnidx"]), d[f"{pre}/qntot"], bool(d[f"{pre}/to_right"]))
+    mpo = Mpo.from_tensors(model, [d[f"{tag}/{mpo_key}/W_{i}"] for i in range(n)]) if mpo_key else None
     return mps, mpo
 
 

@@ -347,6 +347,43 @@ def gen_dmrg(out):
     np.savez_compressed(out / "dmrg_cases.npz", **cases)
 
 
+def gen_obs(out):
+    """calc_1site_rdm, calc_bond_singular_values / calc_bond_entropy and
+    expectations (the shared-environment path) of an entangled complex MPS:
+    a 3-molecule two-mode Holstein chain after 4 TDVP-PS2 steps."""
+    from renormalizer.mps import Mps, Mpo
+    from renormalizer.model import Op
+    from renormalizer.utils import EvolveConfig, EvolveMethod, CompressConfig, CompressCriteria
+    cases = {}
+    np.random.seed(77)
+    model = _holstein(3, 4, [(1.0, 1.0), (0.5, 0.7)])
+    mpo = Mpo(model)
+    mps = Mps.hartree_product_state(model, {0: 1})
+    mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=10)
+    mps = mps.expand_bond_dimension(mpo, include_ex=False)
+    mps.evolve_config = EvolveConfig(EvolveMethod.tdvp_ps2)
+    for _ in range(4):
+        mps = mps.evolve(mpo, 0.1)
+    _dump_mps("obs/mps", mps, cases)
+    rdm = mps.calc_1site_rdm()
+    for i in range(len(mps)):
+        cases[f"obs/rdm_{i}"] = np.asarray(rdm[i])
+    s_array = mps.calc_bond_singular_values()
+    cases["obs/bond_sv"] = np.asarray(s_array)
+    cases["obs/bond_entropy"] = np.asarray(mps.calc_bond_entropy(s_array))
+    # operators sharing prefixes / suffixes: every electronic occupation, the
+    # Hamiltonian, and one phonon coordinate
+    e_dofs = model.e_dofs
+    ops = [Mpo(model, Op(r"a^\dagger a", d)) for d in e_dofs] + [mpo]
+    ops.append(Mpo(model, Op("x", model.v_dofs[0])))
+    for k, m in enumerate(ops):
+        _dump_mpo(f"obs/op{k}", m, cases)
+    cases["obs/nops"] = np.array(len(ops))
+    cases["obs/expectations"] = np.asarray(mps.expectations(ops))
+    cases["obs/expectations_naive"] = np.asarray(mps.expectations(ops, opt=False))
+    np.savez_compressed(out / "obs_cases.npz", **cases)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -354,7 +391,7 @@ def main():
     args = ap.parse_args()
     _import_reference(args.reference)
     gens = dict(heff=gen_heff, env=gen_env, krylov=gen_krylov, svd=gen_svd, mpo=gen_mpo, tdvp=gen_tdvp,
-                dmrg=gen_dmrg)
+                dmrg=gen_dmrg, obs=gen_obs)
     for name, fn in gens.items():
         if args.only and name not in args.only.split(","):
             continue
