@@ -253,8 +253,7 @@ static bool fused2_eligible(const reno_heff_desc* d) {
   if (d->nsite != 2 || d->prec == RENO_PREC_FP64 || d->mpo_dtype != RENO_F64) return false;
   const bool allc = d->env_dtype == RENO_C128 && d->psi_dtype == RENO_C128;
   const bool allr = d->env_dtype == RENO_F64 && d->psi_dtype == RENO_F64;
-  // grid.z of S2 / S3 is the batch (ml, ml * d1)
-  return (allc || allr) && (int64_t)d->ml * d->d1 <= 65535;
+  return allc || allr;
 }
 
 static Fused2 fused2_layout(const reno_heff_desc* d, char* base) {
@@ -342,9 +341,97 @@ static cudaError_t fused2_run(const reno_heff_desc* d, const Fused2& f, const vo
   return e;
 }
 
+// ---------------------------------------------------------------- fused split 1-site matvec
+// The 2-site chain without its middle stage:
+//   S1  T1 = L . psi      N order (k, e): e runs along S2's K = (b, e)
+//   S2  T2 = Wt . T1[a]   written as S3's A ([re | im] along K = (f, k))
+//   S3  y  = T2 . R^T     FP64 output
+struct Fused1 {
+  SplitPacked s1a, s1b, s2a, s2b, s3a, s3b;
+  size_t bytes;
+};
+
+static bool fused1_eligible(const reno_heff_desc* d) {
+  if (d->nsite != 1 || d->prec == RENO_PREC_FP64 || d->mpo_dtype != RENO_F64) return false;
+  const bool allc = d->env_dtype == RENO_C128 && d->psi_dtype == RENO_C128;
+  const bool allr = d->env_dtype == RENO_F64 && d->psi_dtype == RENO_F64;
+  return allc || allr;
+}
+
+static Fused1 fused1_layout(const reno_heff_desc* d, char* base) {
+  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wr = d->wr, dd = d->d1;
+  const bool c = d->env_dtype == RENO_C128;
+  const int pr = d->prec;
+  const int64_t x2 = c ? 2 : 1;
+  struct Spec { int64_t rows, kext, nb; int mode; };
+  const Spec s1a{x2 * ml * wl, x2 * ml, 1, c ? SPLIT_DBL_CPLX : SPLIT_REAL};
+  const Spec s1b{dd * mr, x2 * ml, 1, c ? SPLIT_CAT : SPLIT_REAL};
+  const Spec s2a{dd * wr, wl * dd, 1, SPLIT_REAL};
+  const Spec s2b{x2 * mr, wl * dd, ml, c ? SPLIT_DBL_SPLIT : SPLIT_REAL};
+  const Spec s3a{ml * dd, x2 * wr * mr, 1, c ? SPLIT_CAT : SPLIT_REAL};
+  const Spec s3b{x2 * mr, x2 * wr * mr, 1, c ? SPLIT_DBL_CPLX : SPLIT_REAL};
+  auto sz = [&](const Spec& q) { return split_packed_bytes(q.rows, q.kext, q.nb, pr); };
+  auto at = [&](size_t off, const Spec& q) {
+    return split_packed_at(base ? base + off : nullptr, q.rows, q.kext, q.nb, q.mode, pr);
+  };
+  Fused1 f{};
+  size_t off = 0;
+  f.s1a = at(off, s1a);
+  off = align256(off + sz(s1a));
+  f.s2a = at(off, s2a);
+  off = align256(off + sz(s2a));
+  f.s3b = at(off, s3b);
+  off = align256(off + sz(s3b));
+  // region P: psi packed (S1's B), later S3's A; region Q: S2's B
+  const size_t P = off;
+  off = align256(off + std::max(sz(s1b), sz(s3a)));
+  const size_t Q = off;
+  off = align256(off + sz(s2b));
+  f.s1b = at(P, s1b);
+  f.s3a = at(P, s3a);
+  f.s2b = at(Q, s2b);
+  f.bytes = off;
+  return f;
+}
+
+static cudaError_t fused1_run(const reno_heff_desc* d, const Fused1& f, const void* L, const void* Wt,
+                              const void* R, const void* psi, void* y, cudaStream_t st) {
+  const int64_t ml = d->ml, mr = d->mr, wl = d->wl, wr = d->wr, dd = d->d1;
+  const int ev = d->env_dtype, pv = d->psi_dtype, pr = d->prec;
+  const int64_t x2 = ev == RENO_C128 ? 2 : 1;
+  cudaError_t e = split_pack(opnd(L, ev, ml, 1), (int)(ml * wl), (int)ml, 1, SplitRows{}, f.s1a, pr, st);
+  // psi rows in (k, e) order: e at stride mr, k at 1; K = c at dd*mr
+  SplitRows ke;
+  ke.D0 = (int)dd;
+  ke.D1 = (int)mr;
+  ke.s_r1 = 1;
+  ke.s_r2 = 0;
+  if (e == cudaSuccess) e = split_pack(opnd(psi, pv, mr, dd * mr), (int)(dd * mr), (int)ml, 1, ke, f.s1b, pr, st);
+  if (e == cudaSuccess)
+    e = split_pack(opnd(Wt, RENO_F64, wl * dd, 1), (int)(dd * wr), (int)(wl * dd), 1, SplitRows{}, f.s2a, pr, st);
+  if (e == cudaSuccess)
+    e = split_pack(opnd(R, ev, wr * mr, 1), (int)mr, (int)(wr * mr), 1, SplitRows{}, f.s3b, pr, st);
+  if (e != cudaSuccess) return e;
+  // S1: rows (a, b) of L, columns (k, e) -> S2's B[a][k re/im][(b, e)]
+  SplitPackOut o1{f.s2b.hi, f.s2b.lo, 0, f.s2b.rows * f.s2b.pitch, dd, x2 * f.s2b.pitch, 1, f.s2b.pitch,
+                  (int)wl, (int)dd};
+  e = split_run(f.s1a, f.s1b, (int)(ml * wl), (int)(dd * mr), 1, nullptr, &o1, pr, st);
+  // S2 (batch a): rows (d', f), columns k -> S3's A[(a, d')][re/im | (f, k)]
+  SplitPackOut o2{f.s3a.hi, f.s3a.lo, dd * f.s3a.pitch, f.s3a.pitch, mr, 0, 1, wr * mr, (int)wr, (int)mr};
+  if (e == cudaSuccess) e = split_run(f.s2a, f.s2b, (int)(dd * wr), (int)mr, (int)ml, nullptr, &o2, pr, st);
+  // S3: y[(a, d'), l] = T2 . R^T
+  GemmParams out;
+  out.C = y;
+  out.sCm = mr;
+  out.sCn = 1;
+  if (e == cudaSuccess) e = split_run(f.s3a, f.s3b, (int)(ml * dd), (int)mr, 1, &out, nullptr, pr, st);
+  return e;
+}
+
 static size_t heff_total(const reno_heff_desc* d) {
   const HeffLayout lay = heff_layout(d);
   if (fused2_eligible(d)) return lay.off_t1 + fused2_layout(d, nullptr).bytes;
+  if (fused1_eligible(d)) return lay.off_t1 + fused1_layout(d, nullptr).bytes;
   char* nul = nullptr;
   return lay.off_split + align256(split_need(heff_stages(d, lay, nul, nullptr, nullptr, nullptr, nullptr)));
 }
@@ -368,6 +455,15 @@ extern "C" int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* d, const voi
     return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply: null tensor pointer");
   const HeffLayout lay = heff_layout(d);
   char* w = static_cast<char*>(ws);
+  if (fused1_eligible(d)) {
+    const Fused1 f = fused1_layout(d, w ? w + lay.off_t1 : nullptr);
+    if (ws_bytes < lay.off_t1 + f.bytes || !ws)
+      return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heff_apply: workspace too small");
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = launch_wt(W1, w + lay.off_wt1, d->mpo_dtype, d->wl, d->d1, d->wr, 0, st);
+    if (e == cudaSuccess) e = fused1_run(d, f, L, w + lay.off_wt1, R, psi, y, st);
+    return check_cuda(ctx, e, "reno_heff_apply");
+  }
   if (fused2_eligible(d)) {
     const Fused2 f = fused2_layout(d, w ? w + lay.off_t1 : nullptr);
     if (ws_bytes < lay.off_t1 + f.bytes || !ws)

@@ -24,8 +24,8 @@ The MPO enters as W(g) = W(g0) + sum_j (g_j - g0_j) dW/dg_j with dW/dg_j from
 the MPO builder at g0 +- e_j (exact: the Holstein MPO is at most quadratic
 in a coupling), so W(g0) is the MPO itself and the gradient at g0 is exact.
 
-``contract="einsum"`` runs the same trajectory on torch.tensordot / einsum in
-FP64 (torch's own autograd everywhere): the reference gradient the engine's
+``contract="einsum"`` runs the same trajectory on torch.tensordot in FP64
+(torch's own autograd everywhere): the reference gradient the engine's
 is checked against, together with central finite differences.
 """
 from __future__ import annotations
@@ -37,9 +37,6 @@ import torch
 from torch.utils.checkpoint import checkpoint
 
 from .autodiff import heff, tensordot
-
-_EINSUM = {0: "abc,lbk,ck->al", 1: "abc,bdef,lfk,cek->adl"}
-
 
 class Contract(torch.autograd.Function):
     """c = tensordot(a, b, (ia, ib)) on the engine GEMM; backward: grad_a =
@@ -88,8 +85,15 @@ class _Ops:
     def hop(self, psi, L, Ws, R):
         if self.kind == "engine":
             return heff(psi, L, Ws, R, prec="fp64")
-        dt = torch.complex128
-        return torch.einsum(_EINSUM[len(Ws)], L.to(dt), *[w.to(dt) for w in Ws], R.to(dt), psi.to(dt))
+        # the hop_expr contraction in an explicit pairwise order (torch.einsum
+        # without a path optimiser would form an (M d)^2 M^2 intermediate)
+        c = lambda t: t.to(torch.complex128)
+        if not Ws:                                                      # abc, lbk, ck -> al
+            t = torch.tensordot(c(L), c(psi), dims=([2], [0]))          # a b k
+            return torch.tensordot(t, c(R), dims=([1, 2], [1, 2]))      # a l
+        t = torch.tensordot(c(L), c(psi), dims=([2], [0]))              # a b e k
+        t = torch.tensordot(t, c(Ws[0]), dims=([1, 2], [0, 2]))         # a k d f
+        return torch.tensordot(t, c(R), dims=([3, 1], [1, 2]))          # a d l
 
     def env_L(self, E, ms, W):
         """lib.py:200-205: L'[f,g,h] = sum E[a,b,c] conj(ms[a,d,f]) W[b,d,e,g] ms[c,e,h]"""

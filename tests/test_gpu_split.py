@@ -115,6 +115,24 @@ def test_split_heff_2site_fused_shapes(prec, cplx, ml, mr, d1, d2, wl, wm, wr):
     assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
 
 
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("cplx", [True, False])
+@pytest.mark.parametrize("ml,mr,d,wl,wr", [(64, 48, 16, 5, 4), (48, 40, 2, 4, 5), (33, 17, 3, 3, 2),
+                                           (256, 256, 16, 5, 5)])
+def test_split_heff_1site_fused_shapes(prec, cplx, ml, mr, d, wl, wr):
+    """the fused 1-site chain: phonon and electron sites, ragged bonds, the
+    real (DMRG) form, the workload's M = 256 phonon site"""
+    from renormalizer_b200.hop_expr import HeffOperator
+    rng = np.random.default_rng(ml + d)
+    mk = lambda s: rng.standard_normal(s) + (1j * rng.standard_normal(s) if cplx else 0)
+    L, R, psi = mk((ml, wl, ml)), mk((mr, wr, mr)), mk((ml, d, mr))
+    W = rng.standard_normal((wl, d, d, wr))
+    ref = O.hop(L, [W], R, psi)
+    y = HeffOperator(L, R, [W], psi.shape, prec=prec)(torch.from_numpy(psi).cuda()).cpu().numpy()
+    assert y.dtype == ref.dtype
+    assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
+
+
 @pytest.mark.parametrize("prec,atol", [("bf16x3", 2e-5), ("tf32x3", 2e-6)])
 def test_split_tdvp_short_trajectory(prec, atol):
     from renormalizer_b200 import EvolveConfig, EvolveMethod, backend
