@@ -547,9 +547,11 @@ def run_grad(args):
     """16 molecules x (e, one mode omega = 1, 10 levels), J = 1, g_i ~ U(0.5, 1.5)
     (seed 5), exciton on molecule 0, bonds expanded to M = 64, 1-site TDVP-PS,
     50 steps of dt = 0.05 (t = 2.5), checkpoints every 10 steps.  Times the
-    engine gradient; checks it against torch autograd through FP64 einsum on
-    the same device and against central differences (h = 1e-5) for two
-    couplings."""
+    engine gradient; checks it against torch autograd through FP64 tensordot
+    on the same device and against central differences (h = 1e-5 and 1e-3)
+    for the two largest couplings.  The trajectory itself carries ~1e-9 of
+    rounding amplification (the bond-expansion directions of the start state
+    are set by rounding), which bounds both checks."""
     import torch
     from renormalizer_b200 import CompressConfig, CompressCriteria, HolsteinModel, Mol, Mpo, Mps, Phonon, Quantity, \
         backend
@@ -582,18 +584,19 @@ def run_grad(args):
     torch.cuda.synchronize()
     t_einsum = time.time() - t0
     fd = {}
-    for j in (0, nmol - 1):
-        e = np.zeros(nmol)
-        e[j] = 1e-5
-        fp = trajectory_value(build(g0 + e), sites0, dt, nsteps, 0, op, krylov=8)
-        fm = trajectory_value(build(g0 - e), sites0, dt, nsteps, 0, op, krylov=8)
-        fd[j] = (fp - fm) / 2e-5
+    for j in (0, 1):
+        for h in (1e-5, 1e-3):
+            e = np.zeros(nmol)
+            e[j] = h
+            fp = trajectory_value(build(g0 + e), sites0, dt, nsteps, 0, op, krylov=8)
+            fm = trajectory_value(build(g0 - e), sites0, dt, nsteps, 0, op, krylov=8)
+            fd[f"g{j}_h{h:g}"] = {"fd": (fp - fm) / (2 * h), "grad": float(grad[j]),
+                                 "rel_diff": abs((fp - fm) / (2 * h) - grad[j]) / abs(grad[j])}
     print(json.dumps({"metric": "d <n_0>(t=2.5) / d g_i through TDVP-PS (16-molecule Holstein, M=64, 50 steps)",
                       "value": t_grad, "unit": "s per gradient (16 couplings)", "population": val,
                       "gradient": grad.tolist(), "einsum_reference_s": t_einsum,
                       "max_rel_diff_vs_einsum_autograd": float(np.abs(grad - grad_e).max() / np.abs(grad_e).max()),
-                      "finite_differences": {str(j): {"fd": v, "grad": float(grad[j]), "abs_diff": abs(v - grad[j])}
-                                             for j, v in fd.items()},
+                      "population_vs_einsum": abs(val - val_e), "finite_differences": fd,
                       "checkpoint_every": 10, "krylov_vectors": 8}), flush=True)
 
 

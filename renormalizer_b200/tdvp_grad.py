@@ -110,8 +110,11 @@ class _Ops:
 
 def expm_krylov_fixed(apply: Callable, dt: complex, v: torch.Tensor, k: int) -> torch.Tensor:
     """exp(dt A) v from k Lanczos vectors (three-term recurrence as in
-    krylov.py:27-84, fixed length; stops early only on an exact breakdown)."""
+    krylov.py:27-84, fixed length; stops early on the reference's breakdown
+    test beta < 100 n eps, krylov.py:72-74, which also bounds the local
+    Krylov space by the local dimension)."""
     nrm = torch.linalg.vector_norm(v)
+    tiny = 100 * v.numel() * np.finfo(np.float64).eps
     Q = [v / nrm]
     alphas, betas = [], []
     for j in range(k):
@@ -124,7 +127,7 @@ def expm_krylov_fixed(apply: Callable, dt: complex, v: torch.Tensor, k: int) -> 
         if j == k - 1:
             break
         b = torch.linalg.vector_norm(w)
-        if float(b.detach()) < 1e-13 * max(1.0, float(nrm.detach())):
+        if float(b.detach()) < tiny:
             break
         betas.append(b)
         Q.append(w / b)

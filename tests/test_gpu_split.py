@@ -19,6 +19,14 @@ HEFF = load_golden("heff_cases.npz")
 ENV = load_golden("env_cases.npz")
 
 
+def _chain_tol(prec, ks):
+    """bound for a chain of split GEMMs relative to max|y|: 4 x the per-GEMM
+    TOL, grown with sqrt(K / 256) for the longest contraction -- beyond a
+    few hundred terms the FP32 accumulation, not the hi/lo split, sets the
+    error (which is why TF32x3 is then no more accurate than BF16x3)"""
+    return 4 * TOL[prec] * max(1.0, np.sqrt(max(ks) / 256.0))
+
+
 def _eng():
     from renormalizer_b200._native import Engine
     return Engine.get(0)
@@ -112,7 +120,7 @@ def test_split_heff_2site_fused_shapes(prec, cplx, ml, mr, d1, d2, wl, wm, wr):
     op = HeffOperator(L, R, [W1, W2], psi.shape, prec=prec)
     y = op(torch.from_numpy(psi).cuda()).cpu().numpy()
     assert y.dtype == ref.dtype
-    assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
+    assert np.abs(y - ref).max() / np.abs(ref).max() < _chain_tol(prec, [2 * ml, wl * d1, wm * d2, 2 * wr * mr])
 
 
 @pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
@@ -130,7 +138,7 @@ def test_split_heff_1site_fused_shapes(prec, cplx, ml, mr, d, wl, wr):
     ref = O.hop(L, [W], R, psi)
     y = HeffOperator(L, R, [W], psi.shape, prec=prec)(torch.from_numpy(psi).cuda()).cpu().numpy()
     assert y.dtype == ref.dtype
-    assert np.abs(y - ref).max() / np.abs(ref).max() < 4 * TOL[prec]
+    assert np.abs(y - ref).max() / np.abs(ref).max() < _chain_tol(prec, [2 * ml, wl * d, 2 * wr * mr])
 
 
 @pytest.mark.parametrize("prec,atol", [("bf16x3", 2e-5), ("tf32x3", 2e-6)])
