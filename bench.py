@@ -347,6 +347,17 @@ def fp64_peak_tflops(dev):
     return best
 
 
+def reduce_max_ms(t_ms: float, dist, device) -> float:
+    """The multi-GPU timing rule: every rank's device time, max over ranks
+    (one all-reduce; identity without a process group)."""
+    if dist is None:
+        return float(t_ms)
+    import torch
+    tt = torch.tensor([float(t_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def run_engine(args, rank, world, dist):
     import torch
     from renormalizer_b200 import Mpo, backend
@@ -392,11 +403,7 @@ def run_engine(args, rank, world, dist):
                          "oversample": svdmod.subspace.oversample, "rtol": svdmod.subspace.rtol}}
     timer.uninstall()
     phases.uninstall()
-    t_ms = s_ev.elapsed_time(e_ev)
-    if dist is not None:
-        tt = torch.tensor([t_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+    t_ms = reduce_max_ms(s_ev.elapsed_time(e_ev), dist, dev)
     value = world * args.steps / (t_ms * 1e-3)
     fl, heff_ms, nheff = timer.result()
     kry_timed = mps.evolve_config.stat
@@ -417,11 +424,7 @@ def run_engine(args, rank, world, dist):
             pops = m.e_occupations
         e2.record()
         barrier()
-        te = s2.elapsed_time(e2)
-        if dist is not None:
-            tt = torch.tensor([te], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = reduce_max_ms(s2.elapsed_time(e2), dist, dev)
         e2e = {"value": world * ne2e / (te * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(pops.size * 8)}
 
