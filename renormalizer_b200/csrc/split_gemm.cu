@@ -9,12 +9,13 @@
 // so each complex GEMM is ONE real GEMM whose rows (or columns) interleave the
 // real and imaginary parts of the result.
 //
-// Pipeline (one 128 x 256 output tile per CTA, 6 warps):
+// Pipeline (persistent: one CTA per SM walks 128 x 256 output tiles; 10 warps):
 //   warp 0     TMA producer: 4 tiles per stage (A_hi, A_lo, B_hi, B_lo),
 //              128-byte swizzled K-major boxes, mbarrier complete_tx
 //   warp 1     TMEM allocator + single-thread tcgen05.mma issuer: 3 products
 //              per stage, tcgen05.commit frees the stage
-//   warps 2-5  epilogue: tcgen05.ld 32x32b from TMEM, strided writes of the
+//   warps 2-9  epilogue (two warps per TMEM lane quarter, half the columns
+//              each): tcgen05.ld 32x32b from TMEM, strided writes of the
 //              (interleaved complex) output as FP64, or as FP32 when the
 //              output only feeds the next split stage (the accumulator is
 //              FP32, so nothing is lost) -- the operands A, B are FP64 or
@@ -29,7 +30,8 @@
 namespace reno {
 namespace split {
 
-constexpr int BM = 128, BN = 256, STAGES = 2, THREADS = 192;
+constexpr int BM = 128, BN = 256, STAGES = 2, THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int EPI_WARPS = 8;
 constexpr int KROW_BYTES = 128;  // one SW128 row of K per stage
 constexpr int A_TILE = BM * KROW_BYTES;   // 16 KB
 constexpr int B_TILE = BN * KROW_BYTES;   // 32 KB
@@ -244,15 +246,16 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
         "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])     \
       : "r"(taddr))
 
-// Epilogue of one output tile: TMEM columns [tacc, tacc + BN) -> registers
+// Epilogue of columns [c_begin, c_end) of one output tile: TMEM -> registers
 // (32 columns at a time) -> the output in the Epi mode.  Warp w reads TMEM
-// lane quarter q = w % 4, i.e. tile rows q*32 .. q*32+31.
+// lane quarter q = w % 4, i.e. tile rows q*32 .. q*32+31; two warps share a
+// quarter, each taking half of the BN columns.
 template <int ESZ>
 __device__ __forceinline__ void epilogue_tile(const Epi& epi, uint32_t tacc, int q, int lane, int m_tile, int n_tile,
-                                              int bz) {
+                                              int bz, int c_begin, int c_end) {
   const int row = q * 32 + lane;  // tile row of this thread
   const int rp = m_tile * BM + row;
-  for (int c0 = 0; c0 < BN; c0 += 32) {
+  for (int c0 = c_begin; c0 < c_end; c0 += 32) {
     uint32_t r[32];
     const uint32_t taddr = tacc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
     TMEM_LD32(taddr, r);
@@ -371,7 +374,7 @@ __device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity) {
 // overlaps the next tile's TMA + MMA mainloop.  The smem stage ring runs on
 // across tiles.  Barriers: full / empty (TMA <-> MMA, per stage), tmem_full
 // (MMA -> epilogue, per buffer, tcgen05.commit), tmem_empty (epilogue -> MMA,
-// per buffer, one arrive per epilogue warp), drain (the MMA thread's last
+// per buffer, one arrive per epilogue warp, 8 warps), drain (the MMA thread's last
 // commit, waited for before TMEM is freed).
 template <int ESZ>
 __global__ void __launch_bounds__(THREADS, 1)
@@ -398,7 +401,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tmem_full[b], 1);
-      mbar_init(&tmem_empty[b], 4);
+      mbar_init(&tmem_empty[b], EPI_WARPS);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -492,7 +495,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     mbar_drain(drain, 0);
   } else if (warp >= 2) {
     // ---------------- epilogue
-    const int q = warp % 4;  // TMEM lane quarter this warp may access
+    const int q = warp % 4;                      // TMEM lane quarter this warp may access
+    const int c_begin = ((warp - 2) / 4) * (BN / 2);  // warps 2-5: columns [0, BN/2), warps 6-9: the rest
     int i = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
       const int b = i & 1;
@@ -502,7 +506,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (*abort_flag) break;
       int m_tile, n_tile, bz;
       tile_coords(t, mt, nt, m_fast, m_tile, n_tile, bz);
-      epilogue_tile<ESZ>(epi, tmem + (uint32_t)(b * TMEM_COLS), q, lane, m_tile, n_tile, bz);
+      epilogue_tile<ESZ>(epi, tmem + (uint32_t)(b * TMEM_COLS), q, lane, m_tile, n_tile, bz, c_begin,
+                         c_begin + BN / 2);
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
       if (lane == 0) mbar_arrive(&tmem_empty[b]);
