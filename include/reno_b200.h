@@ -25,6 +25,7 @@
  *                         svd_qn.py:89-96 blockrecover, lib.py:302-316
  *                         select_basis column copy
  *  - reno_heff_diag    <- renormalizer/mps/gs.py:419-445 hdiag einsums
+ *  - reno_heff_backward   (no counterpart: gradients of the matvec)
  */
 #ifndef RENO_B200_H
 #define RENO_B200_H
@@ -138,6 +139,25 @@ int reno_heff_apply_noalloc(reno_ctx* ctx, const reno_heff_desc* desc,
 int reno_heff_diag(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
                    const void* W1, const void* W2, const void* R,
                    double* hdiag);
+
+/* Reverse mode of reno_heff_apply.  No counterpart in the reference (it has
+ * no gradients): for y = H_eff psi (hop_expr.py:57-103) and gy the gradient
+ * with respect to y (torch's convention for complex tensors), writes
+ *   gpsi = the matvec with conjugate-transposed L, W and R applied to gy
+ *          (desc->prec, the fused split chains included);
+ *   gL, gR, gW1, gW2 = contractions of gy with the conjugates of the other
+ *          operands (FP64), each in the operand's own shape.
+ * Every output pointer may be NULL (not computed).  Outputs are complex128
+ * when any operand is complex, float64 otherwise (a caller holding a real
+ * operand takes the real part).  gy has the type of y.  The workspace holds
+ * the permuted operand copies and contraction intermediates; its size comes
+ * from reno_heff_backward_workspace_bytes. */
+int reno_heff_backward_workspace_bytes(const reno_heff_desc* desc, size_t* bytes);
+int reno_heff_backward(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
+                       const void* W1, const void* W2, const void* R,
+                       const void* psi, const void* gy, void* gpsi, void* gL,
+                       void* gW1, void* gW2, void* gR, void* ws,
+                       size_t ws_bytes);
 
 /* ------------------------------------------------------------------------
  * Environment update, lib.py:169-250 contract_one_site (3-leg site tensors).

@@ -52,6 +52,9 @@ _SIGS = {
     "reno_device_error": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
     "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),
+    "reno_heff_backward_workspace_bytes": (_c_int, [ctypes.POINTER(HeffDesc), ctypes.POINTER(_c_sz)]),
+    "reno_heff_backward": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                    _vp, _vp, _c_sz]),
     "reno_env_workspace_bytes": (_c_int, [ctypes.POINTER(EnvDesc), ctypes.POINTER(_c_sz)]),
     "reno_env_update": (_c_int, [_vp, ctypes.POINTER(EnvDesc), _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
     "reno_vec_workspace_bytes": (_c_int, [_c_i64, ctypes.POINTER(_c_sz)]),
@@ -225,6 +228,17 @@ class Engine:
         self.check(self.lib.reno_heff_apply(self.ctx, ctypes.byref(desc), ptr(L), ptr(W1), ptr(W2), ptr(R), ptr(psi),
                                             ptr(y), ptr(ws), ws.numel()), "reno_heff_apply")
         self.launches += 1
+
+    def heff_backward(self, desc: HeffDesc, L, W1, W2, R, psi, gy, gpsi, gL, gW1, gW2, gR):
+        """reno_heff_backward: any output may be None (not computed)."""
+        n = _c_sz()
+        self.check(self.lib.reno_heff_backward_workspace_bytes(ctypes.byref(desc), ctypes.byref(n)),
+                   "reno_heff_backward_workspace_bytes")
+        ws = self.workspace(int(n.value))
+        opt = lambda t: ptr(t) if t is not None else None
+        self.check(self.lib.reno_heff_backward(self.ctx, ctypes.byref(desc), ptr(L), opt(W1), opt(W2), ptr(R), ptr(psi),
+                                               ptr(gy), opt(gpsi), opt(gL), opt(gW1), opt(gW2), opt(gR), ptr(ws),
+                                               ws.numel()), "reno_heff_backward")
 
     def device_error(self) -> int:
         """first timed-out wait of the tensor-core kernels since the last call (0 = none)"""

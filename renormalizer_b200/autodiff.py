@@ -4,16 +4,18 @@
 For y = H_eff(L, W.., R) psi, a multilinear map, the gradient with respect to
 each operand is the contraction of the upstream gradient gy with the complex
 conjugates of the other operands (torch's convention for complex tensors:
-grad_x = J^H grad_y):
+grad_x = J^H grad_y).  All of it runs in libreno_b200's reno_heff_backward:
 
 * d psi: the same matvec with L'[c,b,a] = conj L[a,b,c], W'[b,e,d,f] =
-  conj W[b,d,e,f] and R'[k,f,l] = conj R[l,f,k] applied to gy -- it runs on
-  the engine's matvec kernels (fused split chain included);
-* d L, d R, d W: fixed chains of pairwise contractions (``tensordot`` below),
-  each one GEMM on the engine's FP64 DMMA kernel after a layout permute.
+  conj W[b,d,e,f] and R'[k,f,l] = conj R[l,f,k] applied to gy, on the
+  engine's matvec kernels (fused split chain included);
+* d L, d R, d W: fixed chains of pairwise contractions, each a permute-copy
+  kernel per operand and one FP64 DMMA GEMM.
 
-Real operands (MPO tensors, DMRG environments) receive the real part.  The
-reference has no gradients; ``tests/test_autodiff.py`` checks these against
+Real operands (MPO tensors, DMRG environments) receive the real part.
+``tensordot`` below is the same contraction primitive for host-side use (the
+TDVP gradient's environment updates).  The reference has no gradients;
+``tests/test_autodiff.py`` checks these against
 torch autograd through an FP64 einsum of the same contraction and against
 central finite differences.
 """
@@ -42,76 +44,33 @@ def tensordot(a: torch.Tensor, b: torch.Tensor, axes, eng: Engine = None) -> tor
     return C.reshape([a.shape[i] for i in fa] + [b.shape[i] for i in fb])
 
 
-def _c(t: Optional[torch.Tensor]) -> Optional[torch.Tensor]:
-    return None if t is None else (t.conj() if t.is_complex() else t)
-
-
-def _dagger_operands(L, Ws, R):
-    """operands of the adjoint matvec: L'[c,b,a] = conj L[a,b,c], W'[b,e,d,f] =
-    conj W[b,d,e,f], R'[k,f,l] = conj R[l,f,k]"""
-    fix = lambda t: t.resolve_conj().contiguous()
-    return (fix(_c(L).permute(2, 1, 0)), [fix(_c(w).permute(0, 2, 1, 3)) for w in Ws],
-            fix(_c(R).permute(2, 1, 0)))
-
-
 def heff_backward(L, Ws: Sequence[torch.Tensor], R, psi, gy, need_psi=True, need_L=False, need_W=(False, False),
                   need_R=False, prec: str = None):
-    """Gradients of Re<gy, y> style losses for y = H_eff psi (0, 1 or 2 sites).
-    Returns (g_psi, g_L, [g_W1, g_W2], g_R) with None where not requested."""
+    """Gradients for y = H_eff psi (0, 1 or 2 sites) given gy, through
+    reno_heff_backward.  Returns (g_psi, g_L, [g_W1, g_W2], g_R) with None
+    where not requested; real operands get the real part."""
+    import ctypes
+    from ._native import dtype_code
     from .hop_expr import HeffOperator
-    eng = Engine.get(psi.device)
-    n = len(Ws)
-    gpsi = gL = gR = None
-    gW: List[Optional[torch.Tensor]] = [None] * n
-    if need_psi:
-        Ld, Wd, Rd = _dagger_operands(L, Ws, R)
-        gpsi = HeffOperator(Ld, Rd, Wd, psi.shape, prec=prec).apply(gy.resolve_conj().contiguous())
-    cL, cR, cP = _c(L), _c(R), _c(psi)
-    cW = [_c(w) for w in Ws]
-    td = lambda x, y, ax: tensordot(x, y, ax, eng)
-    if need_L:
-        if n == 0:
-            T = td(cP, cR, ([1], [2]))                                  # c l b
-            gL = td(gy, T, ([1], [1])).permute(0, 2, 1)                 # a c b -> a b c
-        elif n == 1:
-            T = td(cP, cR, ([2], [2]))                                  # c e l f
-            T = td(T, cW[0], ([1, 3], [2, 3]))                          # c l b d
-            gL = td(gy, T, ([1, 2], [3, 1])).permute(0, 2, 1)           # a c b -> a b c
-        else:
-            T = td(cP, cR, ([3], [2]))                                  # c e h l j
-            T = td(T, cW[1], ([2, 4], [2, 3]))                          # c e l f g
-            T = td(T, cW[0], ([1, 3], [2, 3]))                          # c l g b d
-            gL = td(gy, T, ([1, 2, 3], [4, 2, 1])).permute(0, 2, 1)     # a c b -> a b c
-    if need_R:
-        if n == 0:
-            T = td(cL, cP, ([2], [0]))                                  # a b k
-            gR = td(gy, T, ([0], [0]))                                  # l b k
-        elif n == 1:
-            T = td(cL, cP, ([2], [0]))                                  # a b e k
-            T = td(T, cW[0], ([1, 2], [0, 2]))                          # a k d f
-            gR = td(gy, T, ([0, 1], [0, 2])).permute(0, 2, 1)           # l k f -> l f k
-        else:
-            T = td(cL, cP, ([2], [0]))                                  # a b e h k
-            T = td(T, cW[0], ([1, 2], [0, 2]))                          # a h k d f
-            T = td(T, cW[1], ([4, 1], [0, 2]))                          # a k d g j
-            gR = td(gy, T, ([0, 1, 2], [0, 2, 3])).permute(0, 2, 1)     # l k j -> l j k
-    if n >= 1 and need_W[0]:
-        if n == 1:
-            T = td(cL, cP, ([2], [0]))                                  # a b e k
-            T = td(T, cR, ([3], [2]))                                   # a b e l f
-            gW[0] = td(gy, T, ([0, 2], [0, 3])).permute(1, 0, 2, 3)     # d b e f -> b d e f
-        else:
-            T = td(cP, cR, ([3], [2]))                                  # c e h l j
-            T = td(T, cW[1], ([2, 4], [2, 3]))                          # c e l f g
-            T = td(T, cL, ([0], [2]))                                   # e l f g a b
-            gW[0] = td(gy, T, ([0, 2, 3], [4, 3, 1])).permute(3, 0, 1, 2)   # d e f b -> b d e f
-    if n == 2 and need_W[1]:
-        T = td(cL, cP, ([2], [0]))                                      # a b e h k
-        T = td(T, cW[0], ([1, 2], [0, 2]))                              # a h k d f
-        T = td(T, cR, ([2], [2]))                                       # a h d f l j
-        gW[1] = td(gy, T, ([0, 1, 3], [0, 2, 4])).permute(2, 0, 1, 3)  # g h f j -> f g h j
-    fix = lambda g, like: None if g is None else (g.contiguous() if like.is_complex() else g.real.contiguous())
-    return (fix(gpsi, psi), fix(gL, L), [fix(g, w) for g, w in zip(gW, Ws)], fix(gR, R))
+    op = HeffOperator(L, R, list(Ws), psi.shape, prec=prec)
+    p = psi.reshape(op.cshape)
+    if p.dtype not in (torch.float64, torch.complex128):
+        p = p.to(torch.complex128 if p.is_complex() else torch.float64)
+    p = p.resolve_conj().contiguous()
+    desc = type(op.desc)()
+    ctypes.pointer(desc)[0] = op.desc
+    desc.psi_dtype = dtype_code(p)
+    ydt = op.out_dtype(p)
+    g = gy.reshape(op.cshape).to(ydt).resolve_conj().contiguous()
+    new = lambda like, cond: torch.empty(like.shape, dtype=ydt, device=p.device) if cond else None
+    n = len(op.W)
+    gpsi, gL, gR = new(p, need_psi), new(op.L, need_L), new(op.R, need_R)
+    gW = [new(op.W[i], need_W[i]) if i < n else None for i in range(2)]
+    op.engine.sync_stream()
+    op.engine.heff_backward(desc, op.L, op.W[0] if n >= 1 else None, op.W[1] if n == 2 else None, op.R, p, g,
+                            gpsi, gL, gW[0], gW[1], gR)
+    fix = lambda t, like: None if t is None else (t if like.is_complex() else t.real.contiguous())
+    return (fix(gpsi, psi), fix(gL, L), [fix(gW[i], Ws[i]) for i in range(len(Ws))], fix(gR, R))
 
 
 class HeffFunction(torch.autograd.Function):

@@ -23,7 +23,7 @@ class FakeEngine:
 
     def __getattribute__(self, name):
         attr = object.__getattribute__(self, name)
-        if name in ("heff_apply", "heff_diag", "env_update", "vec_norm", "vec_dotc", "krylov_alpha", "krylov_orth",
+        if name in ("heff_apply", "heff_backward", "heff_diag", "env_update", "vec_norm", "vec_dotc", "krylov_alpha", "krylov_orth",
                     "scale_inv", "lincomb", "allclose", "axpy", "precond", "qn_gather"):
             def checked(*a, **k):
                 _chk(*a)
@@ -44,6 +44,19 @@ class FakeEngine:
             r = torch.einsum("abc,bdef,fghj,ljk,cehk->adgl", L.to(y.dtype), W1.to(y.dtype), W2.to(y.dtype),
                              R.to(y.dtype), psi.to(y.dtype))
         y.copy_(r)
+
+    def heff_backward(self, d, L, W1, W2, R, psi, gy, gpsi, gL, gW1, gW2, gR):
+        spec = {0: "abc,lbk,ck->al", 1: "abc,bdef,lfk,cek->adl", 2: "abc,bdef,fghj,ljk,cehk->adgl"}[d.nsite]
+        dt = gy.dtype
+        leaves = [t.detach().to(dt).requires_grad_(True) for t in [L] + [w for w in (W1, W2) if w is not None] +
+                  [R, psi]]
+        with torch.enable_grad():
+            y = torch.einsum(spec, *leaves)
+            grads = torch.autograd.grad(y, leaves, gy)
+        outs = [gL] + [o for o, w in ((gW1, W1), (gW2, W2)) if w is not None] + [gR, gpsi]
+        for o, g in zip(outs, grads):
+            if o is not None:
+                o.copy_(g)
 
     def heff_diag(self, d, L, W1, W2, R, out):
         tl = torch.einsum("aba->ba", L).real
