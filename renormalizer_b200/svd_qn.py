@@ -351,37 +351,48 @@ def _subspace_block(eng, X, keep_left, k, opts, Q=None, iters=None):
     return K, Ph.transpose(0, 1).conj().resolve_conj(), S, chk, Q
 
 
-def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool) -> dict:
+def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optional[int] = None) -> dict:
     """Kept-side basis K, projection P and sigma S of one block from the full
-    Gram eigendecomposition of its smaller side (all min(m, n) triplets)."""
+    Gram eigendecomposition of its smaller side (all min(m, n) triplets).
+
+    With ``ktop`` < min(m, n) (a fixed cap on the kept dimension is known and
+    the block is larger) only the leading ktop singular vectors are projected:
+    P has ktop rows/columns and the other sigma come from the Gram
+    eigenvalues, sqrt(max(lambda, 0)) -- none of them can be selected, they
+    only fill the list the truncation rule reads."""
     m, n = X.shape
     dim = min(m, n)
+    kt = dim if ktop is None else min(int(ktop), dim)
+
+    def tail(w_desc):
+        return torch.sqrt(torch.clamp(w_desc[kt:dim], min=0.0))
+
     if keep_left and m <= n:
         G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-        _, K = torch.linalg.eigh(G)
-        K = torch.flip(K, dims=[1])
-        P = eng.matmul(K[:, :dim].transpose(0, 1), X, conj_a=True)
-        S = torch.linalg.vector_norm(P, dim=1)
+        w, K = torch.linalg.eigh(G)
+        K, w = torch.flip(K, dims=[1]), torch.flip(w, dims=[0])
+        P = eng.matmul(K[:, :kt].transpose(0, 1), X, conj_a=True)           # (kt, n) = sigma Vh
+        S = torch.cat([torch.linalg.vector_norm(P, dim=1), tail(w)])
     elif keep_left:
         G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-        _, V = torch.linalg.eigh(G)
-        V = torch.flip(V, dims=[1])
-        Us = eng.matmul(X, V)
-        S = torch.linalg.vector_norm(Us, dim=0)
+        w, V = torch.linalg.eigh(G)
+        V, w = torch.flip(V, dims=[1]), torch.flip(w, dims=[0])
+        Us = eng.matmul(X, V[:, :kt])                                        # (m, kt) = U sigma
+        S = torch.cat([torch.linalg.vector_norm(Us, dim=0), tail(w)])
         K, _ = torch.linalg.qr(Us, mode="reduced")
         P = eng.matmul(K.transpose(0, 1), X, conj_a=True)
     elif n <= m:
         G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-        _, K = torch.linalg.eigh(G)
-        K = torch.flip(K, dims=[1])
-        P = eng.matmul(X, K[:, :dim])
-        S = torch.linalg.vector_norm(P, dim=0)
+        w, K = torch.linalg.eigh(G)
+        K, w = torch.flip(K, dims=[1]), torch.flip(w, dims=[0])
+        P = eng.matmul(X, K[:, :kt])                                         # (m, kt) = U sigma
+        S = torch.cat([torch.linalg.vector_norm(P, dim=0), tail(w)])
     else:
         G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-        _, U = torch.linalg.eigh(G)
-        U = torch.flip(U, dims=[1])
-        Vs = eng.matmul(X.transpose(0, 1), U, conj_a=True)
-        S = torch.linalg.vector_norm(Vs, dim=0)
+        w, U = torch.linalg.eigh(G)
+        U, w = torch.flip(U, dims=[1]), torch.flip(w, dims=[0])
+        Vs = eng.matmul(X.transpose(0, 1), U[:, :kt], conj_a=True)           # (n, kt): sigma v
+        S = torch.cat([torch.linalg.vector_norm(Vs, dim=0), tail(w)])
         K, _ = torch.linalg.qr(Vs, mode="reduced")
         P = eng.matmul(X, K)
     return dict(K=K, P=P, S=S, dim=dim)
@@ -433,7 +444,8 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
             blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=ksub, npad=npad, res=chk,
                                X=X, Q=Q))
             continue
-        full = _full_kept_side(eng, X, keep_left)
+        ktop = kcap + 64 if kcap is not None and kcap + 64 < dim else None
+        full = _full_kept_side(eng, X, keep_left, ktop)
         K, P, S = full["K"], full["P"], full["S"]
         npad = upad if keep_left else vpad
         blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=dim, npad=npad))

@@ -100,3 +100,29 @@ def test_subspace_matches_full_path_gpu(keep_left):
         assert svd_qn.subspace.fallbacks == f0
     finally:
         svd_qn.subspace.min_dim = saved
+
+
+@pytest.mark.parametrize("keep_left", [True, False])
+@pytest.mark.parametrize("shape", [(160, 160), (160, 96), (96, 160)])
+def test_capped_projection_matches_full_cpu(cpu_engine, keep_left, shape):
+    """with a fixed cap the full decomposition projects only the leading
+    cap + 64 vectors; the selection, the kept factors and the leading sigma
+    are those of the uncapped call"""
+    from renormalizer_b200.svd_qn import svd_truncate
+    g = torch.Generator().manual_seed(1)
+    m, n = shape
+    X = torch.complex(torch.randn(m, n, dtype=torch.float64, generator=g),
+                      torch.randn(m, n, dtype=torch.float64, generator=g))
+    U, _ = torch.linalg.qr(X)
+    V, _ = torch.linalg.qr(X.mH)
+    k = min(m, n)
+    s = torch.exp(-torch.arange(k, dtype=torch.float64) / 9.0)
+    coef = (U[:, :k] * s) @ V[:, :k].mH
+    ql = np.zeros((m, 1), dtype=int)
+    qr = np.zeros((n, 1), dtype=int)
+    kcap = 16
+    full = svd_truncate(coef, ql, qr, np.array([0]), keep_left, lambda sg: min(kcap, len(sg)))
+    capped = svd_truncate(coef, ql, qr, np.array([0]), keep_left, lambda sg: min(kcap, len(sg)), kcap=kcap)
+    assert capped.mdim == full.mdim == kcap
+    np.testing.assert_allclose(capped.sigma, full.sigma, rtol=1e-12)
+    assert torch.allclose(capped.left @ capped.right, full.left @ full.right, atol=1e-12)
