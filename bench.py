@@ -247,7 +247,7 @@ def run_reference(args, rank, world):
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "nsites": 3 * args.nmol, "M": args.M, "nlev": args.nlev,
-                       "dt": args.dt, "parallelism": "replicas"},
+                       "dt": args.dt, "parallelism": "replicas" if world > 1 else "single"},
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
