@@ -67,6 +67,9 @@ def parse():
                          "largest site-population difference after every step (no timing)")
     ap.add_argument("--truncation", default="subspace", choices=["subspace", "exact"],
                     help="exact: every QN block uses the full Gram eigendecomposition")
+    ap.add_argument("--dmrg", action="store_true",
+                    help="ground-state DMRG of the spin-boson model (one spin, 64 Ohmic modes with alpha=0.5, "
+                         "omega_c=10, 8 levels; M=256) in the chosen split precision and in FP64")
     ap.add_argument("--grad", action="store_true",
                     help="gradient of the site-0 population after a TDVP-PS trajectory with respect to per-molecule "
                          "couplings (16-molecule Holstein, 10 levels, M=64, 50 steps of dt=0.05)")
@@ -566,6 +569,45 @@ def run_accuracy(args):
                       "max": max(dev) if dev else None}), flush=True)
 
 
+def run_dmrg(args):
+    """Davidson DMRG (gs.optimize_mps, 2-site, one root) of eps = 0, Delta = 1
+    and 64 modes from the Ohmic spectral density alpha = 0.5, omega_c = 10
+    (Wang1 discretisation), 8 SHO levels (65 sites, real float64), M = 256,
+    procedure [[256, .4], [256, .2], [256, .1]] + [[256, 0]] * 8 until the two
+    lowest sweep energies agree to 1e-9; the same seeded random start in
+    --prec (split matvecs) and in FP64."""
+    import torch
+    from renormalizer_b200 import Mpo, Mps, Phonon, Quantity, SpectralDensityFunction, SpinBosonModel, backend
+    from renormalizer_b200.gs import optimize_mps
+    torch.cuda.set_device(0)
+    nmodes, nlev, M = 64, 8, 256
+    w, c2 = SpectralDensityFunction(0.5, Quantity(10.0)).Wang1(nmodes)
+    ph = [Phonon.simple_phonon(Quantity(wi), Quantity(np.sqrt(ci) / wi ** 2), nlev) for wi, ci in zip(w, c2)]
+    model = SpinBosonModel(Quantity(0.0), Quantity(1.0), ph)
+    mpo = Mpo(model)
+    proc = [[M, 0.4], [M, 0.2], [M, 0.1]] + [[M, 0]] * 8
+    out = {}
+    for prec in (args.prec, "fp64"):
+        backend.prec = prec
+        np.random.seed(9012)
+        mps = Mps.random(model, 0, M)
+        mps.optimize_config.procedure = proc
+        mps.optimize_config.method = "2site"
+        mps.optimize_config.e_atol = 1e-9
+        torch.cuda.synchronize()
+        t0 = time.time()
+        energies, _ = optimize_mps(mps, mpo)
+        torch.cuda.synchronize()
+        out[prec] = {"energies": [float(e) for e in energies], "seconds": time.time() - t0,
+                     "sweeps": len(energies)}
+    a, b = out[args.prec], out["fp64"]
+    print(json.dumps({"metric": "spin-boson DMRG (65 sites, M=256): lowest energy, split precision vs FP64",
+                      "value": a["seconds"] / a["sweeps"], "unit": f"s per sweep ({args.prec})",
+                      "fp64_s_per_sweep": b["seconds"] / b["sweeps"], "e_min": {args.prec: min(a["energies"]),
+                                                                              "fp64": min(b["energies"])},
+                      "e_min_abs_diff": abs(min(a["energies"]) - min(b["energies"])), "runs": out}), flush=True)
+
+
 def run_grad(args):
     """16 molecules x (e, one mode omega = 1, 10 levels), J = 1, g_i ~ U(0.5, 1.5)
     (seed 5), exciton on molecule 0, bonds expanded to M = 64, 1-site TDVP-PS,
@@ -625,6 +667,9 @@ def run_grad(args):
 
 def main():
     args = parse()
+    if args.dmrg:
+        run_dmrg(args)
+        return
     if args.grad:
         run_grad(args)
         return
