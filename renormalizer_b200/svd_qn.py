@@ -163,6 +163,13 @@ def _scatter(eng: Engine, src: torch.Tensor, rows, scols, dcols, sigma, dst: tor
     """dst[rows[i]*dst_rs + dcols[j]*dst_cs] = sigma_j * src[i, scols[j]] (src: any 2-D view)"""
     if len(rows) == 0 or len(scols) == 0:
         return
+    # the kernel does not bound-check its index lists: check them here
+    r, c = np.asarray(rows, dtype=np.int64), np.asarray(scols, dtype=np.int64)
+    dc = np.asarray(dcols, dtype=np.int64)
+    if (len(r) > src.shape[0] or len(dc) != len(c) or c.min() < 0 or c.max() >= src.shape[1] or r.min() < 0
+            or dc.min() < 0 or int(r.max()) * dst_rs + int(dc.max()) * dst_cs >= dst.numel()):
+        raise IndexError(f"qn scatter out of range: src {tuple(src.shape)}, {len(r)} rows (max {r.max()}), "
+                         f"source columns up to {c.max()}, dst {tuple(dst.shape)}")
     dev = dst.device
     sig = None
     if sigma is not None:
@@ -358,27 +365,36 @@ def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optiona
     With ``ktop`` < min(m, n) (a fixed cap on the kept dimension is known and
     the block is larger) only the leading ktop singular vectors are projected:
     P has ktop rows/columns and the other sigma come from the Gram
-    eigenvalues, sqrt(max(lambda, 0)) -- none of them can be selected, they
-    only fill the list the truncation rule reads."""
+    eigenvalues, sqrt(max(lambda, 0)), capped at the smallest projected
+    sigma.  The cap matters: below sqrt(eps) ||X|| the Gram eigenvalues are
+    rounding noise, so an uncapped tail value (~1e-8 ||X||) can exceed the
+    true, projected sigma of the head (1e-10 and below in a nearly product
+    state) and be selected although it has no projection.  Capped, every tail
+    entry sorts after every head entry of its block, and since a block
+    contributes at most the cap (< ktop) entries, none is selected; they only
+    fill the list the truncation rule reads."""
     m, n = X.shape
     dim = min(m, n)
     kt = dim if ktop is None else min(int(ktop), dim)
 
-    def tail(w_desc):
-        return torch.sqrt(torch.clamp(w_desc[kt:dim], min=0.0))
+    def tail(w_desc, head):
+        t = torch.sqrt(torch.clamp(w_desc[kt:dim], min=0.0))
+        return torch.minimum(t, head.min()) if kt < dim and head.numel() else t
 
     if keep_left and m <= n:
         G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
         w, K = torch.linalg.eigh(G)
         K, w = torch.flip(K, dims=[1]), torch.flip(w, dims=[0])
         P = eng.matmul(K[:, :kt].transpose(0, 1), X, conj_a=True)           # (kt, n) = sigma Vh
-        S = torch.cat([torch.linalg.vector_norm(P, dim=1), tail(w)])
+        S = torch.linalg.vector_norm(P, dim=1)
+        S = torch.cat([S, tail(w, S)])
     elif keep_left:
         G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
         w, V = torch.linalg.eigh(G)
         V, w = torch.flip(V, dims=[1]), torch.flip(w, dims=[0])
         Us = eng.matmul(X, V[:, :kt])                                        # (m, kt) = U sigma
-        S = torch.cat([torch.linalg.vector_norm(Us, dim=0), tail(w)])
+        S = torch.linalg.vector_norm(Us, dim=0)
+        S = torch.cat([S, tail(w, S)])
         K, _ = torch.linalg.qr(Us, mode="reduced")
         P = eng.matmul(K.transpose(0, 1), X, conj_a=True)
     elif n <= m:
@@ -386,13 +402,15 @@ def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optiona
         w, K = torch.linalg.eigh(G)
         K, w = torch.flip(K, dims=[1]), torch.flip(w, dims=[0])
         P = eng.matmul(X, K[:, :kt])                                         # (m, kt) = U sigma
-        S = torch.cat([torch.linalg.vector_norm(P, dim=0), tail(w)])
+        S = torch.linalg.vector_norm(P, dim=0)
+        S = torch.cat([S, tail(w, S)])
     else:
         G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
         w, U = torch.linalg.eigh(G)
         U, w = torch.flip(U, dims=[1]), torch.flip(w, dims=[0])
         Vs = eng.matmul(X.transpose(0, 1), U[:, :kt], conj_a=True)           # (n, kt): sigma v
-        S = torch.cat([torch.linalg.vector_norm(Vs, dim=0), tail(w)])
+        S = torch.linalg.vector_norm(Vs, dim=0)
+        S = torch.cat([S, tail(w, S)])
         K, _ = torch.linalg.qr(Vs, mode="reduced")
         P = eng.matmul(X, K)
     return dict(K=K, P=P, S=S, dim=dim)

@@ -126,3 +126,35 @@ def test_capped_projection_matches_full_cpu(cpu_engine, keep_left, shape):
     assert capped.mdim == full.mdim == kcap
     np.testing.assert_allclose(capped.sigma, full.sigma, rtol=1e-12)
     assert torch.allclose(capped.left @ capped.right, full.left @ full.right, atol=1e-12)
+
+
+@pytest.mark.parametrize("keep_left", [True, False])
+@pytest.mark.parametrize("shape", [(160, 160), (160, 96), (96, 160)])
+def test_capped_projection_nearly_product_cpu(cpu_engine, keep_left, shape):
+    """a nearly product block (sigma = 1, then 1e-10 and below, as in a
+    bond-expanded product state in FP64): the Gram eigenvalues past the
+    first are rounding noise (~1e-16, sqrt ~1e-8, above the true sigma), so
+    the unprojected tail must never outrank the projected head -- the
+    selection stays within the projected vectors, the kept side is
+    orthonormal and left @ right reproduces the block to 1e-9"""
+    from renormalizer_b200.svd_qn import svd_truncate
+    g = torch.Generator().manual_seed(4)
+    m, n = shape
+    X = torch.complex(torch.randn(m, n, dtype=torch.float64, generator=g),
+                      torch.randn(m, n, dtype=torch.float64, generator=g))
+    U, _ = torch.linalg.qr(X)
+    V, _ = torch.linalg.qr(X.mH)
+    k = min(m, n)
+    s = torch.cat([torch.ones(1, dtype=torch.float64),
+                   1e-10 * torch.exp(-torch.arange(k - 1, dtype=torch.float64) / 4.0)])
+    coef = (U[:, :k] * s) @ V[:, :k].mH
+    ql = np.zeros((m, 1), dtype=int)
+    qr = np.zeros((n, 1), dtype=int)
+    kcap = 4  # projects 68 of the 95 or 159 tiny directions: the rest of the positive noise is tail
+    capped = svd_truncate(coef, ql, qr, np.array([0]), keep_left, lambda sg: min(kcap, len(sg)), kcap=kcap)
+    assert capped.mdim == kcap
+    assert abs(capped.sigma[0] - 1.0) < 1e-12 and np.all(capped.sigma[1:] < 1e-9)
+    kept = capped.left if keep_left else capped.right.mH
+    eye = torch.eye(kcap, dtype=kept.dtype)
+    assert float((kept.mH @ kept - eye).abs().max()) < 1e-12
+    assert float((capped.left @ capped.right - coef).abs().max()) < 1e-9
