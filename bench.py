@@ -65,8 +65,9 @@ def parse():
     ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
                     help="run STEPS steps with --prec and with plain FP64 from the same start and report the "
                          "largest site-population difference after every step (no timing)")
-    ap.add_argument("--truncation", default="subspace", choices=["subspace", "exact"],
-                    help="exact: every QN block uses the full Gram eigendecomposition")
+    ap.add_argument("--truncation", default="exact", choices=["exact", "subspace"],
+                    help="exact (default): every QN block uses the full Gram eigendecomposition; subspace: blocks "
+                         "with at least 1024 rows on the smaller side use the opt-in top-k subspace iteration")
     ap.add_argument("--dmrg", action="store_true",
                     help="ground-state DMRG of the spin-boson model (one spin, 64 Ohmic modes with alpha=0.5, "
                          "omega_c=10, 8 levels; M=256) in the chosen split precision and in FP64")
@@ -673,9 +674,8 @@ def main():
     if args.grad:
         run_grad(args)
         return
-    if args.truncation == "exact":
-        import importlib
-        importlib.import_module("renormalizer_b200.svd_qn").subspace.min_dim = 0
+    import importlib
+    importlib.import_module("renormalizer_b200.svd_qn").subspace.min_dim = 1024 if args.truncation == "subspace" else 0
     if args.accuracy:
         run_accuracy(args)
         return
