@@ -80,13 +80,15 @@ def _qr_into(space: _Space, xs, lindep, start):
     return nv
 
 
-def davidson(aop, x0, precond, tol=1e-12, max_cycle=50, max_space=12, lindep=1e-14, nroots=1, **kwargs):
+def davidson(aop, x0, precond, tol=1e-12, max_cycle=50, max_space=12, lindep=1e-14, nroots=1, tol_residual=None,
+             **kwargs):
     """Lowest eigenpair of a Hermitian operator.
 
     aop(x) maps a 1-D device vector to a 1-D device vector; x0 is a 1-D
     vector or a list of them; precond(dx, e, x0) returns the preconditioned
-    residual (a device vector).  Returns (e, c) like the reference with
-    nroots=1."""
+    residual (a device vector).  Converged when the energy change is below
+    ``tol`` and the residual norm below ``tol_residual`` (default sqrt(tol),
+    davidson.py:230-233).  Returns (e, c) like the reference with nroots=1."""
     if nroots != 1:
         raise NotImplementedError("the sweep engine's Davidson solves one root")
     if isinstance(x0, (np.ndarray, torch.Tensor)) and x0.ndim == 1:
@@ -97,7 +99,7 @@ def davidson(aop, x0, precond, tol=1e-12, max_cycle=50, max_space=12, lindep=1e-
     eng = Engine.get(dev)
     n = x0[0].numel()
     dtype = torch.complex128 if any(x.is_complex() for x in x0) else torch.float64
-    toloose = np.sqrt(tol)
+    toloose = np.sqrt(tol) if tol_residual is None else tol_residual
     rows = max_space + 2
     sp = _Space(eng, n, dtype, dev, rows)
     heff = None

@@ -12,6 +12,15 @@ diagonal comes from reno_heff_diag (gs.py:419-445, 532-538).  The masked
 vector <-> block tensor moves (lib.py:442-457 cvec2cmat) are reno_qn
 gather/scatter calls.  Truncation is the engine's QN-blocked
 ``Mps._update_mps`` with the procedure's ``percent``.
+
+In split precision (backend.prec bf16x3 / tf32x3) the Davidson runs in two
+stages: on the split operator until the residual reaches its rounding floor
+(``SPLIT_NOISE`` times the largest diagonal entry), then on the FP64 operator
+from that vector to the reference's tolerance, so energies and states carry
+FP64 accuracy while most matvecs are split.  A split operator alone leaves a
+Rayleigh quotient up to its error norm below the true ground state and a
+residual that never reaches sqrt(tol).  The environments and the dense
+small-block H_eff are FP64 for the same reason.
 """
 from __future__ import annotations
 
@@ -32,6 +41,10 @@ from .mps import Mps
 from .svd_qn import get_qn_mask
 
 logger = logging.getLogger(__name__)
+
+# relative error of one split-precision H_eff matvec against FP64 (a residual
+# below this times the largest diagonal entry is rounding of the split operator)
+SPLIT_NOISE = {"bf16x3": 1e-4, "tf32x3": 1e-5}
 
 
 class _Mask:
@@ -97,7 +110,7 @@ def optimize_mps(mps: Mps, mpo: Mpo, omega: float = None) -> Tuple[List, Mps]:
         mps.ensure_left_canonical()
         env = "L"
     compress_config_bk = mps.compress_config
-    environ = Environ(mps, mpo, env)
+    environ = Environ(mps, mpo, env, prec="fp64")
     macro = []
     opt_e_idx = None
     res_mps = None
@@ -148,11 +161,12 @@ def single_sweep(mps: Mps, mpo: Mpo, environ: Environ, percent, last_opt_e_idx, 
         cshape = qn_mask.shape
         cmo = [mpo[i] for i in cidx]
         op = HeffOperator(ltensor, rtensor, cmo, cshape)
+        op64 = op if op.prec == "fp64" else HeffOperator(ltensor, rtensor, cmo, cshape, prec="fp64")
         dtype = torch.complex128 if (mps.is_complex or op.complex_env) else torch.float64
         mask = _Mask(qn_mask, mps[0].device)
         inverse = mps.optimize_config.inverse
         if np.prod(cshape) < 1000 or mps.optimize_config.algo == "direct":
-            ham = _dense_heff(op, mask, dtype) * inverse
+            ham = _dense_heff(op64, mask, dtype) * inverse
             w, v = scipy.linalg.eigh(ham)
             e = float(w[0])
             c = torch.as_tensor(v[:, 0]).to(mps[0].device)
@@ -167,10 +181,15 @@ def single_sweep(mps: Mps, mpo: Mpo, environ: Environ, percent, last_opt_e_idx, 
             hdiag = mask.take(op.diag()) * inverse
             precond = make_diag_precond(hdiag.contiguous())
 
-            def aop(x):
-                return mask.take(op.apply(mask.place(x, dtype))) * inverse
+            def aop_of(o):
+                return lambda x: mask.take(o.apply(mask.place(x, dtype))) * inverse
 
-            e, c = davidson(aop, cguess, precond, max_cycle=100)
+            if op is not op64:
+                # split-precision stage down to the split operator's noise
+                # floor, then FP64 refinement from its vector
+                floor = SPLIT_NOISE[op.prec] * float(hdiag.abs().max())
+                _, cguess = davidson(aop_of(op), cguess, precond, tol=floor, tol_residual=floor, max_cycle=100)
+            e, c = davidson(aop_of(op64), cguess, precond, max_cycle=100)
             c = sign_fix(c)
         micro.append((e, cidx))
         cstruct = mask.place(c, mps.dtype if not c.is_complex() else torch.complex128)

@@ -63,9 +63,15 @@ class Environ:
     """lib.py:12-118 with device-resident storage.
 
     idx convention: L(idx-1) - mpo(idx) - R(idx+1); out-of-range reads of
-    GetLR return the ones((1,1,1)) sentinel (lib.py:80-81)."""
+    GetLR return the ones((1,1,1)) sentinel (lib.py:80-81).
 
-    def __init__(self, mps, mpo, domain=None, mps_conj=None):
+    ``prec`` (not in the reference) fixes the arithmetic of every update of
+    this environment; None follows the backend's precision at each call.
+    The ground-state search keeps its environments in FP64: their rounding
+    accumulates along the chain into every later effective Hamiltonian."""
+
+    def __init__(self, mps, mpo, domain=None, mps_conj=None, prec: str = None):
+        self.prec = prec
         self._virtual_disk = {}
         self.sentinel = torch.ones((1, 1, 1), dtype=torch.float64, device=backend.device)
         self._construct(mps, mpo, domain, mps_conj)
@@ -85,7 +91,7 @@ class Environ:
         tensor = self.sentinel
         for idx in range(start, end, inc):
             conj = mps_conj[idx] if mps_conj is not None else None
-            tensor = contract_one_site(tensor, mps[idx], mpo[idx], domain, ms_conj=conj)
+            tensor = contract_one_site(tensor, mps[idx], mpo[idx], domain, ms_conj=conj, prec=self.prec)
             self.write(domain, idx, tensor)
 
     def GetLR(self, domain, siteidx, mps, mpo, itensor=None, method="Scratch", mps_conj=None):
@@ -98,7 +104,7 @@ class Environ:
             sitelist = range(siteidx + 1) if domain == "L" else range(len(mps) - 1, siteidx - 1, -1)
             for imps in sitelist:
                 conj = mps_conj[imps] if mps_conj is not None else None
-                itensor = contract_one_site(itensor, mps[imps], mpo[imps], domain, ms_conj=conj)
+                itensor = contract_one_site(itensor, mps[imps], mpo[imps], domain, ms_conj=conj, prec=self.prec)
         elif method == "Enviro":
             itensor = self.read(domain, siteidx)
         else:
@@ -106,7 +112,7 @@ class Environ:
                 offset = -1 if domain == "L" else 1
                 itensor = self.read(domain, siteidx + offset)
             conj = mps_conj[siteidx] if mps_conj is not None else None
-            itensor = contract_one_site(itensor, mps[siteidx], mpo[siteidx], domain, ms_conj=conj)
+            itensor = contract_one_site(itensor, mps[siteidx], mpo[siteidx], domain, ms_conj=conj, prec=self.prec)
             self.write(domain, siteidx, itensor)
         return itensor
 

@@ -23,16 +23,19 @@ PROC = {"hol_test_gs": ([[10, 0.4], [20, 0.2], [30, 0.1], [40, 0], [40, 0]], 1e-
         "sbm6x4": ([[12, 0.4], [12, 0.2], [12, 0.1], [12, 0], [12, 0], [12, 0]], 1e-9)}
 
 
-def run_dmrg(tag, method="2site"):
+def run_dmrg(tag, method="2site", prec="fp64"):
     from renormalizer_b200 import backend
     from renormalizer_b200.gs import optimize_mps
-    backend.prec = "fp64"
-    mps, mpo = engine_chain(DMRG, tag)
-    proc, e_atol = PROC[tag]
-    mps.optimize_config.procedure = proc
-    mps.optimize_config.method = method
-    mps.optimize_config.e_atol = e_atol
-    energies, res = optimize_mps(mps, mpo)
+    backend.prec = prec
+    try:
+        mps, mpo = engine_chain(DMRG, tag)
+        proc, e_atol = PROC[tag]
+        mps.optimize_config.procedure = proc
+        mps.optimize_config.method = method
+        mps.optimize_config.e_atol = e_atol
+        energies, res = optimize_mps(mps, mpo)
+    finally:
+        backend.prec = "fp64"
     return np.array(energies), res, mpo
 
 
@@ -58,3 +61,27 @@ def test_dmrg_matches_reference(tag):
 def test_dmrg_host_logic_matches_reference(cpu_engine):
     """the sweep logic on the CPU stand-in engine, on the Holstein chain"""
     check("hol_test_gs", *run_dmrg("hol_test_gs"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+@pytest.mark.parametrize("tag", ["hol_test_gs", "sbm6x4"])
+def test_dmrg_split_precision_refined(tag, prec):
+    """split-precision Davidson stages refined by FP64 matvecs, FP64
+    environments: the sweep energies must be the FP64 ones (1e-9 relative
+    on the percent = 0 sweeps, the lowest within 1e-9), never below the
+    reference's ground state by more than that"""
+    energies, res, mpo = run_dmrg(tag, prec=prec)
+    ref = DMRG[f"{tag}/energies"]
+    pct = np.array([p for _, p in PROC[tag][0]])
+    n = min(len(energies), len(ref))
+    np.testing.assert_allclose(energies[:n][pct[:n] == 0], ref[:n][pct[:n] == 0], rtol=1e-9)
+    assert min(energies) == pytest.approx(min(ref), rel=1e-9)
+    assert min(energies) >= min(ref) - 1e-9 * abs(min(ref))
+    assert res.norm == pytest.approx(1.0, abs=1e-10)
+
+
+def test_dmrg_split_host_logic(cpu_engine):
+    """the two-stage (split, then FP64) Davidson path on the CPU stand-in,
+    whose arithmetic is exact at every precision: same sweeps as FP64"""
+    check("hol_test_gs", *run_dmrg("hol_test_gs", prec="bf16x3"))
