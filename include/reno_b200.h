@@ -132,6 +132,29 @@ int reno_heff_apply_noalloc(reno_ctx* ctx, const reno_heff_desc* desc,
                             const void* L, const void* W1, const void* W2,
                             const void* R, const void* psi, void* y);
 
+/* Leading eigenpairs of a Hermitian Gram block for the truncation
+ * (svd_qn.py:12-49 optimized_svd / mp.py:693-778, where the reference takes
+ * LAPACK gesdd of the block; the engine diagonalises the block's Gram matrix).
+ * reno_heev_top reduces A (n x n complex128, row-major, both triangles, a
+ * private copy: reflector k is written into row k) to a real tridiagonal
+ * matrix (d[n], e[n-1], tau[n-1] complex128) in one cooperative launch, then
+ * writes the kt largest eigenvalues (ascending) to w and the matching
+ * eigenvectors of the tridiagonal matrix (inverse iteration, not yet
+ * orthonormalised) to Z (n x kt float64, row-major).  1 <= kt <= n <= 4096.
+ * The caller orthonormalises Z and passes it as K (n x kt complex128);
+ * reno_heev_backtransform overwrites K with Q K (blocked WY, FP64 GEMMs; A's
+ * reflector rows are cleaned in place, same ws).  The int at
+ * reno_heev_status_offset in ws is 0, or 1 when a grid-barrier wait of the
+ * reduction timed out (results invalid). */
+int reno_heev_workspace_bytes(int32_t n, int32_t kt, size_t* bytes);
+int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, double* d,
+                  double* e, void* tau, double* w, double* Z, void* ws,
+                  size_t ws_bytes);
+int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, void* A,
+                            const void* tau, void* K, void* ws,
+                            size_t ws_bytes);
+int reno_heev_status_offset(size_t* offset);
+
 /* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
  *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]
  *   nsite 2: hdiag[a,c,d,f] = sum L[a,b,a] W1[b,c,c,e] W2[e,d,d,g] R[f,g,f]

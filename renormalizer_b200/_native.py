@@ -52,6 +52,10 @@ _SIGS = {
     "reno_device_error": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
     "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),
+    "reno_heev_workspace_bytes": (_c_int, [_c_int, _c_int, ctypes.POINTER(_c_sz)]),
+    "reno_heev_top": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
+    "reno_heev_backtransform": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _c_sz]),
+    "reno_heev_status_offset": (_c_int, [ctypes.POINTER(_c_sz)]),
     "reno_heff_backward_workspace_bytes": (_c_int, [ctypes.POINTER(HeffDesc), ctypes.POINTER(_c_sz)]),
     "reno_heff_backward": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                     _vp, _vp, _c_sz]),
@@ -245,6 +249,30 @@ class Engine:
         c = ctypes.c_int32(0)
         self.check(self.lib.reno_device_error(self.ctx, ctypes.byref(c)), "reno_device_error")
         return int(c.value)
+
+    def heev_top(self, A, d, e, tau, w, Z, ws):
+        """reno_heev_top: tridiagonal reduction of A (overwritten), top eigenvalues
+        w (ascending) and tridiagonal eigenvectors Z (n x kt); ws from heev_workspace"""
+        n, kt = A.shape[0], w.numel()
+        self.check(self.lib.reno_heev_top(self.ctx, n, kt, ptr(A), ptr(d), ptr(e), ptr(tau), ptr(w), ptr(Z), ptr(ws),
+                                          ws.numel()), "reno_heev_top")
+        self.launches += 1
+
+    def heev_workspace(self, n: int, kt: int) -> torch.Tensor:
+        b = _c_sz()
+        self.check(self.lib.reno_heev_workspace_bytes(n, kt, ctypes.byref(b)), "reno_heev_workspace_bytes")
+        return torch.empty(int(b.value), dtype=torch.uint8, device=f"cuda:{self.device}")
+
+    def heev_status_offset(self) -> int:
+        o = _c_sz()
+        self.check(self.lib.reno_heev_status_offset(ctypes.byref(o)), "reno_heev_status_offset")
+        return int(o.value)
+
+    def heev_backtransform(self, A, tau, K, ws):
+        """K <- Q K for the reflectors of the last heev_top on A (cleaned in place)"""
+        self.check(self.lib.reno_heev_backtransform(self.ctx, A.shape[0], K.shape[1], ptr(A), ptr(tau), ptr(K),
+                                                    ptr(ws), ws.numel()), "reno_heev_backtransform")
+        self.launches += 1
 
     def heff_diag(self, desc: HeffDesc, L, W1, W2, R, out):
         self.check(self.lib.reno_heff_diag(self.ctx, ctypes.byref(desc), ptr(L), ptr(W1), ptr(W2), ptr(R), ptr(out)),

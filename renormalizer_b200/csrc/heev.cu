@@ -1,0 +1,793 @@
+// Hermitian eigensolver for the truncation's Gram blocks: the leading kt
+// eigenpairs of an n x n Hermitian matrix G (the QN-block Gram matrices of
+// svd_qn.py:12-49 / mp.py:693-778, which the reference factorises with
+// LAPACK gesdd), entirely on the device.
+//
+//   1. hetrd_kernel   Householder reduction G = Q T Q^H to a real symmetric
+//                     tridiagonal T (d, e), one persistent cooperative launch.
+//                     Step k forms reflector k from row k of the trailing
+//                     matrix, then every CTA streams its rows of the trailing
+//                     matrix once: it applies the rank-2 update of step k-1
+//                     (lagged by one step) and accumulates y = A v_k in the
+//                     same pass.  The only inter-CTA dependency per column is
+//                     the sum of y^H v_k, so there is one grid barrier per
+//                     column; each CTA recomputes v_k and w_k itself from
+//                     row k and y (bitwise identical in every CTA: same data,
+//                     same reduction order).  Reflector k is stored in row k.
+//   2. bisect_kernel  eigenvalues of T by Sturm-count multisection, one warp
+//                     per eigenvalue, 32 points per round.
+//   3. inviter_kernel eigenvectors of T by inverse iteration, one thread per
+//                     eigenvalue: LU of T - lambda I with partial pivoting,
+//                     three solves from a hashed start vector.  The host
+//                     orthonormalises the block (CholeskyQR2) and checks the
+//                     residuals ||T z - lambda z||.
+//   4. back-transformation K = Q Z in blocks of 64 reflectors (compact WY
+//                     form, three FP64 GEMMs per block, last block first).
+//
+// Every grid-barrier wait is bounded (WAIT_NS of wall clock): on timeout the
+// CTA raises the abort flag and a status word in the caller's workspace and
+// returns; the others return at their next barrier.
+#include <algorithm>
+#include <cfloat>
+#include <cstddef>
+#include "reno_common.cuh"
+#include "gemm_fp64.cuh"
+
+namespace reno {
+namespace heev {
+
+constexpr int THREADS = 256, WARPS = THREADS / 32;
+constexpr uint64_t WAIT_NS = 2000000000ull;
+constexpr int MAX_N = 4096;
+
+struct Sync {
+  unsigned count, gen;
+  int abort, status;
+};
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 conjg(double2 a) { return make_double2(a.x, -a.y); }
+
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block sum in a fixed order (shuffle tree, then warps 0..NW-1); every
+// thread gets the result
+template <int NW>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) s += red[w];
+  return s;
+}
+
+// grid barrier: false when this or another CTA gave up (abort raised)
+__device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& gen, int* ok_sh) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = gen;
+    bool good = true;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&s->count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(&s->count, 0u);
+      __threadfence();
+      atomicExch(&s->gen, g + 1u);
+    } else {
+      volatile unsigned* vg = &s->gen;
+      volatile int* va = &s->abort;
+      const uint64_t t0 = global_ns();
+      for (uint32_t it = 0;; ++it) {
+        if (*vg != g) break;
+        if ((it & 63u) == 63u) {
+          if (*va) {
+            good = false;
+            break;
+          }
+          if (global_ns() - t0 > WAIT_NS) {
+            atomicExch(&s->abort, 1);
+            atomicCAS(&s->status, 0, 1);
+            good = false;
+            break;
+          }
+        }
+      }
+    }
+    __threadfence();
+    gen = g + 1u;
+    *ok_sh = good && !*(volatile int*)&s->abort;
+  }
+  __syncthreads();
+  return *ok_sh != 0;
+}
+
+constexpr int HT = 512, HW = HT / 32;  // reduction kernel: 16 warps, one CTA per SM
+constexpr int U1 = 4;                  // loads in flight per thread (rows k, y)
+constexpr int U2 = 4;                  // loads in flight per lane (trailing rows)
+
+// A: n x n row-major Hermitian (both triangles), overwritten: row k holds
+// reflector k from column k+1 on.  Y: 2n, P: 2 * gridDim.x scratch.
+__global__ void __launch_bounds__(HT, 1)
+    hetrd_kernel(double2* __restrict__ A, int n, double* __restrict__ d, double* __restrict__ e,
+                 double2* __restrict__ tau, double2* __restrict__ Y, double2* __restrict__ P, Sync* sync) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* vp = reinterpret_cast<double2*>(smem_raw);  // v of step k-1 (pending update)
+  double2* wp = vp + n;                                // w of step k-1
+  double2* vc = wp + n;                                // v of step k
+  __shared__ double red[HW];
+  __shared__ double2 redc[HW];
+  __shared__ double2 s_scale, s_tau, s_dot;
+  __shared__ double s_akk;
+  __shared__ int s_ok;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned G = gridDim.x;
+  unsigned gen = 0;
+  for (int i = tid; i < n; i += HT) {
+    vp[i] = make_double2(0.0, 0.0);
+    wp[i] = make_double2(0.0, 0.0);
+    vc[i] = make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int k = 0; k < n - 1; ++k) {
+    // ---- phase 1 (every CTA): row k with update k-1 applied, reflector k
+    const double2 vpk = vp[k], wpk = wp[k];
+    const double2* rowk = A + (size_t)k * n;
+    double ss = 0.0;
+    for (int base = k + tid; base < n; base += U1 * HT) {
+      double2 a[U1];
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int c = base + u * HT;
+        a[u] = c < n ? __ldcg(&rowk[c]) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int c = base + u * HT;
+        if (c < n) {
+          const double2 x = csub(csub(a[u], cmulc(vpk, wp[c])), cmulc(wpk, vp[c]));
+          if (c == k) {
+            s_akk = x.x;
+          } else {
+            const double2 xc = conjg(x);  // column k below the diagonal
+            vc[c] = xc;
+            if (c >= k + 2) ss += xc.x * xc.x + xc.y * xc.y;
+          }
+        }
+      }
+    }
+    ss = block_sum<HW>(ss, red);  // includes __syncthreads: vc[k+1], s_akk visible
+    if (tid == 0) {
+      const double2 alpha = vc[k + 1];
+      double beta;
+      if (ss == 0.0 && alpha.y == 0.0) {
+        s_tau = make_double2(0.0, 0.0);
+        s_scale = make_double2(0.0, 0.0);
+        beta = alpha.x;
+      } else {
+        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+        s_tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+        const double2 den = make_double2(alpha.x - beta, alpha.y);
+        const double m2 = den.x * den.x + den.y * den.y;
+        s_scale = make_double2(den.x / m2, -den.y / m2);
+      }
+      if (blockIdx.x == 0) {
+        d[k] = s_akk;
+        e[k] = beta;
+        tau[k] = s_tau;
+      }
+    }
+    __syncthreads();
+    const double2 sc = s_scale, tk = s_tau;
+    for (int c = k + 1 + tid; c < n; c += HT) vc[c] = (c == k + 1) ? make_double2(1.0, 0.0) : cmul(vc[c], sc);
+    // reflector k-1 into row k-1, which no CTA reads any more
+    if (blockIdx.x == 0 && k > 0)
+      for (int c = k + tid; c < n; c += HT) __stcg(&A[(size_t)(k - 1) * n + c], vp[c]);
+    __syncthreads();
+
+    // ---- phase 2 (rows split over all warps of the grid): update k-1, y = A v_k
+    const int gw = blockIdx.x * HW + warp, tw = (int)G * HW;
+    double2 pdot = make_double2(0.0, 0.0);
+    for (int r = k + 1 + gw; r < n; r += tw) {
+      const double2 vpr = vp[r], wpr = wp[r];
+      double2* row = A + (size_t)r * n;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int base = k + 1 + lane; base < n; base += 32 * U2) {
+        double2 a[U2];
+#pragma unroll
+        for (int u = 0; u < U2; ++u) {
+          const int c = base + 32 * u;
+          a[u] = c < n ? __ldcg(&row[c]) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < U2; ++u) {
+          const int c = base + 32 * u;
+          if (c < n) {
+            const double2 x = csub(csub(a[u], cmulc(vpr, wp[c])), cmulc(wpr, vp[c]));
+            __stcg(&row[c], x);
+            acc = cadd(acc, cmul(x, vc[c]));
+          }
+        }
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        __stcg(&Y[(size_t)(k & 1) * n + r], acc);
+        pdot = cadd(pdot, cmulc(vc[r], acc));  // conj(y_r) v_r
+      }
+    }
+    if (lane == 0) redc[warp] = pdot;
+    __syncthreads();
+    if (tid == 0) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int w = 0; w < HW; ++w) s = cadd(s, redc[w]);
+      __stcg(&P[(size_t)(k & 1) * G + blockIdx.x], s);
+    }
+    if (!grid_sync(sync, G, gen, &s_ok)) return;
+
+    // ---- phase 3 (every CTA): w_k = tau y - (|tau|^2 / 2)(y^H v) v
+    if (warp == 0) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int base = lane; base < (int)G; base += 32 * U1) {
+        double2 p[U1];
+#pragma unroll
+        for (int u = 0; u < U1; ++u) {
+          const int b = base + 32 * u;
+          p[u] = b < (int)G ? __ldcg(&P[(size_t)(k & 1) * G + b]) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < U1; ++u) s = cadd(s, p[u]);
+      }
+      s = warp_sum(s);
+      if (lane == 0) s_dot = s;
+    }
+    __syncthreads();
+    const double t2 = tk.x * tk.x + tk.y * tk.y;
+    const double2 alph = make_double2(-0.5 * t2 * s_dot.x, -0.5 * t2 * s_dot.y);
+    for (int base = k + 1 + tid; base < n; base += U1 * HT) {
+      double2 y[U1];
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int c = base + u * HT;
+        y[u] = c < n ? __ldcg(&Y[(size_t)(k & 1) * n + c]) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int c = base + u * HT;
+        if (c < n) {
+          const double2 v = vc[c];
+          wp[c] = cadd(cmul(tk, y[u]), cmul(alph, v));
+          vp[c] = v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    if (n == 1) {
+      d[0] = __ldcg(&A[0]).x;
+    } else {
+      double2 a = __ldcg(&A[(size_t)(n - 1) * n + (n - 1)]);
+      a = csub(csub(a, cmulc(vp[n - 1], wp[n - 1])), cmulc(wp[n - 1], vp[n - 1]));
+      d[n - 1] = a.x;
+      __stcg(&A[(size_t)(n - 2) * n + (n - 1)], vp[n - 1]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- eigenvalues
+// Number of eigenvalues of T below x (LDL^T pivots, LAPACK dstebz's guard
+// |q| >= pivmin).
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x, double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int cnt = q < 0.0;
+  for (int i = 1; i < n; ++i) {
+    q = (d[i] - x) - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += q < 0.0;
+  }
+  return cnt;
+}
+
+// Gershgorin bounds and pivmin of T into out[0..2] (one block)
+__global__ void __launch_bounds__(THREADS) bounds_kernel(const double* __restrict__ d, const double* __restrict__ e,
+                                                         int n, double* __restrict__ out) {
+  __shared__ double rmin[WARPS], rmax[WARPS], re2[WARPS];
+  double lo = DBL_MAX, hi = -DBL_MAX, m2 = 0.0;
+  for (int i = threadIdx.x; i < n; i += THREADS) {
+    const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
+    lo = fmin(lo, d[i] - r);
+    hi = fmax(hi, d[i] + r);
+    if (i < n - 1) m2 = fmax(m2, e[i] * e[i]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    rmin[warp] = lo;
+    rmax[warp] = hi;
+    re2[warp] = m2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < WARPS; ++w) {
+      lo = fmin(lo, rmin[w]);
+      hi = fmax(hi, rmax[w]);
+      m2 = fmax(m2, re2[w]);
+    }
+    lo = fmin(lo, rmin[0]);
+    hi = fmax(hi, rmax[0]);
+    m2 = fmax(m2, re2[0]);
+    const double tn = fmax(fabs(lo), fabs(hi));
+    const double pivmin = DBL_MIN * fmax(1.0, m2);
+    out[0] = lo - 2.0 * DBL_EPSILON * tn - 2.0 * pivmin;
+    out[1] = hi + 2.0 * DBL_EPSILON * tn + 2.0 * pivmin;
+    out[2] = pivmin;
+  }
+}
+
+// eigenvalue i0 + j (ascending) of T for j < cnt, one warp each
+__global__ void __launch_bounds__(THREADS) bisect_kernel(const double* __restrict__ d, const double* __restrict__ e,
+                                                         int n, int i0, int cnt, const double* __restrict__ bnd,
+                                                         double* __restrict__ w) {
+  extern __shared__ double sh[];
+  double* sd = sh;
+  double* se2 = sh + n;
+  for (int i = threadIdx.x; i < n; i += THREADS) {
+    sd[i] = d[i];
+    if (i < n - 1) se2[i] = e[i] * e[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * WARPS + (threadIdx.x >> 5);
+  if (j >= cnt) return;
+  const int idx = i0 + j;
+  const double pivmin = bnd[2];
+  double lo = bnd[0], hi = bnd[1];
+  for (int round = 0; round < 40; ++round) {
+    if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+    const double x = lo + (hi - lo) * ((double)(lane + 1) / 33.0);
+    const int c = sturm_count(sd, se2, n, x, pivmin);
+    // count(x) > idx  <=>  eigenvalue idx < x
+    const unsigned above = __ballot_sync(0xffffffffu, c > idx);
+    const int first = above ? __ffs(above) - 1 : 32;
+    const double xl = __shfl_sync(0xffffffffu, x, first > 0 ? first - 1 : 0);
+    const double xh = __shfl_sync(0xffffffffu, x, first < 32 ? first : 31);
+    const double nlo = first == 0 ? lo : xl;
+    const double nhi = first == 32 ? hi : xh;
+    if (nlo == lo && nhi == hi) break;
+    lo = nlo;
+    hi = nhi;
+  }
+  if (lane == 0) w[j] = 0.5 * (lo + hi);
+}
+
+// ---------------------------------------------------------------- eigenvectors
+__device__ __forceinline__ double hash_unit(uint32_t a, uint32_t b) {
+  uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  h *= 0x297A2D39u;
+  h ^= h >> 15;
+  return (double)h * (2.0 / 4294967296.0) - 1.0;
+}
+
+// column j of Z (n x cnt row-major) = eigenvector of T for w[j]; scratch:
+// 4 * n * cnt doubles laid out [i * cnt + j] (coalesced across threads).
+// d, e are staged in shared memory; every sequential loop loads the next CH
+// steps' independent inputs before running their dependent chain.
+constexpr int IV_THREADS = 128, CH = 8;
+__global__ void __launch_bounds__(IV_THREADS) inviter_kernel(const double* __restrict__ d,
+                                                             const double* __restrict__ e, int n, int cnt,
+                                                             const double* __restrict__ w,
+                                                             const double* __restrict__ bnd, double* __restrict__ Z,
+                                                             double* __restrict__ scr) {
+  extern __shared__ double sh_de[];
+  double* sd = sh_de;
+  double* se = sh_de + n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    sd[i] = d[i];
+    se[i] = i < n - 1 ? e[i] : 0.0;
+  }
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cnt) return;
+  const size_t S = (size_t)cnt;
+  double* ua = scr;                       // 1 / u_kk
+  double* uc = scr + 1 * (size_t)n * S;   // u_{k,k+1}
+  double* uc2 = scr + 2 * (size_t)n * S;  // u_{k,k+2}
+  double* ml = scr + 3 * (size_t)n * S;   // multiplier (+4 when rows k, k+1 were swapped)
+  const double lam = w[j];
+  const double tn = fmax(fabs(bnd[0]), fabs(bnd[1]));
+  const double tiny = DBL_EPSILON * fmax(tn, DBL_MIN);
+  // LU of T - lam I with partial pivoting.  The current row k has entries
+  // (ak, ck) at columns (k, k+1); the next original row is (bk, ak1, ck1) at
+  // columns (k, k+1, k+2).  U row k is (ak, ck, 0) without a swap and
+  // (bk, ak1, ck1) with one; |multiplier| <= 1 either way.
+  double ak = sd[0] - lam;
+  double ck = se[0];
+  for (int k = 0; k < n - 1; ++k) {
+    const double bk = se[k];
+    const double ak1 = sd[k + 1] - lam;
+    const double ck1 = se[k + 1];
+    double u_kk, u_k1, u_k2, flagged;
+    if (fabs(ak) >= fabs(bk)) {
+      u_kk = ak == 0.0 ? tiny : ak;
+      u_k1 = ck;
+      u_k2 = 0.0;
+      const double m = bk / u_kk;
+      flagged = m;
+      ak = ak1 - m * ck;
+      ck = ck1;
+    } else {
+      u_kk = bk;
+      u_k1 = ak1;
+      u_k2 = ck1;
+      const double m = ak / bk;
+      flagged = m + 4.0;
+      ak = ck - m * ak1;
+      ck = -m * ck1;
+    }
+    if (fabs(u_kk) < tiny) u_kk = copysign(tiny, u_kk);
+    ua[(size_t)k * S + j] = 1.0 / u_kk;
+    uc[(size_t)k * S + j] = u_k1;
+    uc2[(size_t)k * S + j] = u_k2;
+    ml[(size_t)k * S + j] = flagged;
+  }
+  {
+    double u = ak;
+    if (fabs(u) < tiny) u = copysign(tiny, u == 0.0 ? 1.0 : u);
+    ua[(size_t)(n - 1) * S + j] = 1.0 / u;
+    uc[(size_t)(n - 1) * S + j] = 0.0;
+    uc2[(size_t)(n - 1) * S + j] = 0.0;
+  }
+  double* z = Z;
+#pragma unroll 8
+  for (int i = 0; i < n; ++i) z[(size_t)i * S + j] = hash_unit((uint32_t)j + 1u, (uint32_t)i);
+  for (int it = 0; it < 3; ++it) {
+    // forward: L^-1 with the row swaps
+    double zk = z[j];
+    for (int k0 = 0; k0 < n - 1; k0 += CH) {
+      double mm[CH], zn[CH];
+#pragma unroll
+      for (int u = 0; u < CH; ++u) {
+        const int k = k0 + u;
+        mm[u] = k < n - 1 ? ml[(size_t)k * S + j] : 0.0;
+        zn[u] = k < n - 1 ? z[(size_t)(k + 1) * S + j] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < CH; ++u) {
+        const int k = k0 + u;
+        if (k < n - 1) {
+          if (mm[u] > 2.0) {  // rows k, k+1 swapped
+            z[(size_t)k * S + j] = zn[u];
+            zk = zk - (mm[u] - 4.0) * zn[u];
+          } else {
+            z[(size_t)k * S + j] = zk;
+            zk = zn[u] - mm[u] * zk;
+          }
+        }
+      }
+    }
+    z[(size_t)(n - 1) * S + j] = zk;
+    // backward: U with two super-diagonals
+    double z1 = 0.0, z2 = 0.0, nrm = 0.0;
+    for (int k0 = n - 1; k0 >= 0; k0 -= CH) {
+      double zz[CH], c1[CH], c2[CH], ia[CH];
+#pragma unroll
+      for (int u = 0; u < CH; ++u) {
+        const int k = k0 - u;
+        const bool ok = k >= 0;
+        zz[u] = ok ? z[(size_t)k * S + j] : 0.0;
+        c1[u] = ok ? uc[(size_t)k * S + j] : 0.0;
+        c2[u] = ok ? uc2[(size_t)k * S + j] : 0.0;
+        ia[u] = ok ? ua[(size_t)k * S + j] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < CH; ++u) {
+        const int k = k0 - u;
+        if (k >= 0) {
+          const double v = (zz[u] - c1[u] * z1 - c2[u] * z2) * ia[u];
+          z[(size_t)k * S + j] = v;
+          z2 = z1;
+          z1 = v;
+          nrm += v * v;
+        }
+      }
+    }
+    const double inv = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+#pragma unroll 8
+    for (int i = 0; i < n; ++i) z[(size_t)i * S + j] *= inv;
+  }
+}
+
+// ---------------------------------------------------------------- back-transformation
+// K = Q K with Q = H_0 ... H_{n-2} in blocks of NB reflectors (compact WY:
+// H_k0 ... H_k0+kb-1 = I - V T V^H, LAPACK's forward columnwise larft), the
+// blocks applied from the last to the first, each as three FP64 GEMMs.
+constexpr int NB = 64;
+
+// rows 0..n-2 of A become the reflectors: 0 before column k+1, 1 at k+1
+__global__ void clean_v_kernel(double2* __restrict__ A, int n) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)(n - 1) * n) return;
+  const int k = (int)(idx / n), c = (int)(idx % n);
+  if (c <= k) A[idx] = make_double2(0.0, 0.0);
+  else if (c == k + 1) A[idx] = make_double2(1.0, 0.0);
+}
+
+// minus the NB x NB upper-triangular T of block b from S = V^H V and tau.
+// Thread i owns row i of T (written and read only by itself, in Tg).
+__global__ void __launch_bounds__(NB) larft_kernel(const double2* __restrict__ Sg, const double2* __restrict__ tau,
+                                                   double2* __restrict__ Tg, int n) {
+  __shared__ double2 x[NB];
+  const int b = blockIdx.x, i = threadIdx.x;
+  const int k0 = b * NB, kb = min(NB, n - 1 - k0);
+  const double2* S = Sg + (size_t)b * NB * NB;
+  double2* T = Tg + (size_t)b * NB * NB + (size_t)i * NB;
+  for (int c = 0; c < NB; ++c) T[c] = make_double2(0.0, 0.0);
+  for (int j = 0; j < kb; ++j) {
+    const double2 tj = tau[k0 + j];
+    if (i < j) x[i] = cmul(make_double2(-tj.x, -tj.y), S[(size_t)i * NB + j]);
+    __syncthreads();
+    if (i < j) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int l = i; l < j; ++l) acc = cadd(acc, cmul(T[l], x[l]));
+      T[j] = acc;
+    } else if (i == j) {
+      T[j] = tj;
+    }
+    __syncthreads();
+  }
+  for (int c = 0; c < NB; ++c) T[c] = make_double2(-T[c].x, -T[c].y);
+}
+
+}  // namespace heev
+}  // namespace reno
+
+using namespace reno;
+using namespace reno::heev;
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+namespace {
+struct HeevLayout {
+  size_t sync, y, p, bnd, scr, s, t, w1, w2, total;
+};
+HeevLayout heev_layout(int n, int kt) {
+  HeevLayout L{};
+  const size_t nblk = (size_t)ceil_div(std::max(n - 1, 1), NB);
+  size_t off = 0;
+  L.sync = off;
+  off += align256(sizeof(Sync));
+  L.y = off;
+  off += align256(2 * (size_t)n * sizeof(double2));
+  L.p = off;
+  off += align256(2 * 1024 * sizeof(double2));
+  L.bnd = off;
+  off += align256(4 * sizeof(double));
+  L.scr = off;
+  off += align256(4 * (size_t)n * kt * sizeof(double));
+  L.s = off;
+  off += align256(nblk * NB * NB * sizeof(double2));
+  L.t = off;
+  off += align256(nblk * NB * NB * sizeof(double2));
+  L.w1 = off;
+  off += align256((size_t)NB * kt * sizeof(double2));
+  L.w2 = off;
+  off += align256((size_t)NB * kt * sizeof(double2));
+  L.total = off;
+  return L;
+}
+
+GemmOperand op(const void* p, int64_t s_outer, int64_t s_k, int conj) {
+  GemmOperand o;
+  o.ptr = p;
+  o.s_outer = s_outer;
+  o.s_k = s_k;
+  o.is_complex = 1;
+  o.conj = conj;
+  return o;
+}
+}  // namespace
+
+extern "C" int reno_heev_workspace_bytes(int32_t n, int32_t kt, size_t* bytes) {
+  if (!bytes || n < 1 || n > MAX_N || kt < 1 || kt > n) return RENO_ERR_INVALID;
+  *bytes = heev_layout(n, kt).total;
+  return RENO_OK;
+}
+
+// The reflector rows of v are written in place of the upper triangle of A,
+// so A must be a private copy of G.
+extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, double* d, double* e, void* tau,
+                             double* w, double* Z, void* ws, size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (n < 1 || n > MAX_N || kt < 1 || kt > n)
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heev_top: need 1 <= kt <= n <= 4096");
+  if (!A || !d || !e || !tau || !w || !Z || !ws) return set_error(ctx, RENO_ERR_INVALID, "reno_heev_top: null pointer");
+  const HeevLayout L = heev_layout(n, kt);
+  if (ws_bytes < L.total) return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heev_top: workspace too small");
+  char* base = static_cast<char*>(ws);
+  Sync* sync = reinterpret_cast<Sync*>(base + L.sync);
+  double2* Y = reinterpret_cast<double2*>(base + L.y);
+  double2* P = reinterpret_cast<double2*>(base + L.p);
+  double* bnd = reinterpret_cast<double*>(base + L.bnd);
+  double* scr = reinterpret_cast<double*>(base + L.scr);
+  cudaStream_t st = ctx->stream;
+  int rc = check_cuda(ctx, cudaMemsetAsync(sync, 0, sizeof(Sync), st), "reno_heev_top: memset");
+  if (rc != RENO_OK) return rc;
+  static bool attr_set = false;
+  if (!attr_set) {
+    rc = check_cuda(ctx, cudaFuncSetAttribute(hetrd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * MAX_N * 16),
+                    "reno_heev_top: hetrd smem attribute");
+    if (rc == RENO_OK)
+      rc = check_cuda(ctx, cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                2 * MAX_N * (int)sizeof(double)),
+                      "reno_heev_top: bisect smem attribute");
+    if (rc == RENO_OK)
+      rc = check_cuda(ctx, cudaFuncSetAttribute(inviter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                2 * MAX_N * (int)sizeof(double)),
+                      "reno_heev_top: inverse iteration smem attribute");
+    if (rc != RENO_OK) return rc;
+    attr_set = true;
+  }
+  // 1. tridiagonal reduction: one CTA per SM, all co-resident (cooperative launch)
+  const size_t smem = 3 * (size_t)n * sizeof(double2);
+  int per_sm = 0;
+  rc = check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_kernel, HT, smem),
+                  "reno_heev_top: occupancy");
+  if (rc != RENO_OK) return rc;
+  if (per_sm < 1) return set_error(ctx, RENO_ERR_INVALID, "reno_heev_top: hetrd kernel does not fit on an SM");
+  unsigned grid = (unsigned)std::min(ctx->num_sms, 1024);
+  double2* Ac = static_cast<double2*>(A);
+  double2* tauc = static_cast<double2*>(tau);
+  int nn = n;
+  void* args[] = {&Ac, &nn, &d, &e, &tauc, &Y, &P, &sync};
+  count_launch();
+  rc = check_cuda(ctx, cudaLaunchCooperativeKernel((void*)hetrd_kernel, dim3(grid), dim3(HT), args, smem, st),
+                  "reno_heev_top: hetrd launch");
+  if (rc != RENO_OK) return rc;
+  // 2. eigenvalues n-kt .. n-1 (ascending)
+  count_launch();
+  bounds_kernel<<<1, THREADS, 0, st>>>(d, e, n, bnd);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bounds");
+  count_launch();
+  bisect_kernel<<<(unsigned)ceil_div(kt, WARPS), THREADS, 2 * (size_t)n * sizeof(double), st>>>(d, e, n, n - kt, kt,
+                                                                                                 bnd, w);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bisect");
+  // 3. eigenvectors of T
+  count_launch();
+  inviter_kernel<<<(unsigned)ceil_div(kt, IV_THREADS), IV_THREADS, 2 * (size_t)n * sizeof(double), st>>>(
+      d, e, n, kt, w, bnd, Z, scr);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: inverse iteration");
+  return RENO_OK;
+}
+
+// K (n x kt complex128, in: eigenvectors of T, out: Q K) after reno_heev_top
+// on the same A, tau and workspace; A's reflector rows are cleaned in place.
+extern "C" int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, void* A, const void* tau, void* K,
+                                       void* ws, size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (n < 1 || n > MAX_N || kt < 1 || kt > n || !A || !tau || !K || !ws)
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform: invalid arguments");
+  const HeevLayout L = heev_layout(n, kt);
+  if (ws_bytes < L.total) return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heev_backtransform: workspace too small");
+  if (n == 1) return RENO_OK;
+  char* base = static_cast<char*>(ws);
+  double2* Sg = reinterpret_cast<double2*>(base + L.s);
+  double2* Tg = reinterpret_cast<double2*>(base + L.t);
+  double2* W1 = reinterpret_cast<double2*>(base + L.w1);
+  double2* W2 = reinterpret_cast<double2*>(base + L.w2);
+  double2* V = static_cast<double2*>(A);
+  double2* Kc = static_cast<double2*>(K);
+  cudaStream_t st = ctx->stream;
+  const int nblk = (int)ceil_div(n - 1, NB);
+  const size_t nel = (size_t)(n - 1) * n;
+  count_launch();
+  clean_v_kernel<<<(unsigned)ceil_div((int64_t)nel, 256), 256, 0, st>>>(V, n);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: clean");
+  int rc = check_cuda(ctx, cudaMemsetAsync(Sg, 0, (size_t)nblk * NB * NB * sizeof(double2), st),
+                      "reno_heev_backtransform: memset");
+  if (rc != RENO_OK) return rc;
+  // S_b = V_b^H V_b over the columns the block's reflectors touch
+  for (int b = 0; b < nblk; ++b) {
+    const int k0 = b * NB, kb = std::min(NB, n - 1 - k0);
+    GemmParams p;
+    p.M = kb;
+    p.N = kb;
+    p.K = n - k0 - 1;
+    p.A = op(V + (size_t)k0 * n + k0 + 1, n, 1, 1);
+    p.B = op(V + (size_t)k0 * n + k0 + 1, n, 1, 0);
+    p.C = Sg + (size_t)b * NB * NB;
+    p.sCm = NB;
+    p.sCn = 1;
+    count_launch();
+    rc = check_cuda(ctx, gemm_fp64(p, st), "reno_heev_backtransform: gram");
+    if (rc != RENO_OK) return rc;
+  }
+  count_launch();
+  larft_kernel<<<nblk, NB, 0, st>>>(Sg, static_cast<const double2*>(tau), Tg, n);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: larft");
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int k0 = b * NB, kb = std::min(NB, n - 1 - k0);
+    const int rows = n - k0 - 1;
+    // W1 = V_b^H K[k0+1:]
+    GemmParams p1;
+    p1.M = kb;
+    p1.N = kt;
+    p1.K = rows;
+    p1.A = op(V + (size_t)k0 * n + k0 + 1, n, 1, 1);
+    p1.B = op(Kc + (size_t)(k0 + 1) * kt, 1, kt, 0);
+    p1.C = W1;
+    p1.sCm = kt;
+    p1.sCn = 1;
+    // W2 = (-T_b) W1
+    GemmParams p2;
+    p2.M = kb;
+    p2.N = kt;
+    p2.K = kb;
+    p2.A = op(Tg + (size_t)b * NB * NB, NB, 1, 0);
+    p2.B = op(W1, 1, kt, 0);
+    p2.C = W2;
+    p2.sCm = kt;
+    p2.sCn = 1;
+    // K[k0+1:] += V_b W2
+    GemmParams p3;
+    p3.M = rows;
+    p3.N = kt;
+    p3.K = kb;
+    p3.A = op(V + (size_t)k0 * n + k0 + 1, 1, n, 0);
+    p3.B = op(W2, 1, kt, 0);
+    p3.C = Kc + (size_t)(k0 + 1) * kt;
+    p3.sCm = kt;
+    p3.sCn = 1;
+    p3.accumulate = 1;
+    count_launch(3);
+    rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K");
+    if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64(p2, st), "reno_heev_backtransform: T W");
+    if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64(p3, st), "reno_heev_backtransform: K += V W");
+    if (rc != RENO_OK) return rc;
+  }
+  return RENO_OK;
+}
+
+// status word of the last reno_heev_top on a workspace: the int at this
+// byte offset of ws (0 = ok, 1 = a grid barrier timed out)
+extern "C" int reno_heev_status_offset(size_t* offset) {
+  if (!offset) return RENO_ERR_INVALID;
+  *offset = offsetof(Sync, status);
+  return RENO_OK;
+}

@@ -26,6 +26,7 @@ import numpy as np
 import torch
 
 from ._native import Engine, h2d
+from . import heev
 
 
 def add_outer(a: np.ndarray, b: np.ndarray) -> np.ndarray:
@@ -358,7 +359,23 @@ def _subspace_block(eng, X, keep_left, k, opts, Q=None, iters=None):
     return K, Ph.transpose(0, 1).conj().resolve_conj(), S, chk, Q
 
 
-def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optional[int] = None) -> dict:
+def _gram_eigh(eng: Engine, G: torch.Tensor, kt: int, use_heev: bool):
+    """Eigenpairs of the Gram matrix G, descending: (w, V, check).  With the
+    device eigensolver (``heev.heev_opts``) only the leading kt are computed
+    (w has kt entries) and check is its device-side acceptance triple;
+    otherwise cuSOLVER's full decomposition and check None."""
+    n = G.shape[0]
+    if use_heev and heev.heev_opts.enabled and kt < n and n >= heev.heev_opts.min_n and G.is_cuda:
+        w, V, chk = heev.heev_top(eng, G, kt)
+        if not G.is_complex():
+            V = V.real.contiguous()
+        return w, V, chk
+    w, V = torch.linalg.eigh(G)
+    return torch.flip(w, dims=[0]), torch.flip(V, dims=[1]), None
+
+
+def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optional[int] = None,
+                    use_heev: bool = True) -> dict:
     """Kept-side basis K, projection P and sigma S of one block from the full
     Gram eigendecomposition of its smaller side (all min(m, n) triplets).
 
@@ -378,20 +395,21 @@ def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optiona
     kt = dim if ktop is None else min(int(ktop), dim)
 
     def tail(w_desc, head):
-        t = torch.sqrt(torch.clamp(w_desc[kt:dim], min=0.0))
+        # the device eigensolver returns only the leading kt eigenvalues: the
+        # others then read as 0, which the cap below reaches anyway
+        t = torch.sqrt(torch.clamp(w_desc[kt:dim], min=0.0)) if w_desc.numel() >= dim else \
+            torch.zeros(dim - kt, dtype=torch.float64, device=head.device)
         return torch.minimum(t, head.min()) if kt < dim and head.numel() else t
 
     if keep_left and m <= n:
         G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-        w, K = torch.linalg.eigh(G)
-        K, w = torch.flip(K, dims=[1]), torch.flip(w, dims=[0])
+        w, K, chk = _gram_eigh(eng, G, kt, use_heev)
         P = eng.matmul(K[:, :kt].transpose(0, 1), X, conj_a=True)           # (kt, n) = sigma Vh
         S = torch.linalg.vector_norm(P, dim=1)
         S = torch.cat([S, tail(w, S)])
     elif keep_left:
         G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-        w, V = torch.linalg.eigh(G)
-        V, w = torch.flip(V, dims=[1]), torch.flip(w, dims=[0])
+        w, V, chk = _gram_eigh(eng, G, kt, use_heev)
         Us = eng.matmul(X, V[:, :kt])                                        # (m, kt) = U sigma
         S = torch.linalg.vector_norm(Us, dim=0)
         S = torch.cat([S, tail(w, S)])
@@ -399,21 +417,19 @@ def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optiona
         P = eng.matmul(K.transpose(0, 1), X, conj_a=True)
     elif n <= m:
         G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-        w, K = torch.linalg.eigh(G)
-        K, w = torch.flip(K, dims=[1]), torch.flip(w, dims=[0])
+        w, K, chk = _gram_eigh(eng, G, kt, use_heev)
         P = eng.matmul(X, K[:, :kt])                                         # (m, kt) = U sigma
         S = torch.linalg.vector_norm(P, dim=0)
         S = torch.cat([S, tail(w, S)])
     else:
         G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-        w, U = torch.linalg.eigh(G)
-        U, w = torch.flip(U, dims=[1]), torch.flip(w, dims=[0])
+        w, U, chk = _gram_eigh(eng, G, kt, use_heev)
         Vs = eng.matmul(X.transpose(0, 1), U[:, :kt], conj_a=True)           # (n, kt): sigma v
         S = torch.linalg.vector_norm(Vs, dim=0)
         S = torch.cat([S, tail(w, S)])
         K, _ = torch.linalg.qr(Vs, mode="reduced")
         P = eng.matmul(X, K)
-    return dict(K=K, P=P, S=S, dim=dim)
+    return dict(K=K, P=P, S=S, dim=dim, chk=chk)
 
 
 def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_trunc_fn, percent=0,
@@ -466,15 +482,28 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         full = _full_kept_side(eng, X, keep_left, ktop)
         K, P, S = full["K"], full["P"], full["S"]
         npad = upad if keep_left else vpad
-        blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=dim, npad=npad))
+        blk = dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=dim, npad=npad)
+        if full["chk"] is not None:
+            blk.update(chk=full["chk"], X=X, ktop=ktop)
+        blocks.append(blk)
     if not blocks:
         raise ValueError("Invalid quantum number")
     sub = [b for b in blocks if "res" in b]
-    host = torch.cat([b["S"] for b in blocks] + [b["res"] for b in sub]).cpu().numpy()
+    dev_eig = [b for b in blocks if "chk" in b]
+    host = torch.cat([b["S"] for b in blocks] + [b["res"] for b in sub] + [b["chk"] for b in dev_eig]).cpu().numpy()
     off = 0
     for b in blocks:
         b["Sh"] = host[off:off + b["dim"]]
         off += b["dim"]
+    off_chk = off + 2 * len(sub)
+    for i, b in enumerate(dev_eig):
+        if not heev.accepted(host[off_chk + 3 * i: off_chk + 3 * i + 3]):
+            # the device eigensolver missed its checks on this block: cuSOLVER
+            heev.heev_opts.fallbacks += 1
+            b.update(_full_kept_side(eng, b["X"], keep_left, b["ktop"], use_heev=False))
+            b["Sh"] = b["S"].cpu().numpy()
+        b.pop("X", None)
+        b.pop("chk", None)
     ok = lambda e, f: bool(np.isfinite(e) and e <= subspace.rtol * f)
     retry = []
     for b in sub:
