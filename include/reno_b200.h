@@ -132,6 +132,23 @@ int reno_heff_apply_noalloc(reno_ctx* ctx, const reno_heff_desc* desc,
                             const void* L, const void* W1, const void* W2,
                             const void* R, const void* psi, void* y);
 
+/* Grouped FP64 matvec for many independent local problems (static-disorder
+ * realisations advanced in lockstep; the reference evolves each MPS on its
+ * own through hop_expr.py:57-103): count (1..128) descriptors with the same
+ * nsite and dtypes, each with its own dimensions; L, W1, W2, R, psi, y are
+ * host arrays of count device pointers (W1 / W2 unused below 1 / 2 sites).
+ * One launch transposes every MPO tensor, then each contraction stage is one
+ * grouped GEMM launch; every problem's result is its reno_heff_apply result
+ * at RENO_PREC_FP64.  Workspace from reno_heff_grouped_workspace_bytes. */
+int reno_heff_grouped_workspace_bytes(int32_t count,
+                                      const reno_heff_desc* descs,
+                                      size_t* bytes);
+int reno_heff_apply_grouped(reno_ctx* ctx, int32_t count,
+                            const reno_heff_desc* descs, const void* const* L,
+                            const void* const* W1, const void* const* W2,
+                            const void* const* R, const void* const* psi,
+                            void* const* y, void* ws, size_t ws_bytes);
+
 /* Leading eigenpairs of a Hermitian Gram block for the truncation
  * (svd_qn.py:12-49 optimized_svd / mp.py:693-778, where the reference takes
  * LAPACK gesdd of the block; the engine diagonalises the block's Gram matrix).

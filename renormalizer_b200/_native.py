@@ -52,6 +52,10 @@ _SIGS = {
     "reno_device_error": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
     "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),
+    "reno_heff_grouped_workspace_bytes": (_c_int, [_c_int, ctypes.POINTER(HeffDesc), ctypes.POINTER(_c_sz)]),
+    "reno_heff_apply_grouped": (_c_int, [_vp, _c_int, ctypes.POINTER(HeffDesc), ctypes.POINTER(_vp),
+                                         ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                         ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp, _c_sz]),
     "reno_heev_workspace_bytes": (_c_int, [_c_int, _c_int, ctypes.POINTER(_c_sz)]),
     "reno_heev_top": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
     "reno_heev_backtransform": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _c_sz]),
@@ -249,6 +253,22 @@ class Engine:
         c = ctypes.c_int32(0)
         self.check(self.lib.reno_device_error(self.ctx, ctypes.byref(c)), "reno_device_error")
         return int(c.value)
+
+    def heff_apply_grouped(self, descs, Ls, W1s, W2s, Rs, psis, ys):
+        """reno_heff_apply_grouped (FP64): lists of equal length; W1s / W2s
+        entries None below one / two active sites"""
+        m = len(descs)
+        arr = (HeffDesc * m)(*descs)
+        n = _c_sz()
+        self.check(self.lib.reno_heff_grouped_workspace_bytes(m, arr, ctypes.byref(n)),
+                   "reno_heff_grouped_workspace_bytes")
+        ws = self.workspace(int(n.value))
+        pa = lambda ts: (_vp * m)(*[_vp(t.data_ptr()) if t is not None else None for t in ts])
+        for t in list(Ls) + list(Rs) + list(psis) + list(ys) + [w for w in list(W1s) + list(W2s) if w is not None]:
+            ptr(t)  # contiguity / lazy-view checks
+        self.check(self.lib.reno_heff_apply_grouped(self.ctx, m, arr, pa(Ls), pa(W1s), pa(W2s), pa(Rs), pa(psis),
+                                                    pa(ys), ptr(ws), ws.numel()), "reno_heff_apply_grouped")
+        self.launches += 1
 
     def heev_top(self, A, d, e, tau, w, Z, ws):
         """reno_heev_top: tridiagonal reduction of A (overwritten), top eigenvalues

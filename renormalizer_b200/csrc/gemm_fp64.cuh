@@ -93,8 +93,9 @@ __device__ __forceinline__ void load_tile(void* smem, const GemmOperand& op, con
   }
 }
 
+// one BM x BN output tile (tile column bx, tile row by, batch entry bz) of p
 template <bool AC, bool BC>
-__global__ void __launch_bounds__(THREADS) gemm_kernel(GemmParams p) {
+__device__ __forceinline__ void gemm_tile(const GemmParams& p, int bx, int by, int bz) {
   constexpr bool CC = AC || BC;
   using TA = typename std::conditional<AC, double2, double>::type;
   using TB = typename std::conditional<BC, double2, double>::type;
@@ -104,8 +105,8 @@ __global__ void __launch_bounds__(THREADS) gemm_kernel(GemmParams p) {
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm0 = (warp & 1) * 32, wn0 = (warp >> 1) * 32;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int64_t b = blockIdx.z;
+  const int m0 = by * BM, n0 = bx * BN;
+  const int64_t b = bz;
   const char* baseA = reinterpret_cast<const char*>(p.A.ptr) + b * p.A.s_batch * sizeof(TA);
   const char* baseB = reinterpret_cast<const char*>(p.B.ptr) + b * p.B.s_batch * sizeof(TB);
 
@@ -209,6 +210,36 @@ __global__ void __launch_bounds__(THREADS) gemm_kernel(GemmParams p) {
 }
 
 template <bool AC, bool BC>
+__global__ void __launch_bounds__(THREADS) gemm_kernel(GemmParams p) {
+  gemm_tile<AC, BC>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Many independent GEMMs (same operand types) in one launch: CTA t runs tile
+// t - first[i] of problem i, first[i] <= t < first[i + 1], tiles of a problem
+// numbered like the single launch's grid (x fastest, then y, then batch).
+constexpr int MAX_GROUP = 128;
+struct GemmGroup {
+  int count = 0;
+  int first[MAX_GROUP + 1] = {};
+  GemmParams p[MAX_GROUP];
+};
+
+template <bool AC, bool BC>
+__global__ void __launch_bounds__(THREADS) gemm_grouped_kernel(const __grid_constant__ GemmGroup g) {
+  const int t = blockIdx.x;
+  int lo = 0, hi = g.count;  // first[lo] <= t < first[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (g.first[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  const GemmParams& p = g.p[lo];
+  const int lt = t - g.first[lo];
+  const int nx = (int)ceil_div(p.N, BN), ny = (int)ceil_div(p.M, BM);
+  gemm_tile<AC, BC>(p, lt % nx, (lt / nx) % ny, lt / (nx * ny));
+}
+
+template <bool AC, bool BC>
 inline size_t smem_bytes() {
   return STAGES * (BM * BKP * (AC ? 16 : 8) + BN * BKP * (BC ? 16 : 8));
 }
@@ -229,7 +260,45 @@ inline cudaError_t launch_t(const GemmParams& p, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <bool AC, bool BC>
+inline cudaError_t launch_grouped_t(const GemmGroup& g, cudaStream_t st) {
+  const size_t sm = smem_bytes<AC, BC>();
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(gemm_grouped_kernel<AC, BC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  if (g.first[g.count] == 0) return cudaSuccess;
+  count_launch();
+  gemm_grouped_kernel<AC, BC><<<g.first[g.count], THREADS, sm, st>>>(g);
+  return cudaGetLastError();
+}
+
 }  // namespace fp64gemm
+
+// Launch a group of FP64 GEMMs whose operands all have the same types (tile
+// counts filled in here); returns a CUDA error code.
+inline cudaError_t gemm_fp64_grouped(fp64gemm::GemmGroup& g, cudaStream_t st) {
+  if (g.count < 1 || g.count > fp64gemm::MAX_GROUP) return cudaErrorInvalidValue;
+  const bool ac = g.p[0].A.is_complex, bc = g.p[0].B.is_complex;
+  g.first[0] = 0;
+  for (int i = 0; i < g.count; ++i) {
+    const GemmParams& p = g.p[i];
+    if (p.A.is_f32 || p.B.is_f32 || p.c_f32 || (bool)p.A.is_complex != ac || (bool)p.B.is_complex != bc)
+      return cudaErrorInvalidValue;
+    const int64_t tiles = (p.M > 0 && p.N > 0 && p.batch > 0)
+                              ? ceil_div(p.N, fp64gemm::BN) * ceil_div(p.M, fp64gemm::BM) * p.batch
+                              : 0;
+    if (g.first[i] + tiles > 0x7fffffff) return cudaErrorInvalidValue;
+    g.first[i + 1] = g.first[i] + (int)tiles;
+  }
+  if (ac && bc) return fp64gemm::launch_grouped_t<true, true>(g, st);
+  if (ac) return fp64gemm::launch_grouped_t<true, false>(g, st);
+  if (bc) return fp64gemm::launch_grouped_t<false, true>(g, st);
+  return fp64gemm::launch_grouped_t<false, false>(g, st);
+}
 
 // Launch the FP64 GEMM; returns a CUDA error code.
 inline cudaError_t gemm_fp64(const GemmParams& p, cudaStream_t st) {

@@ -14,6 +14,8 @@
 #include "reno_common.cuh"
 #include "gemm_fp64.cuh"
 #include "split_gemm.cuh"
+#include <algorithm>
+#include <memory>
 #include <vector>
 
 namespace reno {
@@ -490,6 +492,126 @@ extern "C" int reno_heff_apply(reno_ctx* ctx, const reno_heff_desc* d, const voi
     e = run_stage(s, w + lay.off_split, need_split, st);
   }
   return check_cuda(ctx, e, "reno_heff_apply");
+}
+
+// ---------------------------------------------------------------- grouped FP64 matvec
+// Many independent local problems (static-disorder realisations, each with
+// its own bond dimensions) advanced together: one launch transposes every
+// problem's MPO tensors, then each stage of the contraction chain is one
+// grouped GEMM launch over all problems.  Every problem's arithmetic is that
+// of its own reno_heff_apply at FP64 (same stages, same tiles).
+namespace reno {
+constexpr int MAX_WT = 2 * fp64gemm::MAX_GROUP;
+struct WtGroup {
+  int count = 0;
+  const void* W[MAX_WT] = {};
+  void* Wt[MAX_WT] = {};
+  int nc[MAX_WT] = {}, d[MAX_WT] = {}, nr[MAX_WT] = {};
+};
+
+template <typename T>
+__global__ void wt_grouped_kernel(const __grid_constant__ WtGroup g) {
+  const int i = blockIdx.y;
+  const T* __restrict__ W = static_cast<const T*>(g.W[i]);
+  T* __restrict__ Wt = static_cast<T*>(g.Wt[i]);
+  const int nc = g.nc[i], d = g.d[i], nr = g.nr[i];
+  const int64_t total = (int64_t)d * nr * nc * d;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int e = idx % d;
+    const int c = (idx / d) % nc;
+    const int r = (idx / ((int64_t)d * nc)) % nr;
+    const int dd = idx / ((int64_t)d * nc * nr);
+    Wt[idx] = W[(((int64_t)c * d + dd) * d + e) * nr + r];
+  }
+}
+
+static int validate_group(int32_t count, const reno_heff_desc* descs) {
+  if (count < 1 || count > fp64gemm::MAX_GROUP || !descs) return RENO_ERR_INVALID;
+  for (int i = 0; i < count; ++i) {
+    const reno_heff_desc* d = descs + i;
+    if (validate_heff(d) != RENO_OK || d->prec != RENO_PREC_FP64) return RENO_ERR_INVALID;
+    if (d->nsite != descs[0].nsite || d->psi_dtype != descs[0].psi_dtype || d->env_dtype != descs[0].env_dtype ||
+        d->mpo_dtype != descs[0].mpo_dtype)
+      return RENO_ERR_INVALID;
+  }
+  return RENO_OK;
+}
+}  // namespace reno
+
+extern "C" int reno_heff_grouped_workspace_bytes(int32_t count, const reno_heff_desc* descs, size_t* bytes) {
+  if (!bytes || validate_group(count, descs) != RENO_OK) return RENO_ERR_INVALID;
+  size_t total = 0;
+  for (int i = 0; i < count; ++i) total += align256(heff_layout(descs + i).off_split);
+  *bytes = total;
+  return RENO_OK;
+}
+
+extern "C" int reno_heff_apply_grouped(reno_ctx* ctx, int32_t count, const reno_heff_desc* descs,
+                                       const void* const* L, const void* const* W1, const void* const* W2,
+                                       const void* const* R, const void* const* psi, void* const* y, void* ws,
+                                       size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (validate_group(count, descs) != RENO_OK)
+    return set_error(ctx, RENO_ERR_INVALID,
+                     "reno_heff_apply_grouped: 1..128 valid FP64 descriptors with the same nsite and dtypes");
+  if (!L || !R || !psi || !y || (descs[0].nsite >= 1 && !W1) || (descs[0].nsite == 2 && !W2))
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply_grouped: null pointer array");
+  size_t need = 0;
+  reno_heff_grouped_workspace_bytes(count, descs, &need);
+  if (!ws || ws_bytes < need) return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heff_apply_grouped: workspace too small");
+  const int nsite = descs[0].nsite;
+  cudaStream_t st = ctx->stream;
+  std::vector<std::vector<Stage>> stages(count);
+  std::unique_ptr<WtGroup> wg(new WtGroup());
+  int64_t max_wt = 0;
+  size_t off = 0;
+  for (int i = 0; i < count; ++i) {
+    const reno_heff_desc* d = descs + i;
+    if (!L[i] || !R[i] || !psi[i] || !y[i] || (nsite >= 1 && !W1[i]) || (nsite == 2 && !W2[i]))
+      return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply_grouped: null tensor pointer");
+    const HeffLayout lay = heff_layout(d);
+    char* w = static_cast<char*>(ws) + off;
+    off += align256(lay.off_split);
+    if (nsite >= 1) {
+      const int k = wg->count++;
+      wg->W[k] = W1[i];
+      wg->Wt[k] = w + lay.off_wt1;
+      wg->nc[k] = d->wl;
+      wg->d[k] = d->d1;
+      wg->nr[k] = nsite == 2 ? d->wm : d->wr;
+      max_wt = std::max(max_wt, (int64_t)d->d1 * d->d1 * d->wl * wg->nr[k]);
+    }
+    if (nsite == 2) {
+      const int k = wg->count++;
+      wg->W[k] = W2[i];
+      wg->Wt[k] = w + lay.off_wt2;
+      wg->nc[k] = d->wm;
+      wg->d[k] = d->d2;
+      wg->nr[k] = d->wr;
+      max_wt = std::max(max_wt, (int64_t)d->d2 * d->d2 * d->wm * d->wr);
+    }
+    stages[i] = heff_stages(d, lay, w, L[i], R[i], psi[i], y[i]);
+    if (stages[i].size() != stages[0].size())
+      return set_error(ctx, RENO_ERR_INVALID, "reno_heff_apply_grouped: mixed contraction chains");
+  }
+  if (wg->count > 0) {
+    const dim3 grid((unsigned)std::min<int64_t>(ceil_div(max_wt, 256), 64), (unsigned)wg->count);
+    count_launch();
+    if (descs[0].mpo_dtype == RENO_C128)
+      wt_grouped_kernel<double2><<<grid, 256, 0, st>>>(*wg);
+    else
+      wt_grouped_kernel<double><<<grid, 256, 0, st>>>(*wg);
+    RENO_LAUNCH_CHECK(ctx, "reno_heff_apply_grouped: MPO transposes");
+  }
+  std::unique_ptr<fp64gemm::GemmGroup> g(new fp64gemm::GemmGroup());
+  for (size_t s = 0; s < stages[0].size(); ++s) {
+    g->count = count;
+    for (int i = 0; i < count; ++i) g->p[i] = stages[i][s].p;
+    const int rc = check_cuda(ctx, gemm_fp64_grouped(*g, st), "reno_heff_apply_grouped: stage");
+    if (rc != RENO_OK) return rc;
+  }
+  return RENO_OK;
 }
 
 // ---------------------------------------------------------------- env update

@@ -9,6 +9,7 @@ arithmetic (FP64 DMMA or BF16x3 / TF32x3 split products).
 """
 from __future__ import annotations
 
+import ctypes
 from typing import List, Sequence
 
 import numpy as np
@@ -106,6 +107,50 @@ class HeffOperator:
         if isinstance(psi, np.ndarray):
             psi = as_device(psi, self.L.device)
         return self.apply(psi)
+
+
+MAX_GROUP = 128  # problems per grouped launch (reno_heff_apply_grouped)
+
+
+def apply_grouped(ops: Sequence["HeffOperator"], psis: Sequence[torch.Tensor]) -> List[torch.Tensor]:
+    """[op.apply(psi) for op, psi in zip(ops, psis)] for independent local
+    problems.  FP64 operators with the same number of sites and dtypes go
+    through reno_heff_apply_grouped, up to 128 per launch; split-precision
+    operators (whose fused chains are not grouped) are applied one by one.
+    Each result equals that operator's own apply."""
+    ys: List[torch.Tensor] = [None] * len(ops)
+    batch = {}
+    for i, (op, psi) in enumerate(zip(ops, psis)):
+        psi = psi.reshape(op.cshape)
+        if not psi.is_contiguous():
+            psi = psi.contiguous()
+        if psi.dtype not in (torch.float64, torch.complex128):
+            psi = psi.to(torch.complex128 if psi.is_complex() else torch.float64)
+        if op.prec != "fp64":
+            ys[i] = op.apply(psi)
+            continue
+        key = (op.nsite, dtype_code(psi), op.desc.env_dtype, op.desc.mpo_dtype, op.L.device)
+        batch.setdefault(key, []).append((i, psi))
+    for items in batch.values():
+        for c0 in range(0, len(items), MAX_GROUP):
+            chunk = items[c0:c0 + MAX_GROUP]
+            descs, outs = [], []
+            for i, psi in chunk:
+                op = ops[i]
+                d = HeffDesc()
+                ctypes.pointer(d)[0] = op.desc
+                d.psi_dtype = dtype_code(psi)
+                descs.append(d)
+                outs.append(torch.empty(op.cshape, dtype=op.out_dtype(psi), device=psi.device))
+            sel = [ops[i] for i, _ in chunk]
+            eng = sel[0].engine
+            eng.sync_stream()
+            eng.heff_apply_grouped(descs, [o.L for o in sel], [o.W[0] if o.nsite >= 1 else None for o in sel],
+                                   [o.W[1] if o.nsite == 2 else None for o in sel], [o.R for o in sel],
+                                   [psi for _, psi in chunk], outs)
+            for (i, _), y in zip(chunk, outs):
+                ys[i] = y
+    return ys
 
 
 def hop_expr(ltensor, rtensor, cmo: List, cshape, twolayer: bool = False):

@@ -64,11 +64,13 @@ class _Krylov:
         return out
 
 
-def expm_krylov(Afunc, dt, vstart, block_size=50):
-    """Krylov approximation of expm(dt*A) @ vstart for Hermitian A.
-
-    Returns (vector, number of matvecs) like the reference.  ``Afunc`` maps a
-    1-D device vector to a device vector (e.g. a HeffOperator)."""
+def _expm_krylov_steps(dt, vstart, block_size=50):
+    """The Lanczos exponential as a generator: it yields each Krylov vector
+    whose image under the operator it needs and receives that image, and
+    returns (vector, number of matvecs).  ``expm_krylov`` serves it one
+    operator; ``expm_krylov_batch`` serves many in lockstep, one grouped
+    matvec per round, with every instance's arithmetic and decisions exactly
+    those of its own expm_krylov."""
     if not np.iscomplex(dt):
         dt = dt.real
     v = as_device(vstart).reshape(-1)
@@ -112,7 +114,7 @@ def expm_krylov(Afunc, dt, vstart, block_size=50):
         return None
 
     for j in range(n):
-        w = Afunc(K.V[j]).reshape(-1)
+        w = (yield K.V[j]).reshape(-1)
         if w.dtype != work_dtype:
             w = w.to(work_dtype)
         if not w.is_contiguous():
@@ -141,3 +143,48 @@ def expm_krylov(Afunc, dt, vstart, block_size=50):
                 if float(K.scal[2].item()) == 1.0:
                     return new_res, j + 1
             state["res"] = new_res
+
+
+def expm_krylov(Afunc, dt, vstart, block_size=50):
+    """Krylov approximation of expm(dt*A) @ vstart for Hermitian A.
+
+    Returns (vector, number of matvecs) like the reference.  ``Afunc`` maps a
+    1-D device vector to a device vector (e.g. a HeffOperator)."""
+    gen = _expm_krylov_steps(dt, vstart, block_size)
+    try:
+        x = next(gen)
+        while True:
+            x = gen.send(Afunc(x))
+    except StopIteration as stop:
+        return stop.value
+
+
+def expm_krylov_batch(group_apply, dts, vstarts, block_size=50):
+    """expm_krylov for many independent problems in lockstep (static-disorder
+    realisations, not in the reference).  ``group_apply(idx, xs)`` maps the
+    Krylov vectors xs of the problems idx (a list) to their images, normally
+    in one grouped launch (hop_expr.apply_grouped); ``dts`` is one step for
+    all or one per problem.  Returns [(vector, number of matvecs)] in input
+    order, each identical to that problem's own expm_krylov."""
+    m = len(vstarts)
+    if np.ndim(dts) == 0:
+        dts = [dts] * m
+    gens = [_expm_krylov_steps(dt, v, block_size) for dt, v in zip(dts, vstarts)]
+    out = [None] * m
+    pending = {}
+    for i, g in enumerate(gens):
+        try:
+            pending[i] = next(g)
+        except StopIteration as stop:
+            out[i] = stop.value
+    while pending:
+        idx = sorted(pending)
+        ys = group_apply(idx, [pending[i] for i in idx])
+        nxt = {}
+        for i, y in zip(idx, ys):
+            try:
+                nxt[i] = gens[i].send(y)
+            except StopIteration as stop:
+                out[i] = stop.value
+        pending = nxt
+    return out

@@ -804,23 +804,41 @@ class Mps:
     # ------------------------------------------------------------ time evolution
     def evolve(self, mpo: Mpo, evolve_dt, normalize=True) -> "Mps":
         """mps.py:644-662"""
-        method = self.evolve_config.method
-        if method == EvolveMethod.tdvp_ps:
-            new = self._evolve_tdvp_ps(mpo, evolve_dt)
-        elif method == EvolveMethod.tdvp_ps2:
-            new = self._evolve_tdvp_ps2(mpo, evolve_dt)
-        else:
-            raise NotImplementedError(f"{method} is outside the sweep engine (TDVP-PS / TDVP-PS2 only)")
+        new = self._drive(self._evolve_steps(mpo, evolve_dt))
         if normalize:
             new.normalize("mps_and_coeff" if np.iscomplex(evolve_dt) else "mps_only")
         return new
 
+    def _evolve_steps(self, mpo: Mpo, evolve_dt):
+        method = self.evolve_config.method
+        if method == EvolveMethod.tdvp_ps:
+            return self._evolve_tdvp_ps_steps(mpo, evolve_dt)
+        if method == EvolveMethod.tdvp_ps2:
+            return self._evolve_tdvp_ps2_steps(mpo, evolve_dt)
+        raise NotImplementedError(f"{method} is outside the sweep engine (TDVP-PS / TDVP-PS2 only)")
+
+    def _drive(self, steps):
+        """Run a sweep generator, serving each local exponential it yields
+        (operator, dt, vector) with expm_krylov; returns the new MPS."""
+        try:
+            req = next(steps)
+            while True:
+                req = steps.send(self._krylov(*req))
+        except StopIteration as stop:
+            return stop.value
+
     def _krylov(self, op: HeffOperator, dt, vec: torch.Tensor):
-        fixed = self.evolve_config.fixed_krylov
         return expm_krylov(lambda y: op.apply(y), dt, vec.reshape(-1))
 
     def _evolve_tdvp_ps(self, mpo: Mpo, evolve_dt) -> "Mps":
-        """mps.py:1267-1404 (Krylov propagator)"""
+        return self._drive(self._evolve_tdvp_ps_steps(mpo, evolve_dt))
+
+    def _evolve_tdvp_ps2(self, mpo: Mpo, evolve_dt) -> "Mps":
+        return self._drive(self._evolve_tdvp_ps2_steps(mpo, evolve_dt))
+
+    def _evolve_tdvp_ps_steps(self, mpo: Mpo, evolve_dt):
+        """mps.py:1267-1404 (Krylov propagator), as a generator that yields each
+        local exponential (operator, dt, vector) and receives (vector, count)"""
         if self.evolve_config.ivp_solver != "krylov":
             raise NotImplementedError("only the Krylov propagator is part of the sweep engine")
         mps = self.copy() if np.iscomplex(evolve_dt) else self.to_complex()
@@ -833,7 +851,7 @@ class Mps:
                 r_array = environ.read("R", imps + 1)
                 shape = list(mps[imps].shape)
                 hop = HeffOperator(l_array, r_array, [mpo[imps]], shape)
-                mps_t, j = self._krylov(hop, -1j * evolve_dt / 2, mps[imps])
+                mps_t, j = yield (hop, -1j * evolve_dt / 2, mps[imps])
                 local_steps.append(j)
                 mps_t = mps_t.reshape(shape)
                 qnbigl, qnbigr, _ = mps._get_big_qn([imps], with_mat=False)
@@ -844,7 +862,7 @@ class Mps:
                     mps.qnidx = imps - 1
                     r_array = environ.GetLR("R", imps, mps, mpo, itensor=r_array, method="System")
                     hop_u = HeffOperator(l_array, r_array, [], u.shape)
-                    mps_u, j = self._krylov(hop_u, 1j * evolve_dt / 2, u)
+                    mps_u, j = yield (hop_u, 1j * evolve_dt / 2, u)
                     local_steps.append(j)
                     mps._absorb_left(imps, mps_u.reshape(u.shape))
                 elif mps.to_right and imps != len(mps) - 1:
@@ -853,7 +871,7 @@ class Mps:
                     mps.qnidx = imps + 1
                     l_array = environ.GetLR("L", imps, mps, mpo, itensor=l_array, method="System")
                     hop_v = HeffOperator(l_array, r_array, [], vt.shape)
-                    mps_v, j = self._krylov(hop_v, 1j * evolve_dt / 2, vt)
+                    mps_v, j = yield (hop_v, 1j * evolve_dt / 2, vt)
                     local_steps.append(j)
                     mps._absorb_right(imps, mps_v.reshape(vt.shape))
                 else:
@@ -862,8 +880,9 @@ class Mps:
         mps.evolve_config.stat = _krylov_stats(local_steps)
         return mps
 
-    def _evolve_tdvp_ps2(self, mpo: Mpo, evolve_dt) -> "Mps":
-        """mps.py:1406-1517 (Krylov propagator)"""
+    def _evolve_tdvp_ps2_steps(self, mpo: Mpo, evolve_dt):
+        """mps.py:1406-1517 (Krylov propagator), as a generator like
+        _evolve_tdvp_ps_steps"""
         if self.evolve_config.ivp_solver != "krylov":
             raise NotImplementedError("only the Krylov propagator is part of the sweep engine")
         mps = self.copy() if np.iscomplex(evolve_dt) else self.to_complex()
@@ -886,7 +905,7 @@ class Mps:
                 ms2 = eng.matmul(a.reshape(-1, a.shape[-1]), b.reshape(b.shape[0], -1))
                 shape2 = [a.shape[0], a.shape[1], b.shape[1], b.shape[2]]
                 hop = HeffOperator(l_array, r_array, [mpo[cidx0], mpo[cidx1]], shape2)
-                mps_t, j = self._krylov(hop, -1j * evolve_dt / 2, ms2)
+                mps_t, j = yield (hop, -1j * evolve_dt / 2, ms2)
                 local_steps.append(j)
                 mps_t = mps_t.reshape(shape2)
                 qnbigl, qnbigr, _ = mps._get_big_qn([cidx0, cidx1], with_mat=False)
@@ -899,7 +918,7 @@ class Mps:
                     r_array = environ.GetLR("R", ridx - 1, mps, mpo, itensor=r_array, method="System")
                 ms1 = mps[cidx2]
                 hop1 = HeffOperator(l_array, r_array, [mpo[cidx2]], list(ms1.shape))
-                mps_t, j = self._krylov(hop1, 1j * evolve_dt / 2, ms1)
+                mps_t, j = yield (hop1, 1j * evolve_dt / 2, ms1)
                 local_steps.append(j)
                 mps[cidx2] = mps_t.reshape(ms1.shape)
                 mps._push_cano(cidx2)
@@ -909,3 +928,44 @@ class Mps:
 
     def __str__(self):
         return f"mps bond dim:{self.bond_dims}"
+
+
+def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True) -> List[Mps]:
+    """Mps.evolve for many independent MPS at once (static-disorder
+    realisations, each with its own MPO and bond dimensions; the reference
+    evolves them one by one through mps.py:644-662).  Every instance runs its
+    own sweep; the local exponentials that are pending at the same time run
+    in lockstep (expm_krylov_batch) and their matvecs as grouped launches
+    (hop_expr.apply_grouped: one launch per contraction stage for all FP64
+    problems).  Each result equals that instance's own evolve."""
+    from .hop_expr import apply_grouped
+    from .krylov import expm_krylov_batch
+    if isinstance(mpo_list, Mpo):
+        mpo_list = [mpo_list] * len(mps_list)
+    assert len(mpo_list) == len(mps_list)
+    gens = [m._evolve_steps(o, evolve_dt) for m, o in zip(mps_list, mpo_list)]
+    out: List[Mps] = [None] * len(gens)
+    pending = {}
+    for i, g in enumerate(gens):
+        try:
+            pending[i] = next(g)
+        except StopIteration as stop:
+            out[i] = stop.value
+    while pending:
+        idx = sorted(pending)
+        reqs = [pending[i] for i in idx]
+        ops = [r[0] for r in reqs]
+        res = expm_krylov_batch(lambda sub, xs: apply_grouped([ops[k] for k in sub], xs), [r[1] for r in reqs],
+                                [r[2].reshape(-1) for r in reqs])
+        nxt = {}
+        for i, r in zip(idx, res):
+            try:
+                nxt[i] = gens[i].send(r)
+            except StopIteration as stop:
+                out[i] = stop.value
+        pending = nxt
+    if normalize:
+        for m in out:
+            m.normalize("mps_and_coeff" if np.iscomplex(evolve_dt) else "mps_only")
+    return out
+

@@ -23,7 +23,7 @@ class FakeEngine:
 
     def __getattribute__(self, name):
         attr = object.__getattribute__(self, name)
-        if name in ("heff_apply", "heff_backward", "heff_diag", "env_update", "vec_norm", "vec_dotc", "krylov_alpha", "krylov_orth",
+        if name in ("heff_apply", "heff_apply_grouped", "heff_backward", "heff_diag", "env_update", "vec_norm", "vec_dotc", "krylov_alpha", "krylov_orth",
                     "scale_inv", "lincomb", "allclose", "axpy", "precond", "qn_gather"):
             def checked(*a, **k):
                 _chk(*a)
@@ -44,6 +44,10 @@ class FakeEngine:
             r = torch.einsum("abc,bdef,fghj,ljk,cehk->adgl", L.to(y.dtype), W1.to(y.dtype), W2.to(y.dtype),
                              R.to(y.dtype), psi.to(y.dtype))
         y.copy_(r)
+
+    def heff_apply_grouped(self, descs, Ls, W1s, W2s, Rs, psis, ys):
+        for d, L, W1, W2, R, psi, y in zip(descs, Ls, W1s, W2s, Rs, psis, ys):
+            self.heff_apply(d, L, W1, W2, R, psi, y)
 
     def heff_backward(self, d, L, W1, W2, R, psi, gy, gpsi, gL, gW1, gW2, gR):
         spec = {0: "abc,lbk,ck->al", 1: "abc,bdef,lfk,cek->adl", 2: "abc,bdef,fghj,ljk,cehk->adgl"}[d.nsite]
