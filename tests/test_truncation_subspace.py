@@ -158,3 +158,34 @@ def test_capped_projection_nearly_product_cpu(cpu_engine, keep_left, shape):
     eye = torch.eye(kcap, dtype=kept.dtype)
     assert float((kept.mH @ kept - eye).abs().max()) < 1e-12
     assert float((capped.left @ capped.right - coef).abs().max()) < 1e-9
+
+
+def test_device_eigensolver_fallback_host_logic(cpu_engine, monkeypatch):
+    """svd_truncate's handling of the device eigensolver's acceptance triple:
+    a stand-in returns only the leading kt eigenpairs with a check that passes
+    for one block and fails for the other; the failing block must be redone by
+    the full decomposition and the result must equal the all-full path"""
+    svd_qn = importlib.import_module("renormalizer_b200.svd_qn")
+    heev = importlib.import_module("renormalizer_b200.heev")
+    coef, ql, qr = _case("cpu", 160, 12.0)
+    kcap = 24
+    full = svd_qn.svd_truncate(coef, ql, qr, np.array([1]), True, lambda s: min(kcap, len(s)), kcap=kcap)
+    calls = []
+
+    def fake_gram_eigh(eng, G, kt, use_heev):
+        w, V = torch.linalg.eigh(G)
+        w, V = torch.flip(w, dims=[0]), torch.flip(V, dims=[1])
+        if not use_heev:
+            return w, V, None
+        calls.append(kt)
+        bad = 1.0 if len(calls) == 1 else 0.0
+        return w[:kt], V[:, :kt], torch.tensor([0.0, bad, 0.0], dtype=torch.float64)
+
+    monkeypatch.setattr(svd_qn, "_gram_eigh", fake_gram_eigh)
+    f0 = heev.heev_opts.fallbacks
+    got = svd_qn.svd_truncate(coef, ql, qr, np.array([1]), True, lambda s: min(kcap, len(s)), kcap=kcap)
+    assert len(calls) == 2 and heev.heev_opts.fallbacks == f0 + 1
+    assert got.mdim == full.mdim == kcap
+    np.testing.assert_array_equal(np.asarray(got.qn), np.asarray(full.qn))
+    np.testing.assert_allclose(got.sigma, full.sigma, rtol=1e-12)
+    assert torch.allclose(got.left @ got.right, full.left @ full.right, atol=1e-12)
