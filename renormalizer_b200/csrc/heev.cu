@@ -32,6 +32,9 @@
 #include <cstddef>
 #include "reno_common.cuh"
 #include "gemm_fp64.cuh"
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 namespace reno {
 namespace heev {
@@ -301,6 +304,150 @@ __global__ void __launch_bounds__(HT, 1)
       __stcg(&A[(size_t)(n - 2) * n + (n - 1)], vp[n - 1]);
     }
   }
+}
+
+// ---------------------------------------------------------------- small matrices
+// n <= 256: the same lagged one-barrier-per-column reduction on one
+// thread-block cluster of CL CTAs whose shared memories hold the matrix
+// (row r in CTA r % CL, slot r / CL).  Row k is read from its owner through
+// distributed shared memory, y_r and the partial dots are pushed to every CTA
+// (double-buffered by column parity, so a CTA that runs ahead never
+// overwrites a buffer another is still reading), and the hardware cluster
+// barrier, which every CTA executes the same number of times, separates the
+// columns.  Reflector k is written to row k of Aout (which may alias Gin: all
+// of Gin is read before the first barrier).  blockIdx.y = matrix.
+constexpr int CL = 8, CT = 256, CW = CT / 32, NMAX_C = 256, RL = NMAX_C / CL;
+
+inline size_t cluster_smem_bytes(int n) {
+  return ((size_t)RL * n + 5 * (size_t)n + 2 * CL) * sizeof(double2);
+}
+
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(CT, 1)
+    hetrd_cluster_kernel(const double2* __restrict__ Gin, double2* Aout, int n, double* __restrict__ d,
+                         double* __restrict__ e, double2* __restrict__ tau) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const size_t mat = blockIdx.y;
+  Gin += mat * n * n;
+  Aout += mat * n * n;
+  d += mat * n;
+  e += mat * n;
+  tau += mat * n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* rows = reinterpret_cast<double2*>(smem_raw);  // RL x n
+  double2* vp = rows + (size_t)RL * n;
+  double2* wp = vp + n;
+  double2* vc = wp + n;
+  double2* yb = vc + n;      // 2 x n
+  double2* pb = yb + 2 * n;  // 2 x CL
+  __shared__ double red[CW];
+  __shared__ double2 redc[CW];
+  __shared__ double2 s_scale, s_tau;
+  __shared__ double s_akk;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int sl = 0; sl < RL; ++sl) {
+    const int r = sl * CL + rank;
+    if (r < n)
+      for (int c = tid; c < n; c += CT) rows[(size_t)sl * n + c] = Gin[(size_t)r * n + c];
+  }
+  for (int i = tid; i < n; i += CT) {
+    vp[i] = make_double2(0.0, 0.0);
+    wp[i] = make_double2(0.0, 0.0);
+    vc[i] = make_double2(0.0, 0.0);
+  }
+  cluster.sync();
+  for (int k = 0; k < n - 1; ++k) {
+    const int par = k & 1;
+    // ---- phase 1: row k from its owner, update k-1 applied, reflector k
+    const double2* rk = cluster.map_shared_rank(rows + (size_t)(k / CL) * n, k % CL);
+    const double2 vpk = vp[k], wpk = wp[k];
+    double ss = 0.0;
+    for (int c = k + tid; c < n; c += CT) {
+      const double2 x = csub(csub(rk[c], cmulc(vpk, wp[c])), cmulc(wpk, vp[c]));
+      if (c == k) {
+        s_akk = x.x;
+      } else {
+        const double2 xc = conjg(x);
+        vc[c] = xc;
+        if (c >= k + 2) ss += xc.x * xc.x + xc.y * xc.y;
+      }
+    }
+    ss = block_sum<CW>(ss, red);
+    if (tid == 0) {
+      const double2 alpha = vc[k + 1];
+      double beta;
+      if (ss == 0.0 && alpha.y == 0.0) {
+        s_tau = make_double2(0.0, 0.0);
+        s_scale = make_double2(0.0, 0.0);
+        beta = alpha.x;
+      } else {
+        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+        s_tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+        const double2 den = make_double2(alpha.x - beta, alpha.y);
+        const double m2 = den.x * den.x + den.y * den.y;
+        s_scale = make_double2(den.x / m2, -den.y / m2);
+      }
+      if (rank == 0) {
+        d[k] = s_akk;
+        e[k] = beta;
+        tau[k] = s_tau;
+      }
+    }
+    __syncthreads();
+    const double2 sc = s_scale, tk = s_tau;
+    for (int c = k + 1 + tid; c < n; c += CT) {
+      const double2 v = (c == k + 1) ? make_double2(1.0, 0.0) : cmul(vc[c], sc);
+      vc[c] = v;
+      if (rank == 0) Aout[(size_t)k * n + c] = v;
+    }
+    __syncthreads();
+    // ---- phase 2: owned rows r >= k+1: update k-1, y_r = row . v_k, pushed to every CTA
+    double2 pdot = make_double2(0.0, 0.0);
+    for (int sl = warp; sl < RL; sl += CW) {
+      const int r = sl * CL + rank;
+      if (r <= k || r >= n) continue;
+      double2* row = rows + (size_t)sl * n;
+      const double2 vpr = vp[r], wpr = wp[r];
+      double2 acc = make_double2(0.0, 0.0);
+      for (int c = k + 1 + lane; c < n; c += 32) {
+        const double2 x = csub(csub(row[c], cmulc(vpr, wp[c])), cmulc(wpr, vp[c]));
+        row[c] = x;
+        acc = cadd(acc, cmul(x, vc[c]));
+      }
+      acc = warp_sum(acc);
+      if (lane < CL) cluster.map_shared_rank(yb + (size_t)par * n, lane)[r] = acc;
+      if (lane == 0) pdot = cadd(pdot, cmulc(vc[r], acc));
+    }
+    if (lane == 0) redc[warp] = pdot;
+    __syncthreads();
+    if (tid < CL) {
+      double2 sum = make_double2(0.0, 0.0);
+      for (int w = 0; w < CW; ++w) sum = cadd(sum, redc[w]);
+      cluster.map_shared_rank(pb + par * CL, tid)[rank] = sum;
+    }
+    cluster.sync();
+    // ---- phase 3: w_k = tau y - (|tau|^2 / 2)(y^H v) v
+    double2 dot = make_double2(0.0, 0.0);
+    for (int q = 0; q < CL; ++q) dot = cadd(dot, pb[par * CL + q]);
+    const double t2 = tk.x * tk.x + tk.y * tk.y;
+    const double2 alph = make_double2(-0.5 * t2 * dot.x, -0.5 * t2 * dot.y);
+    for (int c = k + 1 + tid; c < n; c += CT) {
+      const double2 v = vc[c];
+      wp[c] = cadd(cmul(tk, yb[(size_t)par * n + c]), cmul(alph, v));
+      vp[c] = v;
+    }
+    __syncthreads();
+  }
+  if (rank == 0 && tid == 0) {
+    if (n == 1) {
+      d[0] = rows[0].x;
+    } else {
+      const double2* rn = cluster.map_shared_rank(rows + (size_t)((n - 1) / CL) * n, (n - 1) % CL);
+      const double2 a = csub(csub(rn[n - 1], cmulc(vp[n - 1], wp[n - 1])), cmulc(wp[n - 1], vp[n - 1]));
+      d[n - 1] = a.x;
+    }
+  }
+  cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
 
 // ---------------------------------------------------------------- eigenvalues
@@ -664,6 +811,22 @@ extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, doub
     if (rc != RENO_OK) return rc;
     attr_set = true;
   }
+  if (n <= NMAX_C) {
+    // 1. tridiagonal reduction of a small matrix: one thread-block cluster
+    static bool cl_attr = false;
+    if (!cl_attr) {
+      rc = check_cuda(ctx, cudaFuncSetAttribute(hetrd_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)cluster_smem_bytes(NMAX_C)),
+                      "reno_heev_top: cluster smem attribute");
+      if (rc != RENO_OK) return rc;
+      cl_attr = true;
+    }
+    count_launch();
+    hetrd_cluster_kernel<<<dim3(CL, 1), CT, cluster_smem_bytes(n), st>>>(static_cast<const double2*>(A),
+                                                                         static_cast<double2*>(A), n, d, e,
+                                                                         static_cast<double2*>(tau));
+    RENO_LAUNCH_CHECK(ctx, "reno_heev_top: cluster hetrd");
+  } else {
   // 1. tridiagonal reduction: one CTA per SM, all co-resident (cooperative launch)
   const size_t smem = 3 * (size_t)n * sizeof(double2);
   int per_sm = 0;
@@ -680,6 +843,7 @@ extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, doub
   rc = check_cuda(ctx, cudaLaunchCooperativeKernel((void*)hetrd_kernel, dim3(grid), dim3(HT), args, smem, st),
                   "reno_heev_top: hetrd launch");
   if (rc != RENO_OK) return rc;
+  }
   // 2. eigenvalues n-kt .. n-1 (ascending)
   count_launch();
   bounds_kernel<<<1, THREADS, 0, st>>>(d, e, n, bnd);

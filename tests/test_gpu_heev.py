@@ -35,7 +35,7 @@ def _gram(n, cplx, kind, seed):
 @pytest.mark.gpu
 @pytest.mark.parametrize("cplx", [True, False])
 @pytest.mark.parametrize("kind", ["generic", "nearly_product"])
-@pytest.mark.parametrize("n,kt", [(96, 40), (700, 128), (2048, 320)])
+@pytest.mark.parametrize("n,kt", [(96, 40), (256, 128), (700, 128), (2048, 320)])
 def test_heev_top_matches_eigh(n, kt, kind, cplx):
     from renormalizer_b200._native import Engine
     from renormalizer_b200.heev import accepted, heev_opts, heev_top
