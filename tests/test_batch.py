@@ -82,3 +82,31 @@ def test_grouped_matvec_matches_single():
         ys = apply_grouped(ops, psis)
         for op, psi, y in zip(ops, psis, ys):
             assert torch.equal(y, op.apply(psi)), nsite
+
+
+def test_expm_krylov_batch_matches_single(cpu_engine):
+    """lockstep Lanczos exponentials of independent problems (different sizes,
+    step sizes and stopping points) equal their own expm_krylov results
+    exactly, and the grouped operator sees only the still-running problems"""
+    from renormalizer_b200.krylov import expm_krylov, expm_krylov_batch
+    rng = np.random.default_rng(8)
+    mats, vecs, dts = [], [], []
+    for n, dt in ((6, -0.3j), (40, -0.05j), (25, 0.2), (3, -1j)):
+        h = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        mats.append(torch.as_tensor(h + h.conj().T))
+        vecs.append(torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n)))
+        dts.append(dt)
+    single = [expm_krylov(lambda x, m=m: m @ x, dt, v) for m, dt, v in zip(mats, dts, vecs)]
+    seen = []
+
+    def group_apply(idx, xs):
+        seen.append(list(idx))
+        return [mats[i] @ x for i, x in zip(idx, xs)]
+
+    batch = expm_krylov_batch(group_apply, dts, vecs)
+    for (vs, js), (vb, jb) in zip(single, batch):
+        assert js == jb
+        assert torch.equal(vs, vb)
+    assert seen[0] == [0, 1, 2, 3]
+    assert all(len(a) >= len(b) for a, b in zip(seen, seen[1:]))
+    assert sum(len(s) for s in seen) == sum(j for _, j in single)
