@@ -686,25 +686,31 @@ __global__ void __launch_bounds__(IV_THREADS) inviter_kernel(const double* __res
 // H_k0 ... H_k0+kb-1 = I - V T V^H, LAPACK's forward columnwise larft), the
 // blocks applied from the last to the first, each as three FP64 GEMMs.
 constexpr int NB = 64;
+constexpr int KCH = 256;  // row chunk of the split-K products V_b^H K
 
-// rows 0..n-2 of A become the reflectors: 0 before column k+1, 1 at k+1
+inline int nch_max(int n) { return (int)ceil_div(std::max(n - 1, 1), KCH); }
+
+// rows 0..n-2 of A become the reflectors (0 before column k+1, 1 at k+1) and
+// row n-1 becomes 0, so that every reflector row can be read over all n columns
 __global__ void clean_v_kernel(double2* __restrict__ A, int n) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (size_t)(n - 1) * n) return;
+  if (idx >= (size_t)n * n) return;
   const int k = (int)(idx / n), c = (int)(idx % n);
-  if (c <= k) A[idx] = make_double2(0.0, 0.0);
+  if (k == n - 1 || c <= k) A[idx] = make_double2(0.0, 0.0);
   else if (c == k + 1) A[idx] = make_double2(1.0, 0.0);
 }
 
-// minus the NB x NB upper-triangular T of block b from S = V^H V and tau.
-// Thread i owns row i of T (written and read only by itself, in Tg).
+// minus the NB x NB upper-triangular T of block b from S = V^H V and tau,
+// written rep times side by side (row i of block b at
+// Tg + (b NB + i) NB rep): the split-K partials of V^H K then sum inside the
+// T product.  Thread i owns row i (written and read only by itself).
 __global__ void __launch_bounds__(NB) larft_kernel(const double2* __restrict__ Sg, const double2* __restrict__ tau,
-                                                   double2* __restrict__ Tg, int n) {
+                                                   double2* __restrict__ Tg, int n, int rep) {
   __shared__ double2 x[NB];
   const int b = blockIdx.x, i = threadIdx.x;
   const int k0 = b * NB, kb = min(NB, n - 1 - k0);
   const double2* S = Sg + (size_t)b * NB * NB;
-  double2* T = Tg + (size_t)b * NB * NB + (size_t)i * NB;
+  double2* T = Tg + ((size_t)b * NB + i) * NB * rep;
   for (int c = 0; c < NB; ++c) T[c] = make_double2(0.0, 0.0);
   for (int j = 0; j < kb; ++j) {
     const double2 tj = tau[k0 + j];
@@ -719,7 +725,10 @@ __global__ void __launch_bounds__(NB) larft_kernel(const double2* __restrict__ S
     }
     __syncthreads();
   }
-  for (int c = 0; c < NB; ++c) T[c] = make_double2(-T[c].x, -T[c].y);
+  for (int c = 0; c < NB; ++c) {
+    const double2 v = make_double2(-T[c].x, -T[c].y);
+    for (int r = 0; r < rep; ++r) T[(size_t)r * NB + c] = v;
+  }
 }
 
 }  // namespace heev
@@ -751,9 +760,9 @@ HeevLayout heev_layout(int n, int kt) {
   L.s = off;
   off += align256(nblk * NB * NB * sizeof(double2));
   L.t = off;
-  off += align256(nblk * NB * NB * sizeof(double2));
+  off += align256(nblk * NB * NB * nch_max(n) * sizeof(double2));
   L.w1 = off;
-  off += align256((size_t)NB * kt * sizeof(double2));
+  off += align256((size_t)nch_max(n) * NB * kt * sizeof(double2));
   L.w2 = off;
   off += align256((size_t)NB * kt * sizeof(double2));
   L.total = off;
@@ -879,51 +888,103 @@ extern "C" int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, voi
   double2* Kc = static_cast<double2*>(K);
   cudaStream_t st = ctx->stream;
   const int nblk = (int)ceil_div(n - 1, NB);
-  const size_t nel = (size_t)(n - 1) * n;
+  const int rep = nch_max(n);
+  const size_t nel = (size_t)n * n;
   count_launch();
   clean_v_kernel<<<(unsigned)ceil_div((int64_t)nel, 256), 256, 0, st>>>(V, n);
   RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: clean");
   int rc = check_cuda(ctx, cudaMemsetAsync(Sg, 0, (size_t)nblk * NB * NB * sizeof(double2), st),
                       "reno_heev_backtransform: memset");
   if (rc != RENO_OK) return rc;
-  // S_b = V_b^H V_b over the columns the block's reflectors touch
-  for (int b = 0; b < nblk; ++b) {
-    const int k0 = b * NB, kb = std::min(NB, n - 1 - k0);
+  // S_b = V_b^H V_b: the blocks of NB reflectors in one batched GEMM over all
+  // n columns (zeros before each row's reflector), a partial last block apart
+  const int nfull = (n - 1) / NB;
+  if (nfull > 0) {
     GemmParams p;
-    p.M = kb;
-    p.N = kb;
-    p.K = n - k0 - 1;
-    p.A = op(V + (size_t)k0 * n + k0 + 1, n, 1, 1);
-    p.B = op(V + (size_t)k0 * n + k0 + 1, n, 1, 0);
-    p.C = Sg + (size_t)b * NB * NB;
+    p.M = NB;
+    p.N = NB;
+    p.K = n;
+    p.batch = nfull;
+    p.A = op(V, n, 1, 1);
+    p.A.s_batch = (int64_t)NB * n;
+    p.B = op(V, n, 1, 0);
+    p.B.s_batch = (int64_t)NB * n;
+    p.C = Sg;
     p.sCm = NB;
     p.sCn = 1;
+    p.sCb = (int64_t)NB * NB;
     count_launch();
     rc = check_cuda(ctx, gemm_fp64(p, st), "reno_heev_backtransform: gram");
     if (rc != RENO_OK) return rc;
   }
+  if (nfull < nblk) {
+    const int k0 = nfull * NB, kb = n - 1 - k0;
+    GemmParams p;
+    p.M = kb;
+    p.N = kb;
+    p.K = n;
+    p.A = op(V + (size_t)k0 * n, n, 1, 1);
+    p.B = op(V + (size_t)k0 * n, n, 1, 0);
+    p.C = Sg + (size_t)nfull * NB * NB;
+    p.sCm = NB;
+    p.sCn = 1;
+    count_launch();
+    rc = check_cuda(ctx, gemm_fp64(p, st), "reno_heev_backtransform: gram (last block)");
+    if (rc != RENO_OK) return rc;
+  }
   count_launch();
-  larft_kernel<<<nblk, NB, 0, st>>>(Sg, static_cast<const double2*>(tau), Tg, n);
+  larft_kernel<<<nblk, NB, 0, st>>>(Sg, static_cast<const double2*>(tau), Tg, n, rep);
   RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: larft");
   for (int b = nblk - 1; b >= 0; --b) {
     const int k0 = b * NB, kb = std::min(NB, n - 1 - k0);
     const int rows = n - k0 - 1;
-    // W1 = V_b^H K[k0+1:]
-    GemmParams p1;
-    p1.M = kb;
-    p1.N = kt;
-    p1.K = rows;
-    p1.A = op(V + (size_t)k0 * n + k0 + 1, n, 1, 1);
-    p1.B = op(Kc + (size_t)(k0 + 1) * kt, 1, kt, 0);
-    p1.C = W1;
-    p1.sCm = kt;
-    p1.sCn = 1;
-    // W2 = (-T_b) W1
+    const int nfc = rows / KCH, rem = rows % KCH, nch = nfc + (rem > 0);
+    const double2* Vb = V + (size_t)k0 * n + k0 + 1;
+    double2* Kb = Kc + (size_t)(k0 + 1) * kt;
+    if (kb < NB) {
+      rc = check_cuda(ctx, cudaMemsetAsync(W1, 0, (size_t)nch * NB * kt * sizeof(double2), st),
+                      "reno_heev_backtransform: memset W1");
+      if (rc != RENO_OK) return rc;
+    }
+    // W1[s] = V_b^H K over row chunk s (split K: one batch entry per full chunk)
+    if (nfc > 0) {
+      GemmParams p1;
+      p1.M = kb;
+      p1.N = kt;
+      p1.K = KCH;
+      p1.batch = nfc;
+      p1.A = op(Vb, n, 1, 1);
+      p1.A.s_batch = KCH;
+      p1.B = op(Kb, 1, kt, 0);
+      p1.B.s_batch = (int64_t)KCH * kt;
+      p1.C = W1;
+      p1.sCm = kt;
+      p1.sCn = 1;
+      p1.sCb = (int64_t)NB * kt;
+      count_launch();
+      rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K");
+      if (rc != RENO_OK) return rc;
+    }
+    if (rem > 0) {
+      GemmParams p1;
+      p1.M = kb;
+      p1.N = kt;
+      p1.K = rem;
+      p1.A = op(Vb + (size_t)nfc * KCH, n, 1, 1);
+      p1.B = op(Kb + (size_t)nfc * KCH * kt, 1, kt, 0);
+      p1.C = W1 + (size_t)nfc * NB * kt;
+      p1.sCm = kt;
+      p1.sCn = 1;
+      count_launch();
+      rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K (last chunk)");
+      if (rc != RENO_OK) return rc;
+    }
+    // W2 = (-T_b) sum_s W1[s]: -T_b replicated along K
     GemmParams p2;
     p2.M = kb;
     p2.N = kt;
-    p2.K = kb;
-    p2.A = op(Tg + (size_t)b * NB * NB, NB, 1, 0);
+    p2.K = NB * nch;
+    p2.A = op(Tg + (size_t)b * NB * NB * rep, (int64_t)NB * rep, 1, 0);
     p2.B = op(W1, 1, kt, 0);
     p2.C = W2;
     p2.sCm = kt;
@@ -933,15 +994,14 @@ extern "C" int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, voi
     p3.M = rows;
     p3.N = kt;
     p3.K = kb;
-    p3.A = op(V + (size_t)k0 * n + k0 + 1, 1, n, 0);
+    p3.A = op(Vb, 1, n, 0);
     p3.B = op(W2, 1, kt, 0);
-    p3.C = Kc + (size_t)(k0 + 1) * kt;
+    p3.C = Kb;
     p3.sCm = kt;
     p3.sCn = 1;
     p3.accumulate = 1;
-    count_launch(3);
-    rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K");
-    if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64(p2, st), "reno_heev_backtransform: T W");
+    count_launch(2);
+    rc = check_cuda(ctx, gemm_fp64(p2, st), "reno_heev_backtransform: T W");
     if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64(p3, st), "reno_heev_backtransform: K += V W");
     if (rc != RENO_OK) return rc;
   }
