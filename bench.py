@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--grad", action="store_true",
                     help="gradient of the site-0 population after a TDVP-PS trajectory with respect to per-molecule "
                          "couplings (16-molecule Holstein, 10 levels, M=64, 50 steps of dt=0.05)")
+    ap.add_argument("--heev", type=int, default=0, metavar="N",
+                    help="time the device Hermitian eigensolver (leading 320 eigenpairs, or N/2 below 640) against "
+                         "cuSOLVER eigh on a seeded N x N complex Gram matrix")
     ap.add_argument("--batch", type=int, default=0, metavar="B",
                     help="TDVP-PS2 of B static-disorder realisations (per-molecule couplings g ~ U(0.5, 1.5), "
                          "--batch-nmol molecules with one 10-level mode, M = --batch-M) advanced in lockstep with "
@@ -615,6 +618,38 @@ def run_dmrg(args):
                       "e_min_abs_diff": abs(min(a["energies"]) - min(b["energies"])), "runs": out}), flush=True)
 
 
+def run_heev(args):
+    """heev.heev_top against torch.linalg.eigh (cuSOLVER) on G = X X^H / N,
+    X seeded complex Gaussian; three timed calls each after one warm-up."""
+    import torch
+    from renormalizer_b200._native import Engine
+    from renormalizer_b200.heev import accepted, heev_top
+    torch.cuda.set_device(0)
+    eng = Engine.get(0)
+    n = args.heev
+    kt = 320 if n >= 640 else max(1, n // 2)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    X = torch.complex(torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g),
+                      torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g))
+    G = X @ X.mH / n
+
+    def timed(f, reps=3):
+        f()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            out = f()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps * 1e3, out
+
+    t_ref, (w_ref, _) = timed(lambda: torch.linalg.eigh(G))
+    t_dev, (w, K, chk) = timed(lambda: heev_top(eng, G, kt))
+    top = torch.flip(w_ref, dims=[0])[:kt]
+    print(json.dumps({"metric": f"Hermitian eigensolver, leading {kt} of {n}x{n} complex128", "unit": "ms",
+                      "value": t_dev, "cusolver_eigh_ms": t_ref, "accepted": bool(accepted(chk.cpu().numpy())),
+                      "max_eigenvalue_diff_rel": float((w - top).abs().max() / top.abs().max())}), flush=True)
+
+
 def run_batch(args):
     """evolve_batch (lockstep sweeps, grouped FP64 matvecs) vs per-realisation
     Mps.evolve on the same static-disorder realisations, one warm-up step
@@ -728,6 +763,9 @@ def main():
         return
     if args.batch:
         run_batch(args)
+        return
+    if args.heev:
+        run_heev(args)
         return
     import importlib
     importlib.import_module("renormalizer_b200.svd_qn").subspace.min_dim = 1024 if args.truncation == "subspace" else 0
