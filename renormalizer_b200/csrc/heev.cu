@@ -149,7 +149,6 @@ __global__ void __launch_bounds__(HT, 1)
   double2* vc = wp + n;                                // v of step k
   __shared__ double red[HW];
   __shared__ double2 redc[HW];
-  __shared__ double2 s_scale, s_tau, s_dot;
   __shared__ double s_akk;
   __shared__ int s_ok;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -161,9 +160,21 @@ __global__ void __launch_bounds__(HT, 1)
     vc[i] = make_double2(0.0, 0.0);
   }
   __syncthreads();
+  // Shared-memory discipline: in phases 1 and 3 thread t owns the entries
+  // c = k + t + j HT of vc (phase 1 of column k) and c = k + 1 + t + j HT of
+  // vp, wp (phase 3 of column k), i.e. the same entries as phase 1 of column
+  // k + 1, so those phases need no block barrier between them; every thread
+  // recomputes the scalars that more than one thread needs (the Householder
+  // scalars, the dot y^H v and the pending pivot entries v_{k-1}[k] = 1,
+  // w_{k-1}[k]) with the same operations, so they agree bit for bit.
+  double2 tk_prev = make_double2(0.0, 0.0), alph_prev = make_double2(0.0, 0.0);
   for (int k = 0; k < n - 1; ++k) {
     // ---- phase 1 (every CTA): row k with update k-1 applied, reflector k
-    const double2 vpk = vp[k], wpk = wp[k];
+    double2 vpk = make_double2(0.0, 0.0), wpk = make_double2(0.0, 0.0);
+    if (k > 0) {
+      vpk = make_double2(1.0, 0.0);
+      wpk = cadd(cmul(tk_prev, __ldcg(&Y[(size_t)((k - 1) & 1) * n + k])), cmul(alph_prev, vpk));
+    }
     const double2* rowk = A + (size_t)k * n;
     double ss = 0.0;
     for (int base = k + tid; base < n; base += U1 * HT) {
@@ -188,33 +199,40 @@ __global__ void __launch_bounds__(HT, 1)
         }
       }
     }
-    ss = block_sum<HW>(ss, red);  // includes __syncthreads: vc[k+1], s_akk visible
-    if (tid == 0) {
-      const double2 alpha = vc[k + 1];
-      double beta;
-      if (ss == 0.0 && alpha.y == 0.0) {
-        s_tau = make_double2(0.0, 0.0);
-        s_scale = make_double2(0.0, 0.0);
-        beta = alpha.x;
-      } else {
-        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
-        s_tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-        const double2 den = make_double2(alpha.x - beta, alpha.y);
-        const double m2 = den.x * den.x + den.y * den.y;
-        s_scale = make_double2(den.x / m2, -den.y / m2);
-      }
-      if (blockIdx.x == 0) {
-        d[k] = s_akk;
-        e[k] = beta;
-        tau[k] = s_tau;
-      }
-    }
+    // block sum of ss; alpha = vc[k+1] is read by every thread between the two
+    // barriers, before its writer can rescale it below
+    ss = warp_sum(ss);
     __syncthreads();
-    const double2 sc = s_scale, tk = s_tau;
-    for (int c = k + 1 + tid; c < n; c += HT) vc[c] = (c == k + 1) ? make_double2(1.0, 0.0) : cmul(vc[c], sc);
-    // reflector k-1 into row k-1, which no CTA reads any more
-    if (blockIdx.x == 0 && k > 0)
-      for (int c = k + tid; c < n; c += HT) __stcg(&A[(size_t)(k - 1) * n + c], vp[c]);
+    if (lane == 0) red[warp] = ss;
+    const double2 alpha = vc[k + 1];
+    __syncthreads();
+    ss = 0.0;
+#pragma unroll
+    for (int w = 0; w < HW; ++w) ss += red[w];
+    double beta;
+    double2 tk, sc;
+    if (ss == 0.0 && alpha.y == 0.0) {
+      tk = make_double2(0.0, 0.0);
+      sc = make_double2(0.0, 0.0);
+      beta = alpha.x;
+    } else {
+      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+      tk = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+      const double2 den = make_double2(alpha.x - beta, alpha.y);
+      const double m2 = den.x * den.x + den.y * den.y;
+      sc = make_double2(den.x / m2, -den.y / m2);
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+      d[k] = s_akk;
+      e[k] = beta;
+      tau[k] = tk;
+    }
+    // own entries of vc: v_k; reflector k-1 (own entries of vp) into row k-1,
+    // which no CTA reads any more
+    for (int c = k + tid; c < n; c += HT) {
+      if (c > k) vc[c] = (c == k + 1) ? make_double2(1.0, 0.0) : cmul(vc[c], sc);
+      if (blockIdx.x == 0 && k > 0) __stcg(&A[(size_t)(k - 1) * n + c], vp[c]);
+    }
     __syncthreads();
 
     // ---- phase 2 (rows split over all warps of the grid): update k-1, y = A v_k
@@ -256,25 +274,22 @@ __global__ void __launch_bounds__(HT, 1)
     }
     if (!grid_sync(sync, G, gen, &s_ok)) return;
 
-    // ---- phase 3 (every CTA): w_k = tau y - (|tau|^2 / 2)(y^H v) v
-    if (warp == 0) {
-      double2 s = make_double2(0.0, 0.0);
-      for (int base = lane; base < (int)G; base += 32 * U1) {
-        double2 p[U1];
+    // ---- phase 3 (every CTA): w_k = tau y - (|tau|^2 / 2)(y^H v) v; every
+    // warp sums the CTA partials itself
+    double2 dot = make_double2(0.0, 0.0);
+    for (int base = lane; base < (int)G; base += 32 * U1) {
+      double2 p[U1];
 #pragma unroll
-        for (int u = 0; u < U1; ++u) {
-          const int b = base + 32 * u;
-          p[u] = b < (int)G ? __ldcg(&P[(size_t)(k & 1) * G + b]) : make_double2(0.0, 0.0);
-        }
-#pragma unroll
-        for (int u = 0; u < U1; ++u) s = cadd(s, p[u]);
+      for (int u = 0; u < U1; ++u) {
+        const int b = base + 32 * u;
+        p[u] = b < (int)G ? __ldcg(&P[(size_t)(k & 1) * G + b]) : make_double2(0.0, 0.0);
       }
-      s = warp_sum(s);
-      if (lane == 0) s_dot = s;
+#pragma unroll
+      for (int u = 0; u < U1; ++u) dot = cadd(dot, p[u]);
     }
-    __syncthreads();
+    dot = warp_sum(dot);
     const double t2 = tk.x * tk.x + tk.y * tk.y;
-    const double2 alph = make_double2(-0.5 * t2 * s_dot.x, -0.5 * t2 * s_dot.y);
+    const double2 alph = make_double2(-0.5 * t2 * dot.x, -0.5 * t2 * dot.y);
     for (int base = k + 1 + tid; base < n; base += U1 * HT) {
       double2 y[U1];
 #pragma unroll
@@ -292,7 +307,8 @@ __global__ void __launch_bounds__(HT, 1)
         }
       }
     }
-    __syncthreads();
+    tk_prev = tk;
+    alph_prev = alph;
   }
   if (blockIdx.x == 0 && tid == 0) {
     if (n == 1) {
