@@ -110,3 +110,41 @@ def test_expm_krylov_batch_matches_single(cpu_engine):
     assert seen[0] == [0, 1, 2, 3]
     assert all(len(a) >= len(b) for a, b in zip(seen, seen[1:]))
     assert sum(len(s) for s in seen) == sum(j for _, j in single)
+
+
+def test_apply_grouped_dispatch_host_logic(cpu_engine, monkeypatch):
+    """apply_grouped on the CPU stand-in: FP64 operators (two shapes, 0/1/2
+    sites) go to grouped calls of at most 128 problems with one nsite and
+    dtype set each, split-precision operators one by one; every result equals
+    the operator's own apply"""
+    import importlib
+    hop_expr = importlib.import_module("renormalizer_b200.hop_expr")
+    from renormalizer_b200.hop_expr import HeffOperator, apply_grouped
+    rng = np.random.default_rng(2)
+    c = lambda *s: torch.as_tensor(rng.standard_normal(s) + 1j * rng.standard_normal(s))
+    r = lambda *s: torch.as_tensor(rng.standard_normal(s))
+    ops, psis = [], []
+    for i in range(133):
+        nsite = i % 3
+        ml, mr, w, d1, d2 = (3, 4, 2, 2, 2) if i % 2 else (5, 2, 3, 3, 2)
+        W = [] if nsite == 0 else ([r(w, d1, d1, w)] if nsite == 1 else [r(w, d1, d1, w), r(w, d2, d2, w)])
+        shape = {0: (ml, mr), 1: (ml, d1, mr), 2: (ml, d1, d2, mr)}[nsite]
+        prec = "bf16x3" if i % 7 == 0 else "fp64"
+        ops.append(HeffOperator(c(ml, w, ml), c(mr, w, mr), W, shape, prec=prec))
+        psis.append(c(*shape))
+    calls = []
+    fake = cpu_engine
+    orig = type(fake).heff_apply_grouped
+
+    def spy(self, descs, *rest):
+        calls.append([(d.nsite, d.prec) for d in descs])
+        return orig(self, descs, *rest)
+
+    monkeypatch.setattr(type(fake), "heff_apply_grouped", spy)
+    monkeypatch.setattr(hop_expr, "MAX_GROUP", 20)
+    ys = apply_grouped(ops, psis)
+    for op, psi, y in zip(ops, psis, ys):
+        assert torch.equal(y, op.apply(psi))
+    assert all(len(cl) <= 20 for cl in calls)
+    assert all(len({ns for ns, _ in cl}) == 1 and all(p == 0 for _, p in cl) for cl in calls)
+    assert sum(len(cl) for cl in calls) == sum(1 for op in ops if op.prec == "fp64")
