@@ -178,31 +178,41 @@ def _scatter(eng: Engine, src: torch.Tensor, rows, scols, dcols, sigma, dst: tor
     eng.qn_scatter(src, _i64(rows, dev), _i64(scols, dev), _i64(dcols, dev), sig, dst, dst_rs, dst_cs)
 
 
-def select_basis_indices(sset: np.ndarray, qnlist: List[tuple], Mmax: int, percent=0) -> List[int]:
-    """The index choice of lib.py:253-298 (select_basis) on host scalars."""
-    qnlist = [tuple(q) for q in qnlist]
-    qnset = set(qnlist)
-    basdic = {i: [qnlist[i], sset[i]] for i in range(len(qnlist)) if qnlist[i] in qnset}
-
-    def block_select(qn, n):
-        block = {i: basdic[i] for i in basdic if basdic[i][0] == qn}
-        srt = sorted(block.items(), key=lambda x: x[1][1], reverse=True)
-        sidx = [i[0] for i in srt[0:min(n, len(srt))]]
-        for idx in sidx:
-            del basdic[idx]
-        return sidx
-
-    nbasis = min(len(basdic), Mmax)
-    sidx = []
+def _select_by_code(sset: np.ndarray, codes: np.ndarray, visit: List[int], Mmax: int, percent=0) -> List[int]:
+    """select_basis_indices on integer QN codes; ``visit`` lists the codes in
+    the order the reference's set(qnlist) iterates the QNs they stand for."""
+    n = len(sset)
+    nbasis = min(n, Mmax)
+    alive = np.ones(n, dtype=bool)
+    sidx: List[int] = []
     if percent != 0:
-        nbas_block = int(nbasis * percent / len(qnset))
-        for iqn in qnset:
-            sidx += block_select(iqn, nbas_block)
+        nbas_block = int(nbasis * percent / len(visit))
+        for c in visit:
+            cand = np.flatnonzero(alive & (codes == c))
+            take = cand[np.argsort(-sset[cand], kind="stable")][:nbas_block]
+            alive[take] = False
+            sidx += take.tolist()
     nbasis = nbasis - len(sidx)
-    srt = sorted(basdic.items(), key=lambda x: x[1][1], reverse=True)
-    sidx += [i[0] for i in srt[0:nbasis]]
+    cand = np.flatnonzero(alive)
+    sidx += cand[np.argsort(-sset[cand], kind="stable")][:nbasis].tolist()
     assert len(sidx) == len(set(sidx))
     return sidx
+
+
+def select_basis_indices(sset: np.ndarray, qnlist: List[tuple], Mmax: int, percent=0) -> List[int]:
+    """The index choice of lib.py:253-298 (select_basis) on host scalars.
+
+    Same order and tie-breaking as the reference's sorted(..., reverse=True)
+    over index-ordered dicts (equal sigma keep index order), with the QN
+    blocks of the reserved fraction visited in the reference's set order;
+    each selection is one stable numpy argsort instead of dict rebuilding."""
+    qnlist = [tuple(q) for q in qnlist]
+    code = {}
+    for q in qnlist:
+        code.setdefault(q, len(code))
+    codes = np.fromiter((code[q] for q in qnlist), dtype=np.int64, count=len(qnlist))
+    return _select_by_code(np.asarray(sset, dtype=np.float64), codes, [code[q] for q in set(qnlist)], Mmax,
+                           percent)
 
 
 def _completion(vecs: torch.Tensor, npad: int) -> torch.Tensor:
@@ -532,26 +542,23 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         b.pop("Q", None)
     # the reference's concatenated order: nonzero parts block by block, then
     # the zero-sigma paddings block by block (svd_qn.py:222-230)
-    sig, qns, where = [], [], []
-    for bi, b in enumerate(blocks):
-        for j in range(b["dim"]):
-            sig.append(b["Sh"][j])
-            qns.append(b["nl"] if keep_left else b["nr"])
-            where.append((bi, j))
-    for bi, b in enumerate(blocks):
-        for p in range(b["npad"]):
-            sig.append(0.0)
-            qns.append(b["nl"] if keep_left else b["nr"])
-            where.append((bi, b["dim"] + p))
-    sig = np.asarray(sig, dtype=np.float64)
+    # (entry -> block bi, position j); block bi's QN is its code: the blocks'
+    # sectors are distinct and appear in block order
+    sig = np.concatenate([np.asarray(b["Sh"][:b["dim"]], dtype=np.float64) for b in blocks] +
+                         [np.zeros(b["npad"]) for b in blocks])
+    blk = np.concatenate([np.full(b["dim"], bi, dtype=np.int64) for bi, b in enumerate(blocks)] +
+                         [np.full(b["npad"], bi, dtype=np.int64) for bi, b in enumerate(blocks)])
+    pos = np.concatenate([np.arange(b["dim"], dtype=np.int64) for b in blocks] +
+                         [b["dim"] + np.arange(b["npad"], dtype=np.int64) for b in blocks])
+    qkey = [tuple(b["nl"] if keep_left else b["nr"]) for b in blocks]
+    code_of = {q: bi for bi, q in enumerate(qkey)}
     mtr = m_trunc_fn(sig)
-    sidx = select_basis_indices(sig, qns, mtr, percent)
+    sidx = _select_by_code(sig, blk, [code_of[q] for q in set(qkey)], mtr, percent)
     mdim = len(sidx)
     left = torch.zeros((rows, mdim), dtype=coef.dtype, device=coef.device)
     right = torch.zeros((mdim, cols), dtype=coef.dtype, device=coef.device)
     per_block = {}
-    for out_col, i in enumerate(sidx):
-        bi, j = where[i]
+    for out_col, (bi, j) in enumerate(zip(blk[sidx].tolist(), pos[sidx].tolist())):
         per_block.setdefault(bi, ([], []))
         per_block[bi][0].append(j)
         per_block[bi][1].append(out_col)
@@ -575,7 +582,7 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
                      right, 1, cols)
             if nz:
                 _scatter(eng, b["P"], b["lset"], [j for j, _ in nz], [o for _, o in nz], None, left, mdim, 1)
-    qn_new = np.array([qns[i] for i in sidx]).reshape(mdim, -1)
+    qn_new = np.array([qkey[bi] for bi in blk[sidx].tolist()]).reshape(mdim, -1)
     return TruncatedSplit(left, right, qn_new, mdim, sig[sidx])
 
 

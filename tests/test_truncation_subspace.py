@@ -189,3 +189,26 @@ def test_device_eigensolver_fallback_host_logic(cpu_engine, monkeypatch):
     np.testing.assert_array_equal(np.asarray(got.qn), np.asarray(full.qn))
     np.testing.assert_allclose(got.sigma, full.sigma, rtol=1e-12)
     assert torch.allclose(got.left @ got.right, full.left @ full.right, atol=1e-12)
+
+
+@pytest.mark.parametrize("percent", [0, 0.1, 0.3])
+def test_select_basis_indices_matches_oracle(percent):
+    """the vectorised basis selection returns exactly the reference rule's
+    indices (oracle select_basis, lib.py:253-298), ties included"""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+    import reno_oracle
+    from renormalizer_b200.svd_qn import select_basis_indices
+    rng = np.random.default_rng(6)
+    for trial in range(40):
+        n = int(rng.integers(1, 300))
+        nq = int(rng.integers(1, 5))
+        sig = np.round(rng.random(n), 2) * (rng.random(n) > 0.2)   # many ties and zeros
+        qns = [(int(q),) for q in rng.integers(0, nq, n)]
+        M = int(rng.integers(1, n + 20))
+        got = select_basis_indices(sig, qns, M, percent)
+        vset = np.eye(n)
+        ms, mpsdim, mpsqn, _ = reno_oracle.select_basis(vset, sig, qns, None, M, percent)
+        ref = [int(np.argmax(ms[:, j])) for j in range(mpsdim)]
+        assert got == ref, (trial, n, M)
