@@ -247,12 +247,10 @@ inline size_t smem_bytes() {
 template <bool AC, bool BC>
 inline cudaError_t launch_t(const GemmParams& p, cudaStream_t st) {
   const size_t sm = smem_bytes<AC, BC>();
-  static bool attr_set = false;  // per process; all devices are sm_100a
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<AC, BC>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  static std::atomic<unsigned long long> smem_set{0};
+  {
+    cudaError_t e = smem_optin_once(gemm_kernel<AC, BC>, (int)sm, smem_set);
     if (e != cudaSuccess) return e;
-    attr_set = true;
   }
   dim3 grid((unsigned)ceil_div(p.N, BN), (unsigned)ceil_div(p.M, BM), (unsigned)p.batch);
   count_launch();
@@ -263,12 +261,10 @@ inline cudaError_t launch_t(const GemmParams& p, cudaStream_t st) {
 template <bool AC, bool BC>
 inline cudaError_t launch_grouped_t(const GemmGroup& g, cudaStream_t st) {
   const size_t sm = smem_bytes<AC, BC>();
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_grouped_kernel<AC, BC>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  static std::atomic<unsigned long long> smem_set{0};
+  {
+    cudaError_t e = smem_optin_once(gemm_grouped_kernel<AC, BC>, (int)sm, smem_set);
     if (e != cudaSuccess) return e;
-    attr_set = true;
   }
   if (g.first[g.count] == 0) return cudaSuccess;
   count_launch();

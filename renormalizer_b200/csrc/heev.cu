@@ -821,31 +821,21 @@ extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, doub
   cudaStream_t st = ctx->stream;
   int rc = check_cuda(ctx, cudaMemsetAsync(sync, 0, sizeof(Sync), st), "reno_heev_top: memset");
   if (rc != RENO_OK) return rc;
-  static bool attr_set = false;
-  if (!attr_set) {
-    rc = check_cuda(ctx, cudaFuncSetAttribute(hetrd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * MAX_N * 16),
-                    "reno_heev_top: hetrd smem attribute");
-    if (rc == RENO_OK)
-      rc = check_cuda(ctx, cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                2 * MAX_N * (int)sizeof(double)),
-                      "reno_heev_top: bisect smem attribute");
-    if (rc == RENO_OK)
-      rc = check_cuda(ctx, cudaFuncSetAttribute(inviter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                2 * MAX_N * (int)sizeof(double)),
-                      "reno_heev_top: inverse iteration smem attribute");
-    if (rc != RENO_OK) return rc;
-    attr_set = true;
-  }
+  static std::atomic<unsigned long long> hetrd_set{0}, bisect_set{0}, inviter_set{0};
+  rc = check_cuda(ctx, smem_optin_once(hetrd_kernel, 3 * MAX_N * 16, hetrd_set), "reno_heev_top: hetrd smem attribute");
+  if (rc == RENO_OK)
+    rc = check_cuda(ctx, smem_optin_once(bisect_kernel, 2 * MAX_N * (int)sizeof(double), bisect_set),
+                    "reno_heev_top: bisect smem attribute");
+  if (rc == RENO_OK)
+    rc = check_cuda(ctx, smem_optin_once(inviter_kernel, 2 * MAX_N * (int)sizeof(double), inviter_set),
+                    "reno_heev_top: inverse iteration smem attribute");
+  if (rc != RENO_OK) return rc;
   if (n <= NMAX_C) {
     // 1. tridiagonal reduction of a small matrix: one thread-block cluster
-    static bool cl_attr = false;
-    if (!cl_attr) {
-      rc = check_cuda(ctx, cudaFuncSetAttribute(hetrd_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)cluster_smem_bytes(NMAX_C)),
-                      "reno_heev_top: cluster smem attribute");
-      if (rc != RENO_OK) return rc;
-      cl_attr = true;
-    }
+    static std::atomic<unsigned long long> cluster_set{0};
+    rc = check_cuda(ctx, smem_optin_once(hetrd_cluster_kernel, (int)cluster_smem_bytes(NMAX_C), cluster_set),
+                    "reno_heev_top: cluster smem attribute");
+    if (rc != RENO_OK) return rc;
     count_launch();
     hetrd_cluster_kernel<<<dim3(CL, 1), CT, cluster_smem_bytes(n), st>>>(static_cast<const double2*>(A),
                                                                          static_cast<double2*>(A), n, d, e,

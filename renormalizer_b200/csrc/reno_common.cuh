@@ -45,4 +45,19 @@ inline int check_cuda(reno_ctx* ctx, cudaError_t e, const char* what) {
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Opt a kernel into `bytes` of dynamic shared memory once per device:
+// function attributes belong to each device's context, so a process that
+// drives several GPUs sets them on each (bit d of `done` = device d).
+template <typename Kernel>
+inline cudaError_t smem_optin_once(Kernel* kernel, int bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
+
 }  // namespace reno

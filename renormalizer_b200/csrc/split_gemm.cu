@@ -809,11 +809,10 @@ static cudaError_t launch_split(const SplitPacked& A, const SplitPacked& B, int 
     epi.accumulate = c->accumulate;
     epi.c_f32 = c->c_f32;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(split_gemm_kernel<ESZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  static std::atomic<unsigned long long> smem_set{0};
+  {
+    cudaError_t e = smem_optin_once(split_gemm_kernel<ESZ>, SMEM_BYTES, smem_set);
     if (e != cudaSuccess) return e;
-    attr_set = true;
   }
   const int64_t kstep = KROW_BYTES / ESZ;
   const int64_t mt = ceil_div(A.rows, BM), nt = ceil_div(B.rows, BN);
