@@ -44,7 +44,10 @@ int scratch_for(reno_ctx* ctx, void** out) {
     }
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_heff_noalloc_scratch);
-    if (prev != ctx->device) cudaSetDevice(prev);
+    if (prev != ctx->device) {
+      const cudaError_t er = cudaSetDevice(prev);
+      if (er != cudaSuccess) return reno::check_cuda(ctx, er, "reno_heff_apply_noalloc: restoring the device");
+    }
     if (e != cudaSuccess) return reno::check_cuda(ctx, e, "reno_heff_apply_noalloc: cudaGetSymbolAddress");
     g_scratch_addr[ctx->device] = p;
   }
@@ -65,6 +68,16 @@ extern "C" int reno_heff_apply_noalloc(reno_ctx* ctx, const reno_heff_desc* desc
                                " bytes of scratch but the built-in array holds " +
                                std::to_string((size_t)RENO_NOALLOC_SCRATCH_BYTES) +
                                "; call reno_heff_apply with a workspace instead");
+  // the kernels launch on the caller's current device: the scratch address
+  // must belong to that device
+  int cur = -1;
+  const cudaError_t ce = cudaGetDevice(&cur);
+  if (ce != cudaSuccess) return reno::check_cuda(ctx, ce, "reno_heff_apply_noalloc: cudaGetDevice");
+  if (cur != ctx->device)
+    return reno::set_error(ctx, RENO_ERR_INVALID,
+                           "reno_heff_apply_noalloc: the current device (" + std::to_string(cur) +
+                               ") is not the context's device (" + std::to_string(ctx->device) +
+                               "); make the context's device current first");
   void* scratch = nullptr;
   const int st = scratch_for(ctx, &scratch);
   if (st != RENO_OK) return st;

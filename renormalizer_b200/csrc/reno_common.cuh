@@ -60,4 +60,21 @@ inline cudaError_t smem_optin_once(Kernel* kernel, int bytes, std::atomic<unsign
   return e;
 }
 
+// SM count of the current device, read once per device (entry d of a
+// per-process table; 0 = not read yet) and safe under concurrent first calls.
+inline int sm_count_current_device() {
+  static std::atomic<int> table[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (dev < 0 || dev >= 64) {
+    int n = 0;
+    return (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0) ? n : 148;
+  }
+  int n = table[dev].load(std::memory_order_relaxed);
+  if (n > 0) return n;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  table[dev].store(n, std::memory_order_relaxed);
+  return n;
+}
+
 }  // namespace reno

@@ -820,12 +820,7 @@ static cudaError_t launch_split(const SplitPacked& A, const SplitPacked& B, int 
   const int m_fast = (A.rows <= B.rows && mt > 1) ? 1 : 0;
   const int64_t ntiles = mt * nt * (int64_t)batch;
   if (ntiles > 0x7fffffff) return cudaErrorInvalidValue;
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-  }
+  const int sms = sm_count_current_device();
   const int grid = (int)std::min<int64_t>(ntiles, sms);  // one persistent CTA per SM
   count_launch();
   split_gemm_kernel<ESZ><<<grid, THREADS, SMEM_BYTES, st>>>(tAh, tAl, tBh, tBl, epi, (int)ceil_div(A.kext, kstep),

@@ -553,7 +553,13 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
     qkey = [tuple(b["nl"] if keep_left else b["nr"]) for b in blocks]
     code_of = {q: bi for bi, q in enumerate(qkey)}
     mtr = m_trunc_fn(sig)
-    sidx = _select_by_code(sig, blk, [code_of[q] for q in set(qkey)], mtr, percent)
+    # the reference iterates set(qnlist) over the per-entry QN list in entry
+    # order, where a block without nonzero entries first appears among the
+    # paddings; inserting the distinct QNs in first-occurrence order builds
+    # the same set (duplicates leave a set's table unchanged)
+    _, first = np.unique(blk, return_index=True)
+    visit_set = set(qkey[int(blk[i])] for i in np.sort(first))
+    sidx = _select_by_code(sig, blk, [code_of[q] for q in visit_set], mtr, percent)
     mdim = len(sidx)
     left = torch.zeros((rows, mdim), dtype=coef.dtype, device=coef.device)
     right = torch.zeros((mdim, cols), dtype=coef.dtype, device=coef.device)
