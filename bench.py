@@ -65,6 +65,15 @@ def parse():
     ap.add_argument("--accuracy", type=int, default=0, metavar="STEPS",
                     help="run STEPS steps with --prec and with plain FP64 from the same start and report the "
                          "largest site-population difference after every step (no timing)")
+    ap.add_argument("--start", default="random", choices=["random", "hint"],
+                    help="bond expansion of the start state: seeded random expander, or the reference's "
+                         "expand_bond_dimension(mpo, include_ex=False)")
+    ap.add_argument("--accuracy-precs", default="",
+                    help="comma-separated precisions compared with FP64 in --accuracy mode (default: --prec)")
+    ap.add_argument("--envelope", action="store_true",
+                    help="--accuracy mode: also evolve FP64 from the start state perturbed by one ulp per entry "
+                         "and report its distance from the unperturbed FP64 run (the FP64 engine's own envelope)")
+    ap.add_argument("--out", default="", help="append the per-step JSON lines of --accuracy mode to this file")
     ap.add_argument("--truncation", default="exact", choices=["exact", "subspace"],
                     help="exact (default): every QN block uses the full Gram eigendecomposition; subspace: blocks "
                          "with at least 1024 rows on the smaller side use the opt-in top-k subspace iteration")
@@ -96,12 +105,19 @@ def holstein_2mode(nmol, nlev):
     return HolsteinModel([Mol(Quantity(0), ph)] * nmol, Quantity(1.0), 3)
 
 
-def initial_state(model, M):
+def initial_state(model, M, start="random", mpo=None):
+    """Hartree product with the exciton on site 0, bond dimension expanded to
+    M: "hint" is the reference's idiom expand_bond_dimension(mpo,
+    include_ex=False) (coef 1e-10 weighted H^k psi directions); "random" adds
+    a seeded random expander instead."""
     from renormalizer_b200 import CompressConfig, CompressCriteria, EvolveConfig, EvolveMethod, Mps
     np.random.seed(2024)
     mps = Mps.hartree_product_state(model, {0: 1})
     mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=M)
-    mps = mps.expand_bond_dimension()
+    if start == "hint":
+        mps = mps.expand_bond_dimension(mpo, include_ex=False)
+    else:
+        mps = mps.expand_bond_dimension()
     mps.evolve_config = EvolveConfig(EvolveMethod.tdvp_ps2)
     return mps
 
@@ -556,27 +572,74 @@ def run_heff_only(args):
                       "gpu_launches_per_matvec": (launch_count() - l0) / args.steps}))
 
 
+def perturb_ulp(mps, seed=11):
+    """A copy of mps with every site-tensor entry moved by one unit in the last
+    place (random direction per entry and per real/imaginary part)."""
+    import torch
+    new = mps.copy()
+    g = torch.Generator(device=new[0].device).manual_seed(seed)
+    for i, t in enumerate(new._mp):
+        r = torch.view_as_real(t) if t.is_complex() else t
+        sign = torch.randint(0, 2, r.shape, device=r.device, generator=g).to(torch.float64) * 2 - 1
+        r2 = torch.nextafter(r, sign * float("inf")).contiguous()
+        new._mp[i] = torch.view_as_complex(r2) if t.is_complex() else r2
+    return new
+
+
 def run_accuracy(args):
-    """|population(prec) - population(FP64)| over --accuracy steps."""
+    """max |population(prec) - population(FP64)| after every step, for each
+    precision in --accuracy-precs, from the same start state; with
+    --envelope also FP64 from the 1-ulp perturbed start against FP64 (the
+    size of the FP64 engine's own trajectory spread).  Every step prints one
+    JSON line (and appends it to --out)."""
     import torch
     from renormalizer_b200 import Mpo, backend
     torch.cuda.set_device(0)
     model = holstein_2mode(args.nmol, args.nlev)
     mpo = Mpo(model)
-    mps0 = initial_state(model, args.M)
-    a, b = mps0, mps0
-    dev = []
+    t0 = time.time()
+    mps0 = initial_state(model, args.M, args.start, mpo)
+    t_start = time.time() - t0
+    precs = [p for p in (args.accuracy_precs or args.prec).split(",") if p and p != "fp64"]
+    arms = {p: mps0 for p in precs}
+    if args.envelope:
+        arms["fp64_ulp"] = perturb_ulp(mps0)
+    ref = mps0
+    out = open(args.out, "a") if args.out else None
+    worst = {k: 0.0 for k in arms}
+    step_s = {k: 0.0 for k in list(arms) + ["fp64"]}
+
+    def emit(obj):
+        line = json.dumps(obj)
+        print(line, flush=True)
+        if out:
+            out.write(line + "\n")
+            out.flush()
+
+    emit({"start": args.start, "start_s": t_start, "bond_dims": mps0.bond_dims, "nmol": args.nmol, "M": args.M,
+          "dt": args.dt, "arms": list(arms)})
     for step in range(args.accuracy):
-        backend.prec = args.prec
-        a = a.evolve(mpo, args.dt)
         backend.prec = "fp64"
-        b = b.evolve(mpo, args.dt)
-        dev.append(float(np.abs(a.e_occupations - b.e_occupations).max()))
-        print(json.dumps({"step": step + 1, "max_abs_dpop": dev[-1]}), flush=True)
-    print(json.dumps({"metric": f"max |population({args.prec}) - population(fp64)| per step",
-                      "workload": WORKLOAD, "M": args.M, "nmol": args.nmol, "dt": args.dt,
-                      "truncation": args.truncation, "steps": args.accuracy, "per_step": dev,
-                      "max": max(dev) if dev else None}), flush=True)
+        t1 = time.time()
+        ref = ref.evolve(mpo, args.dt)
+        pref = ref.e_occupations
+        step_s["fp64"] += time.time() - t1
+        row = {"step": step + 1}
+        for k in arms:
+            backend.prec = "fp64" if k == "fp64_ulp" else k
+            t1 = time.time()
+            arms[k] = arms[k].evolve(mpo, args.dt)
+            d = float(np.abs(arms[k].e_occupations - pref).max())
+            step_s[k] += time.time() - t1
+            worst[k] = max(worst[k], d)
+            row[k] = d
+        emit(row)
+    backend.prec = args.prec
+    emit({"metric": "max |population(arm) - population(fp64)| over the trajectory", "workload": WORKLOAD,
+          "nmol": args.nmol, "M": args.M, "dt": args.dt, "start": args.start, "steps": args.accuracy,
+          "max": worst, "s_per_step": {k: v / max(args.accuracy, 1) for k, v in step_s.items()}})
+    if out:
+        out.close()
 
 
 def run_dmrg(args):

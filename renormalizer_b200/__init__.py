@@ -12,7 +12,7 @@ from .configs import CompressConfig, CompressCriteria, EvolveConfig, EvolveMetho
 from .model import (BasisHalfSpin, BasisSHO, BasisSimpleElectron, HolsteinModel, Model, Mol, Op, Phonon, Quantity,
                     SpectralDensityFunction, SpinBosonModel)
 from .mpo import Mpo
-from .mps import Mps, evolve_batch
+from .mps import Mps, compressed_sum, evolve_batch
 from .lib import Environ, contract_one_site
 from .hop_expr import hop_expr
 from .krylov import expm_krylov
@@ -21,7 +21,7 @@ from .davidson import davidson
 from .gs import optimize_mps
 from .autodiff import heff as heff_autograd
 
-__all__ = ["backend", "evolve_batch", "CompressConfig", "CompressCriteria", "EvolveConfig", "EvolveMethod", "OptimizeConfig",
+__all__ = ["backend", "evolve_batch", "compressed_sum", "CompressConfig", "CompressCriteria", "EvolveConfig", "EvolveMethod", "OptimizeConfig",
            "BasisHalfSpin", "BasisSHO", "BasisSimpleElectron", "HolsteinModel", "Model", "Mol", "Op", "Phonon",
            "Quantity", "SpectralDensityFunction", "SpinBosonModel", "Mpo", "Mps", "Environ", "contract_one_site",
            "hop_expr", "expm_krylov", "svd_qn", "davidson", "optimize_mps", "heff_autograd"]

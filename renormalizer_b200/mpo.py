@@ -115,16 +115,48 @@ def build_mpo_tensors(model: Model, terms: Sequence[Op], offset: float = 0.0) ->
     return Ws
 
 
+def mpo_qn_labels(model: Model, tensors: Sequence[np.ndarray]):
+    """Bond QN labels of an MPO in the reference's convention
+    (symbolic_mpo.py:105-161): the label of a channel is the QN its operators
+    add to the sites on its left, the last bond is labelled 0 and the total
+    goes to qntot.  Derived from the tensors: every nonzero entry
+    W[a, bra, ket, b] moves QN qn[a] + sigmaqn[bra] - sigmaqn[ket] into
+    channel b.  Channels no entry reaches are labelled 0."""
+    n = len(tensors)
+    if model is None or n == 0:
+        return [], None
+    qs = model.qn_size
+    qn = [np.zeros((1, qs), dtype=int)]
+    for i, W in enumerate(tensors):
+        sq = np.asarray(model.basis[i].sigmaqn, dtype=int).reshape(W.shape[1], -1)
+        lab = np.zeros((W.shape[3], qs), dtype=int)
+        seen = np.zeros(W.shape[3], dtype=bool)
+        a, p, q, b = np.nonzero(W)
+        for ai, pi, qi, bi in zip(a, p, q, b):
+            v = qn[i][ai] + sq[pi] - sq[qi]
+            if not seen[bi]:
+                lab[bi] = v
+                seen[bi] = True
+        qn.append(lab)
+    qntot = qn[-1][0].copy()
+    qn[-1] = np.zeros((1, qs), dtype=int)
+    return qn, qntot
+
+
 class Mpo:
     """Drop-in for the parts of renormalizer.mps.Mpo the sweep path reads:
     construction from a Model (optionally with an energy offset), len(),
-    indexing (device site tensors), identity / onsite constructors."""
+    indexing (device site tensors), identity / onsite constructors, bond QN
+    labels (qn, qnidx, qntot) and the MPO x MPS product (``@``)."""
 
     def __init__(self, model: Model = None, terms: Union[Op, List[Op]] = None, offset: Quantity = Quantity(0)):
         self.model = model
         self.offset = 0.0
         self._np: List[np.ndarray] = []
         self._dev: List[torch.Tensor] = []
+        self.qn: List[np.ndarray] = []
+        self.qntot = None
+        self.qnidx = None
         if model is None:
             return
         if not isinstance(offset, Quantity):
@@ -151,6 +183,46 @@ class Mpo:
         self._np = [np.ascontiguousarray(t) for t in tensors]
         dev = backend.device if torch.cuda.is_available() else None
         self._dev = [torch.from_numpy(t).to(dev) if dev is not None else torch.from_numpy(t) for t in self._np]
+        self.qn, self.qntot = mpo_qn_labels(self.model, self._np)
+        self.qnidx = len(self._np) - 1
+
+    def apply(self, mp, canonicalise: bool = False):
+        """MPO x MPS (mpo.py:331-389): site i becomes
+        einsum("apqb,cqd->acpbd") reshaped to (a c, p, b d), the bond QN
+        labels add as add_outer(mpo qn, mps qn) with the MPS labels taken on
+        the MPO's boundary (qnidx), and the total QN adds."""
+        from .mps import Mps
+        from .svd_qn import add_outer
+        assert len(self) == len(mp)
+        new = mp.copy()
+        if self.dtype == torch.complex128 and not new.is_complex:
+            new.to_complex(inplace=True)
+        from ._native import Engine
+        dt = new.dtype
+        sites = []
+        for W, ms in zip(self._dev, new._mp):
+            a, p, q, b = W.shape
+            c, q2, d = ms.shape
+            assert q == q2
+            eng = Engine.get(ms.device)
+            # (a p b, q) x (q, c d) on the engine's GEMM, then (a, c, p, b, d)
+            wm = W.to(dt).permute(0, 1, 3, 2).reshape(a * p * b, q).contiguous()
+            mm = ms.to(dt).permute(1, 0, 2).reshape(q, c * d).contiguous()
+            t = eng.matmul(wm, mm).reshape(a, p, b, c, d).permute(0, 3, 1, 2, 4)
+            sites.append(t.reshape(a * c, p, b * d).contiguous())
+        new._mp = sites
+        orig = new.qnidx
+        new.move_qnidx(self.qnidx)
+        new.qn = [add_outer(np.asarray(qo), np.asarray(qm)).reshape(-1, qo.shape[1])
+                  for qo, qm in zip(self.qn, new.qn)]
+        new.qntot = new.qntot + self.qntot
+        new.move_qnidx(orig)
+        if canonicalise:
+            new.canonicalise()
+        return new
+
+    def __matmul__(self, other):
+        return self.apply(other)
 
     @classmethod
     def identity(cls, model: Model) -> "Mpo":

@@ -13,8 +13,8 @@ the sweep path uses:
   (890-922), ``compress`` (437-511);
 * ``evolve`` with ``tdvp_ps`` (mps.py:1267-1404) and ``tdvp_ps2``
   (1406-1517), ``normalize`` (2025-2059), ``expectation`` / ``expectations``
-  / ``e_occupations`` (471-609), ``expand_bond_dimension`` (1934-2023, the
-  random expander).
+  / ``e_occupations`` (471-609), ``expand_bond_dimension`` (1934-2023, with
+  the random or the hint-MPO expander), ``compressed_sum`` (lib.py:417-440).
 
 Site tensors are device tensors in the reference layout (M_l, d, M_r); QN
 labels are small host integer arrays.  Every contraction, vector operation
@@ -781,21 +781,73 @@ class Mps:
         return np.array([res[s] for s in sites])
 
     # ------------------------------------------------------------ bond expansion
-    def expand_bond_dimension(self, hint_mpo=None, coef=1e-10, include_ex=True):
-        """mps.py:1963-2023 with the random expander (hint_mpo=None): add a
-        coef-weighted random MPS with the missing bond dimension, then
-        canonicalise, compress to max_dims and move the norm to coeff."""
-        if hint_mpo is not None:
-            raise NotImplementedError("the hint-MPO expander needs MPO x MPS products, outside the sweep engine")
-        self.compress_config.set_bonddim(len(self.bond_dims))
+    @classmethod
+    def ground_state(cls, model: Model, max_entangled: bool = False) -> "Mps":
+        """mps.py:259-350 for max_entangled=False: every site in its basis
+        state 0 (electrons empty, SHO modes in their ground state), QN 0."""
+        if max_entangled:
+            raise NotImplementedError("the maximally entangled (T = infinity) state belongs to the MPDM path")
+        sites = []
+        for b in model.basis:
+            ms = np.zeros((1, b.nbas, 1))
+            ms[0, 0, 0] = 1.0
+            sites.append(ms)
+        qn = [np.zeros((1, model.qn_size), dtype=int) for _ in range(model.nsite + 1)]
+        return cls.from_arrays(model, sites, qn, model.nsite - 1, np.zeros(model.qn_size, dtype=int), False)
+
+    @property
+    def bond_dims_exact(self) -> np.ndarray:
+        """mp.py:131-142: bond dimensions of an exact factorisation"""
         pb = np.array(self.pbond_list, dtype=float)
         with np.errstate(over="ignore"):
             d1 = [1] + list(np.cumprod(pb))
             d2 = ([1] + list(np.cumprod(pb[::-1])))[::-1]
-        exact = np.minimum(d1, d2)
-        m_target = np.minimum(np.array(self.compress_config.max_dims) - np.array(self.bond_dims), exact).astype(int)
-        m_target = np.maximum(m_target, 1)
-        expander = Mps.random(self.model, self.qntot, m_target)
+        return np.minimum(d1, d2)
+
+    def expand_bond_dimension(self, hint_mpo=None, coef=1e-10, include_ex=True):
+        """mps.py:1934-2023: add a coef-weighted expander with the missing
+        bond dimension, then canonicalise, compress to max_dims and move the
+        norm to coeff.  Without ``hint_mpo`` the expander is a random MPS;
+        with it, the expander is the compressed sum of the normalised states
+        H psi, H^2 psi, ... (psi plus the excited product state when
+        ``include_ex``), grown until every bond reaches its target or stops
+        growing."""
+        self.compress_config.set_bonddim(len(self.bond_dims))
+        m_target = np.minimum(np.array(self.compress_config.max_dims) - np.array(self.bond_dims),
+                              self.bond_dims_exact).astype(int)
+        if hint_mpo is None:
+            expander = Mps.random(self.model, self.qntot, np.maximum(m_target, 1))
+        else:
+            if include_ex:
+                assert self.model.qn_size == 1, "the excited expander state supports one QN only"
+                ex = Mps.ground_state(self.model, False)
+                for _ in range(int(self.qntot[0])):
+                    ex = Mpo.onsite(self.model, r"a^\dagger") @ ex
+                ex.compress_config = self.compress_config
+                ex.move_qnidx(self.qnidx)
+                ex.to_right = self.to_right
+                lastone = self + ex
+            else:
+                lastone = self
+            expander_list = []
+            expander_dims = np.zeros_like(m_target)
+            hint_max = int(np.max(hint_mpo.bond_dims))
+            while True:
+                lastone = (hint_mpo @ lastone).normalize("mps_and_coeff")
+                lastone = lastone.canonicalise().compress(int(np.max(m_target)))
+                expander_list.append(lastone)
+                expander = compressed_sum(expander_list, temp_m_trunc=m_target)
+                dims = np.array(expander.bond_dims)
+                if np.all(dims >= m_target):
+                    break
+                if np.all(dims == expander_dims):
+                    logger.warning("Expander does not increase anymore. The expand target is too high")
+                    m_target2 = int(np.max(m_target - expander_dims))
+                    expander2 = (hint_mpo @ lastone).canonicalise().compress(max(m_target2, 1))
+                    expander = expander + expander2
+                    break
+                expander_dims = dims
+                lastone = lastone.canonicalise().compress(int(np.max(m_target) / hint_max) + 1)
         total = self + expander.scale(coef * self.norm, inplace=True)
         total.canonicalise()
         total.compress(self.compress_config.max_dims)
@@ -928,6 +980,25 @@ class Mps:
 
     def __str__(self):
         return f"mps bond dim:{self.bond_dims}"
+
+
+def compressed_sum(mps_list: List[Mps], batchsize=5, temp_m_trunc=None) -> Mps:
+    """lib.py:417-440: sum the list in groups of ``batchsize``, each partial
+    sum canonicalised and compressed (a single MPS is compressed in place)."""
+    assert len(mps_list) != 0
+    queue = list(mps_list)
+    if len(queue) == 1:
+        new = queue[0].canonicalise()
+        return new.compress(temp_m_trunc=temp_m_trunc)
+    while len(queue) != 1:
+        group, queue = queue[:batchsize], queue[batchsize:]
+        s = group[0]
+        for other in group[1:]:
+            s = s.add(other)
+        s.canonicalise()
+        s.compress(temp_m_trunc=temp_m_trunc)
+        queue.append(s)
+    return queue[0]
 
 
 def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True) -> List[Mps]:
