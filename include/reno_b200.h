@@ -172,6 +172,52 @@ int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, void* A,
                             size_t ws_bytes);
 int reno_heev_status_offset(size_t* offset);
 
+/* The same for up to RENO_HEEV_MAX_BATCH matrices at once (the QN blocks of
+ * one bond): the matrices above 256 share one cooperative reduction launch,
+ * the grid divided among them in proportion to n^2.  status[i] (device int)
+ * receives problem i's status word.  k is used by the back-transformation
+ * only.  Workspace from reno_heev_batched_workspace_bytes. */
+#define RENO_HEEV_MAX_BATCH 8
+typedef struct {
+  int32_t n, kt;
+  void* a;      /* n x n complex128, private copy, overwritten */
+  double* d;    /* n */
+  double* e;    /* n - 1 */
+  void* tau;    /* n - 1 complex128 */
+  double* w;    /* kt eigenvalues, ascending */
+  double* z;    /* n x kt tridiagonal eigenvectors */
+  void* k;      /* n x kt complex128: in Z (orthonormalised), out Q Z */
+} reno_heev_problem;
+int reno_heev_batched_workspace_bytes(int32_t count,
+                                      const reno_heev_problem* probs,
+                                      size_t* bytes);
+int reno_heev_top_batched(reno_ctx* ctx, int32_t count,
+                          const reno_heev_problem* probs, int32_t* status,
+                          void* ws, size_t ws_bytes);
+int reno_heev_backtransform_batched(reno_ctx* ctx, int32_t count,
+                                    const reno_heev_problem* probs, void* ws,
+                                    size_t ws_bytes);
+
+/* Householder QR of the QN blocks of one site tensor, svd_qn.py:195-204
+ * (scipy.linalg.qr(mode="economic") per block; the RQ of system "R" is the
+ * QR of the reversed conjugate transpose, done by the caller).  LAPACK
+ * conventions (zgeqrf/dgeqrf + zungqr/dorgqr): R's diagonal is
+ * beta_j = -sign(Re alpha_j) |column|, so Q and R carry scipy's signs.
+ * Each block: a (m x k, row-major, overwritten), q (m x min(m,k)), r
+ * (min(m,k) x k, upper trapezoidal), all of one dtype.  1 <= count <=
+ * RENO_QR_MAX_BLOCKS; m up to 81920.  Workspace from reno_qr_workspace_bytes. */
+#define RENO_QR_MAX_BLOCKS 16
+typedef struct {
+  int32_t m, k, dtype, reserved;
+  void* a;
+  void* q;
+  void* r;
+} reno_qr_block;
+int reno_qr_workspace_bytes(int32_t count, const reno_qr_block* blocks,
+                            size_t* bytes);
+int reno_qr_blocks(reno_ctx* ctx, int32_t count, const reno_qr_block* blocks,
+                   void* workspace, size_t ws_bytes);
+
 /* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
  *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]
  *   nsite 2: hdiag[a,c,d,f] = sum L[a,b,a] W1[b,c,c,e] W2[e,d,d,g] R[f,g,f]

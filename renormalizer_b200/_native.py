@@ -29,6 +29,22 @@ class HeffDesc(ctypes.Structure):
                 ("nsite", "ml", "mr", "wl", "wm", "wr", "d1", "d2", "psi_dtype", "env_dtype", "mpo_dtype", "prec")]
 
 
+class QrBlock(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_int32), ("k", ctypes.c_int32), ("dtype", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("a", _vp), ("q", _vp), ("r", _vp)]
+
+
+QR_MAX_BLOCKS = 16
+
+
+class HeevProblem(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("kt", ctypes.c_int32), ("a", _vp), ("d", _vp), ("e", _vp), ("tau", _vp),
+                ("w", _vp), ("z", _vp), ("k", _vp)]
+
+
+HEEV_MAX_BATCH = 8
+
+
 class EnvDesc(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in
                 ("side", "d", "w_in", "w_out", "mk_in", "mk_out", "mb_in", "mb_out", "env_dtype", "ket_dtype",
@@ -60,6 +76,11 @@ _SIGS = {
     "reno_heev_top": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_sz]),
     "reno_heev_backtransform": (_c_int, [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _c_sz]),
     "reno_heev_status_offset": (_c_int, [ctypes.POINTER(_c_sz)]),
+    "reno_heev_batched_workspace_bytes": (_c_int, [_c_int, ctypes.POINTER(HeevProblem), ctypes.POINTER(_c_sz)]),
+    "reno_heev_top_batched": (_c_int, [_vp, _c_int, ctypes.POINTER(HeevProblem), _vp, _vp, _c_sz]),
+    "reno_heev_backtransform_batched": (_c_int, [_vp, _c_int, ctypes.POINTER(HeevProblem), _vp, _c_sz]),
+    "reno_qr_workspace_bytes": (_c_int, [_c_int, ctypes.POINTER(QrBlock), ctypes.POINTER(_c_sz)]),
+    "reno_qr_blocks": (_c_int, [_vp, _c_int, ctypes.POINTER(QrBlock), _vp, _c_sz]),
     "reno_heff_backward_workspace_bytes": (_c_int, [ctypes.POINTER(HeffDesc), ctypes.POINTER(_c_sz)]),
     "reno_heff_backward": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                     _vp, _vp, _c_sz]),
@@ -247,6 +268,50 @@ class Engine:
         self.check(self.lib.reno_heff_backward(self.ctx, ctypes.byref(desc), ptr(L), opt(W1), opt(W2), ptr(R), ptr(psi),
                                                ptr(gy), opt(gpsi), opt(gL), opt(gW1), opt(gW2), opt(gR), ptr(ws),
                                                ws.numel()), "reno_heff_backward")
+
+    def heev_batched(self, probs, status, ws, stage):
+        """reno_heev_top_batched (stage "top") or reno_heev_backtransform_batched
+        (stage "back") on a list of HeevProblem; ws sized by heev_batched_bytes"""
+        arr = (HeevProblem * len(probs))(*probs)
+        if stage == "top":
+            self.check(self.lib.reno_heev_top_batched(self.ctx, len(probs), arr, ptr(status), ptr(ws), ws.numel()),
+                       "reno_heev_top_batched")
+        else:
+            self.check(self.lib.reno_heev_backtransform_batched(self.ctx, len(probs), arr, ptr(ws), ws.numel()),
+                       "reno_heev_backtransform_batched")
+
+    def heev_batched_bytes(self, probs) -> int:
+        arr = (HeevProblem * len(probs))(*probs)
+        n = _c_sz()
+        self.check(self.lib.reno_heev_batched_workspace_bytes(len(probs), arr, ctypes.byref(n)),
+                   "reno_heev_batched_workspace_bytes")
+        return int(n.value)
+
+    def qr_blocks(self, mats):
+        """Economic Householder QR of every matrix of ``mats`` (2-D device
+        tensors of one dtype; not modified): lists Q (m x min(m,k)) and R
+        (min(m,k) x k) with LAPACK's signs (reno_qr_blocks)."""
+        Qs, Rs = [], []
+        for i0 in range(0, len(mats), QR_MAX_BLOCKS):
+            part = mats[i0:i0 + QR_MAX_BLOCKS]
+            blocks, keep = [], []
+            for a in part:
+                m, k = a.shape
+                kq = min(m, k)
+                work = a.contiguous().clone()
+                q = torch.empty((m, kq), dtype=a.dtype, device=a.device)
+                r = torch.empty((kq, k), dtype=a.dtype, device=a.device)
+                keep += [work, q, r]
+                blocks.append(QrBlock(m, k, dtype_code(a), 0, _vp(work.data_ptr()), _vp(q.data_ptr()),
+                                      _vp(r.data_ptr())))
+                Qs.append(q)
+                Rs.append(r)
+            arr = (QrBlock * len(blocks))(*blocks)
+            n = _c_sz()
+            self.check(self.lib.reno_qr_workspace_bytes(len(blocks), arr, ctypes.byref(n)), "reno_qr_workspace_bytes")
+            ws = self.workspace(int(n.value))
+            self.check(self.lib.reno_qr_blocks(self.ctx, len(blocks), arr, ptr(ws), ws.numel()), "reno_qr_blocks")
+        return Qs, Rs
 
     def device_error(self) -> int:
         """first timed-out wait of the tensor-core kernels since the last call (0 = none)"""

@@ -94,41 +94,37 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;
 }
 
-// grid barrier: false when this or another CTA gave up (abort raised)
-__device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& gen, int* ok_sh) {
+// grid barrier over the nblocks CTAs that share `s`: a monotonic arrival
+// counter (no reset between columns), released by each CTA's thread 0 after
+// a CTA barrier and acquired by polling, the ordering pattern of CUTLASS's
+// generic barrier.  false when this or another CTA gave up (abort raised).
+__device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& epoch, int* ok_sh) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned g = gen;
+    epoch += 1u;
+    const unsigned target = epoch * nblocks;
     bool good = true;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&s->count, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(&s->count, 0u);
-      __threadfence();
-      atomicExch(&s->gen, g + 1u);
-    } else {
-      volatile unsigned* vg = &s->gen;
-      volatile int* va = &s->abort;
-      const uint64_t t0 = global_ns();
-      for (uint32_t it = 0;; ++it) {
-        if (*vg != g) break;
-        if ((it & 63u) == 63u) {
-          if (*va) {
-            good = false;
-            break;
-          }
-          if (global_ns() - t0 > WAIT_NS) {
-            atomicExch(&s->abort, 1);
-            atomicCAS(&s->status, 0, 1);
-            good = false;
-            break;
-          }
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&s->count) : "memory");
+    volatile int* va = &s->abort;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0;; ++it) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&s->count) : "memory");
+      if (v >= target) break;
+      if ((it & 63u) == 63u) {
+        if (*va) {
+          good = false;
+          break;
+        }
+        if (global_ns() - t0 > WAIT_NS) {
+          atomicExch(&s->abort, 1);
+          atomicCAS(&s->status, 0, 1);
+          good = false;
+          break;
         }
       }
     }
-    __threadfence();
-    gen = g + 1u;
-    *ok_sh = good && !*(volatile int*)&s->abort;
+    *ok_sh = good && !*va;
   }
   __syncthreads();
   return *ok_sh != 0;
@@ -136,13 +132,43 @@ __device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& gen, int* ok_sh) 
 
 constexpr int HT = 512, HW = HT / 32;  // reduction kernel: 16 warps, one CTA per SM
 constexpr int U1 = 4;                  // loads in flight per thread (rows k, y)
-constexpr int U2 = 4;                  // loads in flight per lane (trailing rows)
+constexpr int U2 = 8;                  // loads in flight per lane (trailing rows)
+constexpr int MAXM = 8;                // matrices per batched launch
+
+// One matrix of a batched reduction: CTAs first .. first + nblk - 1 of the
+// cooperative grid work on it, with their own barrier word and buffers.
+struct HetrdProb {
+  double2* A;
+  int n;
+  double* d;
+  double* e;
+  double2* tau;
+  double2* Y;
+  double2* P;
+  Sync* sync;
+  int first, nblk;
+};
+struct HetrdTable {
+  int count;
+  HetrdProb p[MAXM];
+};
 
 // A: n x n row-major Hermitian (both triangles), overwritten: row k holds
-// reflector k from column k+1 on.  Y: 2n, P: 2 * gridDim.x scratch.
-__global__ void __launch_bounds__(HT, 1)
-    hetrd_kernel(double2* __restrict__ A, int n, double* __restrict__ d, double* __restrict__ e,
-                 double2* __restrict__ tau, double2* __restrict__ Y, double2* __restrict__ P, Sync* sync) {
+// reflector k from column k+1 on.  Y: 2n, P: 2 * nblk scratch.  Every
+// matrix of the table is reduced by its own share of the grid.
+__global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ HetrdTable tab) {
+  int pi = 0;
+  while (pi + 1 < tab.count && (int)blockIdx.x >= tab.p[pi + 1].first) ++pi;
+  const HetrdProb& PR = tab.p[pi];
+  double2* __restrict__ A = PR.A;
+  const int n = PR.n;
+  double* __restrict__ d = PR.d;
+  double* __restrict__ e = PR.e;
+  double2* __restrict__ tau = PR.tau;
+  double2* __restrict__ Y = PR.Y;
+  double2* __restrict__ P = PR.P;
+  Sync* sync = PR.sync;
+  const int bid = (int)blockIdx.x - PR.first;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* vp = reinterpret_cast<double2*>(smem_raw);  // v of step k-1 (pending update)
   double2* wp = vp + n;                                // w of step k-1
@@ -152,7 +178,7 @@ __global__ void __launch_bounds__(HT, 1)
   __shared__ double s_akk;
   __shared__ int s_ok;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const unsigned G = gridDim.x;
+  const unsigned G = (unsigned)PR.nblk;
   unsigned gen = 0;
   for (int i = tid; i < n; i += HT) {
     vp[i] = make_double2(0.0, 0.0);
@@ -222,7 +248,7 @@ __global__ void __launch_bounds__(HT, 1)
       const double m2 = den.x * den.x + den.y * den.y;
       sc = make_double2(den.x / m2, -den.y / m2);
     }
-    if (blockIdx.x == 0 && tid == 0) {
+    if (bid == 0 && tid == 0) {
       d[k] = s_akk;
       e[k] = beta;
       tau[k] = tk;
@@ -231,12 +257,12 @@ __global__ void __launch_bounds__(HT, 1)
     // which no CTA reads any more
     for (int c = k + tid; c < n; c += HT) {
       if (c > k) vc[c] = (c == k + 1) ? make_double2(1.0, 0.0) : cmul(vc[c], sc);
-      if (blockIdx.x == 0 && k > 0) __stcg(&A[(size_t)(k - 1) * n + c], vp[c]);
+      if (bid == 0 && k > 0) __stcg(&A[(size_t)(k - 1) * n + c], vp[c]);
     }
     __syncthreads();
 
     // ---- phase 2 (rows split over all warps of the grid): update k-1, y = A v_k
-    const int gw = blockIdx.x * HW + warp, tw = (int)G * HW;
+    const int gw = bid * HW + warp, tw = (int)G * HW;
     double2 pdot = make_double2(0.0, 0.0);
     for (int r = k + 1 + gw; r < n; r += tw) {
       const double2 vpr = vp[r], wpr = wp[r];
@@ -270,7 +296,7 @@ __global__ void __launch_bounds__(HT, 1)
     if (tid == 0) {
       double2 s = make_double2(0.0, 0.0);
       for (int w = 0; w < HW; ++w) s = cadd(s, redc[w]);
-      __stcg(&P[(size_t)(k & 1) * G + blockIdx.x], s);
+      __stcg(&P[(size_t)(k & 1) * G + bid], s);
     }
     if (!grid_sync(sync, G, gen, &s_ok)) return;
 
@@ -310,7 +336,7 @@ __global__ void __launch_bounds__(HT, 1)
     tk_prev = tk;
     alph_prev = alph;
   }
-  if (blockIdx.x == 0 && tid == 0) {
+  if (bid == 0 && tid == 0) {
     if (n == 1) {
       d[0] = __ldcg(&A[0]).x;
     } else {
@@ -796,11 +822,99 @@ GemmOperand op(const void* p, int64_t s_outer, int64_t s_k, int conj) {
 }
 }  // namespace
 
+// Cooperative launch of the reduction over the matrices of tab (n > NMAX_C):
+// one CTA per SM, the SMs shared out in proportion to each matrix's n^2.
+static int launch_hetrd(reno_ctx* ctx, HetrdTable& tab, int nmax, const char* what) {
+  static std::atomic<unsigned long long> hetrd_set{0};
+  int rc = check_cuda(ctx, smem_optin_once(hetrd_kernel, 3 * MAX_N * 16, hetrd_set),
+                      (std::string(what) + ": hetrd smem attribute").c_str());
+  if (rc != RENO_OK) return rc;
+  const size_t smem = 3 * (size_t)nmax * sizeof(double2);
+  int per_sm = 0;
+  rc = check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_kernel, HT, smem),
+                  (std::string(what) + ": occupancy").c_str());
+  if (rc != RENO_OK) return rc;
+  if (per_sm < 1) return set_error(ctx, RENO_ERR_INVALID, std::string(what) + ": hetrd kernel does not fit on an SM");
+  const int G = std::min(sm_count_current_device(), 1024);
+  if (tab.count > G) return set_error(ctx, RENO_ERR_INVALID, std::string(what) + ": more matrices than SMs");
+  double work = 0.0;
+  for (int i = 0; i < tab.count; ++i) work += (double)tab.p[i].n * tab.p[i].n;
+  int used = 0;
+  for (int i = 0; i < tab.count; ++i) {
+    const int left = tab.count - 1 - i;  // at least one CTA for every later matrix
+    int nb = i == tab.count - 1 ? G - used
+                                : (int)std::lround(G * (double)tab.p[i].n * tab.p[i].n / std::max(work, 1.0));
+    nb = std::max(1, std::min(nb, G - used - left));
+    tab.p[i].first = used;
+    tab.p[i].nblk = nb;
+    used += nb;
+  }
+  void* args[] = {&tab};
+  count_launch();
+  return check_cuda(ctx, cudaLaunchCooperativeKernel((void*)hetrd_kernel, dim3(used), dim3(HT), args, smem,
+                                                     ctx->stream),
+                    (std::string(what) + ": hetrd launch").c_str());
+}
+
 extern "C" int reno_heev_workspace_bytes(int32_t n, int32_t kt, size_t* bytes) {
   if (!bytes || n < 1 || n > MAX_N || kt < 1 || kt > n) return RENO_ERR_INVALID;
   *bytes = heev_layout(n, kt).total;
   return RENO_OK;
 }
+
+namespace {
+
+int heev_attrs(reno_ctx* ctx) {
+  static std::atomic<unsigned long long> bisect_set{0}, inviter_set{0}, cluster_set{0};
+  int rc = check_cuda(ctx, smem_optin_once(bisect_kernel, 2 * MAX_N * (int)sizeof(double), bisect_set),
+                      "reno_heev_top: bisect smem attribute");
+  if (rc == RENO_OK)
+    rc = check_cuda(ctx, smem_optin_once(inviter_kernel, 2 * MAX_N * (int)sizeof(double), inviter_set),
+                    "reno_heev_top: inverse iteration smem attribute");
+  if (rc == RENO_OK)
+    rc = check_cuda(ctx, smem_optin_once(hetrd_cluster_kernel, (int)cluster_smem_bytes(NMAX_C), cluster_set),
+                    "reno_heev_top: cluster smem attribute");
+  return rc;
+}
+
+// tridiagonal reduction of a small matrix (n <= NMAX_C): one thread-block cluster
+int heev_reduce_small(reno_ctx* ctx, int n, void* A, double* d, double* e, void* tau) {
+  count_launch();
+  hetrd_cluster_kernel<<<dim3(CL, 1), CT, cluster_smem_bytes(n), ctx->stream>>>(
+      static_cast<const double2*>(A), static_cast<double2*>(A), n, d, e, static_cast<double2*>(tau));
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: cluster hetrd");
+  return RENO_OK;
+}
+
+// eigenvalues n-kt .. n-1 of T (ascending) and their inverse-iteration vectors
+int heev_eig(reno_ctx* ctx, int n, int kt, const double* d, const double* e, double* w, double* Z, double* bnd,
+             double* scr) {
+  cudaStream_t st = ctx->stream;
+  count_launch();
+  bounds_kernel<<<1, THREADS, 0, st>>>(d, e, n, bnd);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bounds");
+  count_launch();
+  bisect_kernel<<<(unsigned)ceil_div(kt, WARPS), THREADS, 2 * (size_t)n * sizeof(double), st>>>(d, e, n, n - kt, kt,
+                                                                                                 bnd, w);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bisect");
+  count_launch();
+  inviter_kernel<<<(unsigned)ceil_div(kt, IV_THREADS), IV_THREADS, 2 * (size_t)n * sizeof(double), st>>>(
+      d, e, n, kt, w, bnd, Z, scr);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: inverse iteration");
+  return RENO_OK;
+}
+
+bool heev_problem_ok(const reno_heev_problem& p) {
+  return p.n >= 1 && p.n <= MAX_N && p.kt >= 1 && p.kt <= p.n && p.a && p.d && p.e && p.tau && p.w && p.z;
+}
+
+size_t batched_offset(int32_t count, const reno_heev_problem* probs, int upto) {
+  size_t off = 0;
+  for (int i = 0; i < upto && i < count; ++i) off += align256(heev_layout(probs[i].n, probs[i].kt).total);
+  return off;
+}
+
+}  // namespace
 
 // The reflector rows of v are written in place of the upper triangle of A,
 // so A must be a private copy of G.
@@ -818,60 +932,80 @@ extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, doub
   double2* P = reinterpret_cast<double2*>(base + L.p);
   double* bnd = reinterpret_cast<double*>(base + L.bnd);
   double* scr = reinterpret_cast<double*>(base + L.scr);
-  cudaStream_t st = ctx->stream;
-  int rc = check_cuda(ctx, cudaMemsetAsync(sync, 0, sizeof(Sync), st), "reno_heev_top: memset");
-  if (rc != RENO_OK) return rc;
-  static std::atomic<unsigned long long> hetrd_set{0}, bisect_set{0}, inviter_set{0};
-  rc = check_cuda(ctx, smem_optin_once(hetrd_kernel, 3 * MAX_N * 16, hetrd_set), "reno_heev_top: hetrd smem attribute");
-  if (rc == RENO_OK)
-    rc = check_cuda(ctx, smem_optin_once(bisect_kernel, 2 * MAX_N * (int)sizeof(double), bisect_set),
-                    "reno_heev_top: bisect smem attribute");
-  if (rc == RENO_OK)
-    rc = check_cuda(ctx, smem_optin_once(inviter_kernel, 2 * MAX_N * (int)sizeof(double), inviter_set),
-                    "reno_heev_top: inverse iteration smem attribute");
+  int rc = check_cuda(ctx, cudaMemsetAsync(sync, 0, sizeof(Sync), ctx->stream), "reno_heev_top: memset");
+  if (rc == RENO_OK) rc = heev_attrs(ctx);
   if (rc != RENO_OK) return rc;
   if (n <= NMAX_C) {
-    // 1. tridiagonal reduction of a small matrix: one thread-block cluster
-    static std::atomic<unsigned long long> cluster_set{0};
-    rc = check_cuda(ctx, smem_optin_once(hetrd_cluster_kernel, (int)cluster_smem_bytes(NMAX_C), cluster_set),
-                    "reno_heev_top: cluster smem attribute");
-    if (rc != RENO_OK) return rc;
-    count_launch();
-    hetrd_cluster_kernel<<<dim3(CL, 1), CT, cluster_smem_bytes(n), st>>>(static_cast<const double2*>(A),
-                                                                         static_cast<double2*>(A), n, d, e,
-                                                                         static_cast<double2*>(tau));
-    RENO_LAUNCH_CHECK(ctx, "reno_heev_top: cluster hetrd");
+    rc = heev_reduce_small(ctx, n, A, d, e, tau);
   } else {
-  // 1. tridiagonal reduction: one CTA per SM, all co-resident (cooperative launch)
-  const size_t smem = 3 * (size_t)n * sizeof(double2);
-  int per_sm = 0;
-  rc = check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_kernel, HT, smem),
-                  "reno_heev_top: occupancy");
-  if (rc != RENO_OK) return rc;
-  if (per_sm < 1) return set_error(ctx, RENO_ERR_INVALID, "reno_heev_top: hetrd kernel does not fit on an SM");
-  unsigned grid = (unsigned)std::min(ctx->num_sms, 1024);
-  double2* Ac = static_cast<double2*>(A);
-  double2* tauc = static_cast<double2*>(tau);
-  int nn = n;
-  void* args[] = {&Ac, &nn, &d, &e, &tauc, &Y, &P, &sync};
-  count_launch();
-  rc = check_cuda(ctx, cudaLaunchCooperativeKernel((void*)hetrd_kernel, dim3(grid), dim3(HT), args, smem, st),
-                  "reno_heev_top: hetrd launch");
-  if (rc != RENO_OK) return rc;
+    HetrdTable tab{};
+    tab.count = 1;
+    tab.p[0] = HetrdProb{static_cast<double2*>(A), n, d, e, static_cast<double2*>(tau), Y, P, sync, 0, 0};
+    rc = launch_hetrd(ctx, tab, n, "reno_heev_top");
   }
-  // 2. eigenvalues n-kt .. n-1 (ascending)
-  count_launch();
-  bounds_kernel<<<1, THREADS, 0, st>>>(d, e, n, bnd);
-  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bounds");
-  count_launch();
-  bisect_kernel<<<(unsigned)ceil_div(kt, WARPS), THREADS, 2 * (size_t)n * sizeof(double), st>>>(d, e, n, n - kt, kt,
-                                                                                                 bnd, w);
-  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bisect");
-  // 3. eigenvectors of T
-  count_launch();
-  inviter_kernel<<<(unsigned)ceil_div(kt, IV_THREADS), IV_THREADS, 2 * (size_t)n * sizeof(double), st>>>(
-      d, e, n, kt, w, bnd, Z, scr);
-  RENO_LAUNCH_CHECK(ctx, "reno_heev_top: inverse iteration");
+  if (rc != RENO_OK) return rc;
+  return heev_eig(ctx, n, kt, d, e, w, Z, bnd, scr);
+}
+
+extern "C" int reno_heev_batched_workspace_bytes(int32_t count, const reno_heev_problem* probs, size_t* bytes) {
+  if (!bytes || !probs || count < 1 || count > RENO_HEEV_MAX_BATCH) return RENO_ERR_INVALID;
+  for (int i = 0; i < count; ++i)
+    if (probs[i].n < 1 || probs[i].n > MAX_N || probs[i].kt < 1 || probs[i].kt > probs[i].n) return RENO_ERR_INVALID;
+  *bytes = batched_offset(count, probs, count);
+  return RENO_OK;
+}
+
+// reno_heev_top for several matrices: the matrices larger than the cluster
+// path share one cooperative reduction launch (the grid split among them),
+// so the QN blocks of one bond are reduced side by side.
+extern "C" int reno_heev_top_batched(reno_ctx* ctx, int32_t count, const reno_heev_problem* probs, int32_t* status,
+                                     void* ws, size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (!probs || !status || !ws || count < 1 || count > RENO_HEEV_MAX_BATCH)
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heev_top_batched: invalid batch");
+  for (int i = 0; i < count; ++i)
+    if (!heev_problem_ok(probs[i]))
+      return set_error(ctx, RENO_ERR_INVALID, "reno_heev_top_batched: problem " + std::to_string(i) +
+                                                  " needs 1 <= kt <= n <= 4096 and non-null pointers");
+  if (ws_bytes < batched_offset(count, probs, count))
+    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heev_top_batched: workspace too small");
+  int rc = heev_attrs(ctx);
+  if (rc != RENO_OK) return rc;
+  HetrdTable tab{};
+  int nmax = 0;
+  for (int i = 0; i < count; ++i) {
+    const reno_heev_problem& p = probs[i];
+    char* base = static_cast<char*>(ws) + batched_offset(count, probs, i);
+    const HeevLayout L = heev_layout(p.n, p.kt);
+    Sync* sync = reinterpret_cast<Sync*>(base + L.sync);
+    rc = check_cuda(ctx, cudaMemsetAsync(sync, 0, sizeof(Sync), ctx->stream), "reno_heev_top_batched: memset");
+    if (rc != RENO_OK) return rc;
+    if (p.n <= NMAX_C) {
+      rc = heev_reduce_small(ctx, p.n, p.a, p.d, p.e, p.tau);
+      if (rc != RENO_OK) return rc;
+    } else {
+      tab.p[tab.count++] = HetrdProb{static_cast<double2*>(p.a), p.n, p.d, p.e, static_cast<double2*>(p.tau),
+                                     reinterpret_cast<double2*>(base + L.y), reinterpret_cast<double2*>(base + L.p),
+                                     sync, 0, 0};
+      nmax = std::max(nmax, (int)p.n);
+    }
+  }
+  if (tab.count) {
+    rc = launch_hetrd(ctx, tab, nmax, "reno_heev_top_batched");
+    if (rc != RENO_OK) return rc;
+  }
+  for (int i = 0; i < count; ++i) {
+    const reno_heev_problem& p = probs[i];
+    char* base = static_cast<char*>(ws) + batched_offset(count, probs, i);
+    const HeevLayout L = heev_layout(p.n, p.kt);
+    rc = heev_eig(ctx, p.n, p.kt, p.d, p.e, p.w, p.z, reinterpret_cast<double*>(base + L.bnd),
+                  reinterpret_cast<double*>(base + L.scr));
+    if (rc == RENO_OK)
+      rc = check_cuda(ctx, cudaMemcpyAsync(status + i, base + L.sync + offsetof(Sync, status), sizeof(int32_t),
+                                           cudaMemcpyDeviceToDevice, ctx->stream),
+                      "reno_heev_top_batched: status");
+    if (rc != RENO_OK) return rc;
+  }
   return RENO_OK;
 }
 
@@ -1019,5 +1153,25 @@ extern "C" int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, voi
 extern "C" int reno_heev_status_offset(size_t* offset) {
   if (!offset) return RENO_ERR_INVALID;
   *offset = offsetof(Sync, status);
+  return RENO_OK;
+}
+
+// reno_heev_backtransform for every problem of a reno_heev_top_batched call
+// (same problems and workspace): K_i <- Q_i K_i.
+extern "C" int reno_heev_backtransform_batched(reno_ctx* ctx, int32_t count, const reno_heev_problem* probs,
+                                               void* ws, size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (!probs || !ws || count < 1 || count > RENO_HEEV_MAX_BATCH)
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform_batched: invalid batch");
+  if (ws_bytes < batched_offset(count, probs, count))
+    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heev_backtransform_batched: workspace too small");
+  for (int i = 0; i < count; ++i) {
+    const reno_heev_problem& p = probs[i];
+    if (!p.k) return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform_batched: null K");
+    const size_t off = batched_offset(count, probs, i);
+    const int rc = reno_heev_backtransform(ctx, p.n, p.kt, p.a, p.tau, p.k, static_cast<char*>(ws) + off,
+                                           heev_layout(p.n, p.kt).total);
+    if (rc != RENO_OK) return rc;
+  }
   return RENO_OK;
 }

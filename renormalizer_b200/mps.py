@@ -507,7 +507,9 @@ class Mps:
                     self.qn[c0 + 1] = res.qn
                     self.qnidx = c0 + 1
                 else:
-                    self._mp[c0] = (lmat.reshape(-1, res.mdim) @ res.right).reshape(self._mp[c0].shape[:-1] + (-1,))
+                    eng = Engine.get(res.right.device)
+                    self._mp[c0] = eng.matmul(lmat.reshape(-1, res.mdim).contiguous(), res.right).reshape(
+                        self._mp[c0].shape[:-1] + (-1,))
                     self.qnidx = n - 1
             else:
                 self._mp[c0] = rmat.to(self.dtype)
@@ -516,7 +518,9 @@ class Mps:
                     self.qn[c0] = res.qn
                     self.qnidx = c0 - 1
                 else:
-                    self._mp[c0] = (res.left @ rmat.reshape(res.mdim, -1)).reshape((-1,) + tuple(rmat.shape[1:]))
+                    eng = Engine.get(res.left.device)
+                    self._mp[c0] = eng.matmul(res.left, rmat.reshape(res.mdim, -1).contiguous()).reshape(
+                        (-1,) + tuple(rmat.shape[1:]))
                     self.qnidx = 0
         else:
             self._mp[cidx[0]] = lmat.to(self.dtype).contiguous()

@@ -10,11 +10,14 @@ thousand numbers -- come to the host, where the truncation rule and the
 selection order are decided exactly as in the reference (stable descending
 sort of sigma, zero-sigma padding columns last, ``percent`` per QN block).
 
-The dense per-block factorisations are cuSOLVER routines (through
-torch.linalg); padding columns (the reference's full_matrices=True
-completion, svd_qn.py:43-63) are an orthonormal completion drawn from numpy's
-global RNG like the reference, and are built only when the selection reaches
-them.
+The dense per-block factorisations run in libreno_b200: the truncation
+diagonalises each block's Gram matrix with the device eigensolver (heev.py;
+cuSOLVER only redoes a block whose checks fail) and the QR of svd_qn(QR=True)
+is the batched Householder QR (reno_qr_blocks).  Padding columns (the
+reference's full_matrices=True completion, svd_qn.py:43-63) are an
+orthonormal completion drawn from numpy's global RNG like the reference, and
+are built only when the selection reaches them.  The stand-alone SVD of
+svd_qn(QR=False) (not used by the sweeps) is torch.linalg.svd.
 """
 from __future__ import annotations
 
@@ -124,12 +127,16 @@ def qn_block_svd(coef: torch.Tensor, qnbigl, qnbigr, qntot, full_matrices=True, 
 
 
 def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
-    """Per-block QR (system "L") or RQ (system "R"), economic (svd_qn.py:195-204).
-    RQ comes from the Householder QR of the reversed conjugate transpose:
-    (J A J)^H = Q1 R1 gives A = (J R1^H J)(J Q1^H J), with J R1^H J upper
-    triangular.  Householder QR processes the entries in the same order as
-    LAPACK's RQ (last row first, pivot on its last entry), so R and Q agree
-    with scipy.linalg.rq including the signs, not only up to a rotation."""
+    """Per-block QR (system "L") or RQ (system "R"), economic (svd_qn.py:195-204),
+    every QN block of the site in one batched Householder QR (reno_qr_blocks,
+    LAPACK's sign conventions).  RQ comes from the QR of the reversed
+    conjugate transpose: (J A J)^H = Q1 R1 gives A = (J R1^H J)(J Q1^H J), with
+    J R1^H J upper triangular.  Householder QR processes the entries in the
+    same order as LAPACK's RQ (last row first, pivot on its last entry), so R
+    and Q agree with scipy.linalg.rq including the signs, not only up to a
+    rotation."""
+    if system not in ("L", "R"):
+        raise AssertionError("system must be L or R for QR")
     eng = Engine.get(coef.device)
     rows = int(np.prod(qnbigl.shape[:-1]))
     cols = int(np.prod(qnbigr.shape[:-1]))
@@ -138,7 +145,7 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
     qs = len(qntot)
     lq = qnbigl.reshape(-1, qs)
     rq = qnbigr.reshape(-1, qs)
-    blocks = []
+    found = []
     for nl in qn_sectors(lq):
         nr = tuple(qntot - np.array(nl))
         rset = np.where(get_qn_mask(rq, nr))[0]
@@ -146,17 +153,19 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
             continue
         lset = np.where(get_qn_mask(lq, nl))[0]
         blk = _gather(eng, mat, lset, rset)
-        if system == "L":
-            Q, R = torch.linalg.qr(blk, mode="reduced")
-            blocks.append(QNBlock(nl, nr, lset, rset, Q, None, None, R))
-        elif system == "R":
-            Q1, R1 = torch.linalg.qr(blk.flip([0, 1]).mH, mode="reduced")
-            blocks.append(QNBlock(nl, nr, lset, rset, R1.mH.flip([0, 1]).resolve_conj().contiguous(), None, None,
-                                  Q1.mH.flip([0, 1]).resolve_conj().contiguous()))
-        else:
-            raise AssertionError("system must be L or R for QR")
-    if not blocks:
+        if system == "R":
+            blk = blk.flip([0, 1]).mH.resolve_conj().contiguous()
+        found.append((nl, nr, lset, rset, blk))
+    if not found:
         raise ValueError("Invalid quantum number")
+    Qs, Rs = eng.qr_blocks([f[4] for f in found])
+    blocks = []
+    for (nl, nr, lset, rset, _), Q, R in zip(found, Qs, Rs):
+        if system == "L":
+            blocks.append(QNBlock(nl, nr, lset, rset, Q, None, None, R))
+        else:
+            blocks.append(QNBlock(nl, nr, lset, rset, R.mH.flip([0, 1]).resolve_conj().contiguous(), None, None,
+                                  Q.mH.flip([0, 1]).resolve_conj().contiguous()))
     return blocks, rows, cols
 
 
@@ -219,13 +228,16 @@ def _completion(vecs: torch.Tensor, npad: int) -> torch.Tensor:
     """npad orthonormal columns orthogonal to the columns of vecs (m x k),
     drawn like svd_qn.py:52-63 from numpy's global RNG."""
     m, k = vecs.shape
+    eng = Engine.get(vecs.device)
+    vecs = vecs.contiguous()
     a = torch.as_tensor(np.random.rand(m, npad), device=vecs.device).to(vecs.dtype)
-    a = a - vecs @ (vecs.mH @ a)
-    q, _ = torch.linalg.qr(a, mode="reduced")
+
+    def project_out(x):
+        return x - eng.matmul(vecs, eng.matmul(vecs.transpose(0, 1), x, conj_a=True))
+
+    q = eng.qr_blocks([project_out(a)])[0][0]
     # second pass for orthogonality to vecs at FP64 rounding level
-    q = q - vecs @ (vecs.mH @ q)
-    q, _ = torch.linalg.qr(q, mode="reduced")
-    return q
+    return eng.qr_blocks([project_out(q)])[0][0]
 
 
 class TruncatedSplit:
@@ -309,7 +321,7 @@ def _omega(rows, kk, dtype, device):
 def _orthonormalise(eng: Engine, Y: torch.Tensor, method: str) -> torch.Tensor:
     """An orthonormal basis of the columns of Y (r x kk, r >= kk).
 
-    "householder": torch.linalg.qr.  "cholqr": shifted CholeskyQR3 (Fukaya,
+    "householder": the engine's Householder QR.  "cholqr": shifted CholeskyQR3 (Fukaya,
     Kannan, Nakatsukasa, Yamamoto, Yanagisawa, SIAM J. Sci. Comput. 2020): one
     Cholesky QR of the Gram matrix shifted by 11 (r kk + kk (kk + 1)) u tr(G),
     which keeps it positive definite for any column rank, then two plain
@@ -317,7 +329,7 @@ def _orthonormalise(eng: Engine, Y: torch.Tensor, method: str) -> torch.Tensor:
     kk x kk Gram GEMMs, Cholesky factorisations and triangular solves, with no
     host synchronisation."""
     if method == "householder":
-        return torch.linalg.qr(Y, mode="reduced")[0]
+        return eng.qr_blocks([Y.contiguous()])[0][0]
     r, kk = Y.shape
     u = np.finfo(np.float64).eps / 2
     for shifted in (True, False, False):
@@ -384,10 +396,102 @@ def _gram_eigh(eng: Engine, G: torch.Tensor, kt: int, use_heev: bool):
     return torch.flip(w, dims=[0]), torch.flip(V, dims=[1]), None
 
 
+def _gram_of(eng: Engine, X: torch.Tensor, keep_left: bool):
+    """(G, left) with G the Gram matrix of X's smaller side, X X^H (left) or
+    X^H X; a square block takes the kept side."""
+    m, n = X.shape
+    if m < n or (m == n and keep_left):
+        return eng.matmul(X, X.transpose(0, 1), conj_b=True), True
+    return eng.matmul(X.transpose(0, 1), X, conj_a=True), False
+
+
+def _finish_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, kt: int, w, E, chk, qr_out=None):
+    """Kept-side basis K, projection P and sigma S of block X from the
+    leading kt eigenvectors E of its smaller-side Gram matrix (w descending):
+    see _full_kept_side.  When the kept side is the larger one, the projected
+    vectors are orthonormalised by Householder QR; ``qr_out`` carries that QR
+    (computed for all blocks at once) and is None on the first pass, which
+    returns the matrix to factorise instead."""
+    m, n = X.shape
+    dim = min(m, n)
+
+    def tail(w_desc, head):
+        # only the leading kt eigenvalues may be known: the others then read
+        # as 0, which the cap below reaches anyway
+        t = torch.sqrt(torch.clamp(w_desc[kt:dim], min=0.0)) if w_desc.numel() >= dim else \
+            torch.zeros(dim - kt, dtype=torch.float64, device=head.device)
+        return torch.minimum(t, head.min()) if kt < dim and head.numel() else t
+
+    if keep_left and m <= n:
+        K = E[:, :kt]
+        P = eng.matmul(K.transpose(0, 1).contiguous(), X, conj_a=True)       # (kt, n) = sigma Vh
+        S = torch.linalg.vector_norm(P, dim=1)
+        return dict(K=K, P=P, S=torch.cat([S, tail(w, S)]), dim=dim, chk=chk)
+    if not keep_left and n <= m:
+        K = E[:, :kt]
+        P = eng.matmul(X, K.contiguous())                                     # (m, kt) = U sigma
+        S = torch.linalg.vector_norm(P, dim=0)
+        return dict(K=K, P=P, S=torch.cat([S, tail(w, S)]), dim=dim, chk=chk)
+    if keep_left:
+        Us = eng.matmul(X, E[:, :kt].contiguous())                            # (m, kt) = U sigma
+        if qr_out is None:
+            return dict(need_qr=Us)
+        S = torch.linalg.vector_norm(Us, dim=0)
+        K = qr_out
+        P = eng.matmul(K.transpose(0, 1).contiguous(), X, conj_a=True)
+        return dict(K=K, P=P, S=torch.cat([S, tail(w, S)]), dim=dim, chk=chk)
+    Vs = eng.matmul(X.transpose(0, 1), E[:, :kt].contiguous(), conj_a=True)   # (n, kt): sigma v
+    if qr_out is None:
+        return dict(need_qr=Vs)
+    S = torch.linalg.vector_norm(Vs, dim=0)
+    K = qr_out
+    P = eng.matmul(X, K)
+    return dict(K=K, P=P, S=torch.cat([S, tail(w, S)]), dim=dim, chk=chk)
+
+
+def _device_eig_ok(G: torch.Tensor) -> bool:
+    """whether the device eigensolver takes Gram block G (size 1 .. 4096)"""
+    n = G.shape[0]
+    return heev.heev_opts.enabled and G.is_cuda and heev.heev_opts.min_n <= n <= 4096
+
+
+def _kept_sides(eng: Engine, Xs, keep_left: bool, ktops, use_heev: bool = True) -> list:
+    """_full_kept_side for all QN blocks of one truncation: one Gram matrix
+    per block, the device eigensolver on all of them at once
+    (heev_top_batched; blocks above its size limit, or with the device
+    eigensolver switched off, take cuSOLVER), and one batched Householder QR
+    where a projected basis needs orthonormalising."""
+    items = []
+    for X, ktop in zip(Xs, ktops):
+        m, n = X.shape
+        dim = min(m, n)
+        kt = dim if ktop is None else min(int(ktop), dim)
+        G, _ = _gram_of(eng, X, keep_left)
+        items.append(dict(X=X, G=G, kt=kt, dim=dim))
+    dev_idx = [i for i, it in enumerate(items) if use_heev and _device_eig_ok(it["G"])]
+    if dev_idx:
+        res = heev.heev_top_batched(eng, [items[i]["G"] for i in dev_idx], [items[i]["kt"] for i in dev_idx])
+        for i, (w, K, chk) in zip(dev_idx, res):
+            items[i].update(w=w, E=K if items[i]["G"].is_complex() else K.real.contiguous(), chk=chk)
+    for it in items:
+        if "E" not in it:
+            w, V = torch.linalg.eigh(it["G"])
+            it.update(w=torch.flip(w, dims=[0]), E=torch.flip(V, dims=[1]), chk=None)
+    outs = [_finish_kept_side(eng, it["X"], keep_left, it["kt"], it["w"], it["E"], it["chk"]) for it in items]
+    need = [i for i, o in enumerate(outs) if "need_qr" in o]
+    if need:
+        Qs, _ = eng.qr_blocks([outs[i]["need_qr"] for i in need])
+        for i, Q in zip(need, Qs):
+            it = items[i]
+            outs[i] = _finish_kept_side(eng, it["X"], keep_left, it["kt"], it["w"], it["E"], it["chk"], Q)
+    return outs
+
+
 def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optional[int] = None,
                     use_heev: bool = True) -> dict:
-    """Kept-side basis K, projection P and sigma S of one block from the full
-    Gram eigendecomposition of its smaller side (all min(m, n) triplets).
+    """Kept-side basis K, projection P and sigma S of one block from the
+    Hermitian eigendecomposition of the Gram matrix of its smaller side (all
+    min(m, n) triplets).
 
     With ``ktop`` < min(m, n) (a fixed cap on the kept dimension is known and
     the block is larger) only the leading ktop singular vectors are projected:
@@ -400,46 +504,7 @@ def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optiona
     entry sorts after every head entry of its block, and since a block
     contributes at most the cap (< ktop) entries, none is selected; they only
     fill the list the truncation rule reads."""
-    m, n = X.shape
-    dim = min(m, n)
-    kt = dim if ktop is None else min(int(ktop), dim)
-
-    def tail(w_desc, head):
-        # the device eigensolver returns only the leading kt eigenvalues: the
-        # others then read as 0, which the cap below reaches anyway
-        t = torch.sqrt(torch.clamp(w_desc[kt:dim], min=0.0)) if w_desc.numel() >= dim else \
-            torch.zeros(dim - kt, dtype=torch.float64, device=head.device)
-        return torch.minimum(t, head.min()) if kt < dim and head.numel() else t
-
-    if keep_left and m <= n:
-        G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-        w, K, chk = _gram_eigh(eng, G, kt, use_heev)
-        P = eng.matmul(K[:, :kt].transpose(0, 1), X, conj_a=True)           # (kt, n) = sigma Vh
-        S = torch.linalg.vector_norm(P, dim=1)
-        S = torch.cat([S, tail(w, S)])
-    elif keep_left:
-        G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-        w, V, chk = _gram_eigh(eng, G, kt, use_heev)
-        Us = eng.matmul(X, V[:, :kt])                                        # (m, kt) = U sigma
-        S = torch.linalg.vector_norm(Us, dim=0)
-        S = torch.cat([S, tail(w, S)])
-        K, _ = torch.linalg.qr(Us, mode="reduced")
-        P = eng.matmul(K.transpose(0, 1), X, conj_a=True)
-    elif n <= m:
-        G = eng.matmul(X.transpose(0, 1), X, conj_a=True)
-        w, K, chk = _gram_eigh(eng, G, kt, use_heev)
-        P = eng.matmul(X, K[:, :kt])                                         # (m, kt) = U sigma
-        S = torch.linalg.vector_norm(P, dim=0)
-        S = torch.cat([S, tail(w, S)])
-    else:
-        G = eng.matmul(X, X.transpose(0, 1), conj_b=True)
-        w, U, chk = _gram_eigh(eng, G, kt, use_heev)
-        Vs = eng.matmul(X.transpose(0, 1), U[:, :kt], conj_a=True)           # (n, kt): sigma v
-        S = torch.linalg.vector_norm(Vs, dim=0)
-        S = torch.cat([S, tail(w, S)])
-        K, _ = torch.linalg.qr(Vs, mode="reduced")
-        P = eng.matmul(X, K)
-    return dict(K=K, P=P, S=S, dim=dim, chk=chk)
+    return _kept_sides(eng, [X], keep_left, [ktop], use_heev)[0]
 
 
 def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_trunc_fn, percent=0,
@@ -469,6 +534,7 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
     lq = qnbigl.reshape(-1, qs)
     rq = qnbigr.reshape(-1, qs)
     blocks = []
+    pending = []
     for nl in qn_sectors(lq):
         nr = tuple(qntot - np.array(nl))
         rset = np.where(get_qn_mask(rq, nr))[0]
@@ -480,22 +546,26 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         dim = min(m, n)
         upad, vpad = _pad_counts(m, n, full_matrices)
         ksub = min(kcap, dim) if kcap is not None else 0
+        npad = upad if keep_left else vpad
         if (subspace.min_dim and kcap is not None and dim >= subspace.min_dim
                 and dim >= 2 * (ksub + subspace.oversample)):
             subspace.calls += 1
             K, P, S, chk, Q = _subspace_block(eng, X, keep_left, ksub, subspace)
-            npad = upad if keep_left else vpad
             blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=ksub, npad=npad, res=chk,
                                X=X, Q=Q))
             continue
         ktop = kcap + 64 if kcap is not None and kcap + 64 < dim else None
-        full = _full_kept_side(eng, X, keep_left, ktop)
-        K, P, S = full["K"], full["P"], full["S"]
-        npad = upad if keep_left else vpad
-        blk = dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=dim, npad=npad)
-        if full["chk"] is not None:
-            blk.update(chk=full["chk"], X=X, ktop=ktop)
+        blk = dict(nl=nl, nr=nr, lset=lset, rset=rset, dim=dim, npad=npad, X=X, ktop=ktop)
         blocks.append(blk)
+        pending.append(blk)
+    if pending:
+        fulls = _kept_sides(eng, [b["X"] for b in pending], keep_left, [b["ktop"] for b in pending])
+        for b, full in zip(pending, fulls):
+            b.update(K=full["K"], P=full["P"], S=full["S"])
+            if full["chk"] is not None:
+                b["chk"] = full["chk"]
+            else:
+                b.pop("X")
     if not blocks:
         raise ValueError("Invalid quantum number")
     sub = [b for b in blocks if "res" in b]

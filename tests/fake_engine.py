@@ -90,6 +90,10 @@ class FakeEngine:
             b = b.conj()
         return (a @ b).resolve_conj().contiguous()
 
+    def qr_blocks(self, mats):
+        out = [torch.linalg.qr(a, mode="reduced") for a in mats]
+        return [q.contiguous() for q, _ in out], [r.contiguous() for _, r in out]
+
     # ------------------------------------------------------------ vectors
     def vec_norm(self, x, out):
         out[0] = torch.linalg.vector_norm(x)

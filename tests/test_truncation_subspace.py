@@ -172,16 +172,18 @@ def test_device_eigensolver_fallback_host_logic(cpu_engine, monkeypatch):
     full = svd_qn.svd_truncate(coef, ql, qr, np.array([1]), True, lambda s: min(kcap, len(s)), kcap=kcap)
     calls = []
 
-    def fake_gram_eigh(eng, G, kt, use_heev):
-        w, V = torch.linalg.eigh(G)
-        w, V = torch.flip(w, dims=[0]), torch.flip(V, dims=[1])
-        if not use_heev:
-            return w, V, None
-        calls.append(kt)
-        bad = 1.0 if len(calls) == 1 else 0.0
-        return w[:kt], V[:, :kt], torch.tensor([0.0, bad, 0.0], dtype=torch.float64)
+    def fake_heev_top_batched(eng, Gs, kts):
+        out = []
+        for G, kt in zip(Gs, kts):
+            w, V = torch.linalg.eigh(G)
+            w, V = torch.flip(w, dims=[0]), torch.flip(V, dims=[1])
+            calls.append(kt)
+            bad = 1.0 if len(calls) == 1 else 0.0
+            out.append((w[:kt], V[:, :kt], torch.tensor([0.0, bad, 0.0], dtype=torch.float64)))
+        return out
 
-    monkeypatch.setattr(svd_qn, "_gram_eigh", fake_gram_eigh)
+    monkeypatch.setattr(svd_qn, "_device_eig_ok", lambda G: True)
+    monkeypatch.setattr(heev, "heev_top_batched", fake_heev_top_batched)
     f0 = heev.heev_opts.fallbacks
     got = svd_qn.svd_truncate(coef, ql, qr, np.array([1]), True, lambda s: min(kcap, len(s)), kcap=kcap)
     assert len(calls) == 2 and heev.heev_opts.fallbacks == f0 + 1
