@@ -41,8 +41,12 @@ class FakeEngine:
         elif d.nsite == 1:
             r = torch.einsum("abc,bdef,lfk,cek->adl", L.to(y.dtype), W1.to(y.dtype), R.to(y.dtype), psi.to(y.dtype))
         else:
-            r = torch.einsum("abc,bdef,fghj,ljk,cehk->adgl", L.to(y.dtype), W1.to(y.dtype), W2.to(y.dtype),
-                             R.to(y.dtype), psi.to(y.dtype))
+            # pairwise, in the reference's contraction order (a single 5-operand
+            # einsum would build an M^2 d^2 w^2-sized intermediate)
+            t = torch.einsum("abc,cehk->abehk", L.to(y.dtype), psi.to(y.dtype))
+            t = torch.einsum("abehk,bdef->adfhk", t, W1.to(y.dtype))
+            t = torch.einsum("adfhk,fghj->adgjk", t, W2.to(y.dtype))
+            r = torch.einsum("adgjk,ljk->adgl", t, R.to(y.dtype))
         y.copy_(r)
 
     def heff_apply_grouped(self, descs, Ls, W1s, W2s, Rs, psis, ys):

@@ -320,6 +320,73 @@ def gen_tdvp(out):
     np.savez_compressed(out / "tdvp_cases.npz", **cases)
 
 
+def _config_run(model, method, dt, nsteps, mmax, d, prefix, dump_init=True):
+    """Hartree product (exciton on the first site) expanded with the MPO hint
+    (expand_bond_dimension(mpo, include_ex=False), the configs' idiom), then
+    nsteps of `method`; populations after every step under prefix."""
+    from renormalizer.mps import Mps, Mpo
+    from renormalizer.utils import EvolveConfig, CompressConfig, CompressCriteria
+    np.random.seed(2024)
+    mpo = Mpo(model)
+    init = Mps.hartree_product_state(model, {0: 1})
+    init.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=mmax)
+    init = init.expand_bond_dimension(mpo, include_ex=False)
+    mps = init.copy()
+    mps.evolve_config = EvolveConfig(method)
+    mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=mmax)
+    if dump_init:
+        _dump_mps(f"{prefix}/init", mps, d)
+        _dump_mpo(f"{prefix}/mpo", mpo, d)
+    pops = [np.asarray(mps.e_occupations)]
+    for _ in range(nsteps):
+        mps = mps.evolve(mpo, dt)
+        pops.append(np.asarray(mps.e_occupations))
+    d[f"{prefix}/pops"] = np.array(pops)
+    d[f"{prefix}/dt"] = np.array(dt)
+    d[f"{prefix}/mmax"] = np.array(mmax)
+    d[f"{prefix}/bond_dims_final"] = np.array(mps.bond_dims)
+
+
+def _c1_model():
+    # config 1: 10 molecules, one mode (omega = 1, g = 1), 10 levels, J = 1
+    return _holstein(10, 10, [(1.0, 1.0)])
+
+
+def gen_c1_traj(threads, path):
+    """one config-1 trajectory in this process (BLAS threads set by the caller)"""
+    from renormalizer.utils import EvolveMethod
+    d = {}
+    _config_run(_c1_model(), EvolveMethod.tdvp_ps, 0.05, 100, 32, d, "c1", dump_init=True)
+    np.savez(path, **d)
+
+
+def gen_configs(out):
+    """Config 1 exactly (10-molecule Holstein chain, one mode with omega = 1,
+    g = 1 and 10 levels; hint-expanded Hartree start at M = 32; 100 steps of
+    one-site TDVP-PS at dt = 0.05), run twice by the reference with 1 and 4
+    BLAS threads -- the second run is the reference's own rounding envelope --
+    and a reduced config 2 (4 molecules, two modes omega = 1 / 0.5, g = 1 /
+    0.7, 16 levels, M = 32, ten steps of two-site TDVP-PS at dt = 0.025)."""
+    import subprocess
+    import tempfile
+    from renormalizer.utils import EvolveMethod
+    cases = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        runs = {}
+        for t in (1, 4):
+            path = Path(tmp) / f"c1_t{t}.npz"
+            env = dict(os.environ, OPENBLAS_NUM_THREADS=str(t), OMP_NUM_THREADS=str(t), MKL_NUM_THREADS=str(t),
+                       RENO_NUM_THREADS=str(t))
+            subprocess.run([sys.executable, str(Path(__file__).resolve()), "--c1-traj", str(t), str(path)],
+                           check=True, env=env)
+            runs[t] = dict(np.load(path))
+        cases.update({k: v for k, v in runs[1].items()})
+        cases["c1/pops_t4"] = runs[4]["c1/pops"]
+        cases["c1/threads"] = np.array([1, 4])
+    _config_run(_holstein(4, 16, [(1.0, 1.0), (0.5, 0.7)]), EvolveMethod.tdvp_ps2, 0.025, 10, 32, cases, "c2red")
+    np.savez_compressed(out / "config_cases.npz", **cases)
+
+
 def gen_dmrg(out):
     from renormalizer.mps import Mps, Mpo
     from renormalizer.mps.gs import optimize_mps
@@ -388,10 +455,15 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--c1-traj", nargs=2, default=None, metavar=("THREADS", "PATH"),
+                    help="internal: run one config-1 trajectory into PATH")
     args = ap.parse_args()
     _import_reference(args.reference)
+    if args.c1_traj:
+        gen_c1_traj(int(args.c1_traj[0]), args.c1_traj[1])
+        return
     gens = dict(heff=gen_heff, env=gen_env, krylov=gen_krylov, svd=gen_svd, mpo=gen_mpo, tdvp=gen_tdvp,
-                dmrg=gen_dmrg, obs=gen_obs)
+                dmrg=gen_dmrg, obs=gen_obs, configs=gen_configs)
     for name, fn in gens.items():
         if args.only and name not in args.only.split(","):
             continue
