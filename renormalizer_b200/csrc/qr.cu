@@ -445,9 +445,11 @@ extern "C" int reno_qr_blocks(reno_ctx* ctx, int32_t count, const reno_qr_block*
   }
   const int rows = (nmax + qr::QCL - 1) / qr::QCL;
   const size_t smem = ((size_t)rows * nb + 2 * qr::NBMAX + qr::NBMAX + qr::NBMAX * qr::NBMAX + qr::NBMAX) * es;
+  // the opt-in is made once per device, so it covers the largest panel any call can use
+  const int smem_max = (int)(((size_t)qr::PANEL_ELEMS + 4 * qr::NBMAX + qr::NBMAX * qr::NBMAX) * 16);
   static std::atomic<unsigned long long> set_c{0}, set_r{0};
-  cudaError_t e = cplx ? smem_optin_once(qr::qr_panel_kernel<true>, (int)smem, set_c)
-                       : smem_optin_once(qr::qr_panel_kernel<false>, (int)smem, set_r);
+  cudaError_t e = cplx ? smem_optin_once(qr::qr_panel_kernel<true>, smem_max, set_c)
+                       : smem_optin_once(qr::qr_panel_kernel<false>, smem_max, set_r);
   if (e != cudaSuccess) return check_cuda(ctx, e, "reno_qr_blocks: shared-memory opt-in");
 
   // ---- factorisation, panel by panel

@@ -53,6 +53,49 @@ def test_tdvp_ps2_matches_reference(tag):
     assert max(mps.bond_dims) <= int(TDVP[f"{tag}/mmax"])
 
 
+CFG = load_golden("config_cases.npz")
+
+
+def _config_run(tag, method, nsteps):
+    from renormalizer_b200 import CompressConfig, CompressCriteria, EvolveConfig, EvolveMethod, backend
+    backend.prec = "fp64"
+    mps, mpo = engine_chain(CFG, tag)
+    mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=int(CFG[f"{tag}/mmax"]))
+    mps.evolve_config = EvolveConfig(getattr(EvolveMethod, method))
+    dt = float(CFG[f"{tag}/dt"])
+    pops = [mps.e_occupations]
+    for _ in range(nsteps):
+        mps = mps.evolve(mpo, dt)
+        pops.append(mps.e_occupations)
+    return np.abs(np.array(pops) - CFG[f"{tag}/pops"][:nsteps + 1]).max(axis=1), mps
+
+
+def test_config1_matches_reference():
+    """Config 1 exactly: 10-molecule Holstein chain (omega = 1, g = 1, 10
+    levels), the reference's hint-expanded start at M = 32, 100 steps of
+    one-site TDVP-PS at dt = 0.05.  The first five steps agree with the
+    reference to 1e-10; after that the trajectory amplifies rounding (the
+    reference against itself at 1 vs 4 BLAS threads: 2e-12 after 5 steps,
+    5e-10 after 15, 1e-5 after 80), and the engine must stay within 100 times
+    the reference's own spread so far."""
+    dev, _ = _config_run("c1", "tdvp_ps", 100)
+    env = np.maximum.accumulate(np.abs(CFG["c1/pops"] - CFG["c1/pops_t4"]).max(axis=1))
+    assert dev[:6].max() <= 1e-10, dev[:6]
+    bound = np.maximum(100 * env, 1e-10)
+    assert np.all(dev <= bound), [(i, dev[i], env[i]) for i in np.nonzero(dev > bound)[0][:5]]
+
+
+def test_config2_reduced_matches_reference():
+    """Config 2 at reduced size: 4 molecules with two modes (omega = 1 / 0.5,
+    g = 1 / 0.7), 16 levels, M = 32, two-site TDVP-PS at dt = 0.025 from the
+    reference's hint-expanded start: 1e-10 over the first five steps, 1e-8 to
+    step 10, and the reference's final bond dimensions."""
+    dev, mps = _config_run("c2red", "tdvp_ps2", 10)
+    assert dev[:6].max() <= 1e-10, dev
+    assert dev.max() <= 1e-8, dev
+    assert list(mps.bond_dims) == list(CFG["c2red/bond_dims_final"])
+
+
 def test_tdvp_ps_energy_conserved():
     from renormalizer_b200 import EvolveConfig, EvolveMethod
     mps, mpo = engine_state("ps_hol4")

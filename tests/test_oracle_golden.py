@@ -69,15 +69,16 @@ def test_oracle_svd_qn_matches_reference():
         np.testing.assert_allclose(u @ v.T, c.reshape(u.shape[0], v.shape[0]), atol=1e-12)
 
 
-def _traj(tag, fn):
-    init = mps_from_golden(TDVP, f"{tag}/init", compress=O.Compress("fixed", max_bonddim=int(TDVP[f"{tag}/mmax"])))
-    mpo = mpo_from_golden(TDVP, f"{tag}/mpo", len(init))
-    dt = float(TDVP[f"{tag}/dt"])
+def _traj(tag, fn, src=None, nsteps=None):
+    src = TDVP if src is None else src
+    init = mps_from_golden(src, f"{tag}/init", compress=O.Compress("fixed", max_bonddim=int(src[f"{tag}/mmax"])))
+    mpo = mpo_from_golden(src, f"{tag}/mpo", len(init))
+    dt = float(src[f"{tag}/dt"])
     e_sites = [i for i, s in enumerate(init.sigmaqn) if s.shape[0] == 2 and s[1, 0] == 1]
     op = np.diag([0.0, 1.0])
     pops = [[O.site_expectations(init, {i: op for i in e_sites})[i] for i in e_sites]]
     mps = init
-    for _ in range(TDVP[f"{tag}/pops"].shape[0] - 1):
+    for _ in range(src[f"{tag}/pops"].shape[0] - 1 if nsteps is None else nsteps):
         mps = fn(mps, mpo, dt)
         ex = O.site_expectations(mps, {i: op for i in e_sites})
         pops.append([ex[i] for i in e_sites])
@@ -97,6 +98,18 @@ def test_oracle_tdvp_ps2_matches_reference(tag):
     pops = _traj(tag, O.evolve_tdvp_ps2)
     ref = TDVP[f"{tag}/pops"]
     np.testing.assert_allclose(pops, ref, atol=1e-8)
+
+
+def test_oracle_config1_first_steps_match_reference():
+    """Config 1 (10-molecule Holstein chain, M = 32, TDVP-PS, dt = 0.05) from
+    the reference's own hint-expanded start: the oracle's first five steps
+    reproduce the reference's populations to 1e-10 (the reference moves by
+    2e-12 between 1 and 4 BLAS threads over these steps)."""
+    cfg = load_golden("config_cases.npz")
+    pops = _traj("c1", O.evolve_tdvp_ps, src=cfg, nsteps=5)
+    np.testing.assert_allclose(pops, cfg["c1/pops"][:6], atol=1e-10)
+    env = np.abs(cfg["c1/pops"] - cfg["c1/pops_t4"]).max(axis=1)
+    assert env[5] < 1e-10 < env[30]
 
 
 def test_oracle_dense_exact_dynamics():
