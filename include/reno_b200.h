@@ -117,6 +117,21 @@ int reno_gemm(reno_ctx* ctx, int32_t M, int32_t N, int32_t K, const void* A,
  * (the kernel then skipped its remaining work and freed its TMEM). */
 int reno_device_error(reno_ctx* ctx, int32_t* code);
 
+/* Wall-clock limit of every bounded device wait -- the pipeline mbarriers of
+ * the tensor-core GEMM and the grid barriers of the eigensolver reduction --
+ * for launches made after the call; 1 ms .. 60 s, default 2 s. */
+int reno_set_wait_limit_ns(uint64_t ns);
+/* Test hook of the failure path (no counterpart in the reference, which has
+ * no device code): the NEXT launch of the named kernel has CTA 0 leave one
+ * wait without its arrival, so that wait runs out after the limit above and
+ * the kernel returns with its error status set (reno_device_error 1000 + site
+ * for RENO_SKIP_SPLIT_STAGE, where `at` is the CTA's k-stage left unloaded;
+ * the reduction's status word = 1 for RENO_SKIP_HETRD_ARRIVAL, where `at` is
+ * the column whose barrier it skips).  at = -1 cancels.  Nothing faults: the
+ * kernel drains its own copies, frees its tensor memory and exits. */
+enum { RENO_SKIP_SPLIT_STAGE = 1, RENO_SKIP_HETRD_ARRIVAL = 2 };
+int reno_test_skip_arrival(int32_t kind, int32_t at);
+
 /* Allocation-free variant of reno_heff_apply.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory (hosts
  * that own the whole GPU through their own pool, foreign-language hosts that

@@ -66,6 +66,8 @@ _SIGS = {
     "reno_gemm": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _c_i64, _c_i64, _c_int, _vp, _c_int, _c_i64,
                            _c_i64, _c_int, _vp, _c_i64, _c_int, _vp, _c_sz]),
     "reno_device_error": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "reno_set_wait_limit_ns": (_c_int, [ctypes.c_uint64]),
+    "reno_test_skip_arrival": (_c_int, [ctypes.c_int32, ctypes.c_int32]),
     "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
     "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),
     "reno_heff_grouped_workspace_bytes": (_c_int, [_c_int, ctypes.POINTER(HeffDesc), ctypes.POINTER(_c_sz)]),

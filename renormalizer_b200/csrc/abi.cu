@@ -46,3 +46,17 @@ extern "C" int reno_launch_count(long long* count) {
   *count = g_launches.load();
   return RENO_OK;
 }
+
+extern "C" int reno_set_wait_limit_ns(uint64_t ns) {
+  if (ns < 1000000ull || ns > 60000000000ull) return RENO_ERR_INVALID;  // 1 ms .. 60 s
+  g_wait_ns.store(ns, std::memory_order_relaxed);
+  return RENO_OK;
+}
+
+extern "C" int reno_test_skip_arrival(int32_t kind, int32_t at) {
+  if (at < -1) return RENO_ERR_INVALID;
+  if (kind == RENO_SKIP_SPLIT_STAGE) g_skip_split_stage.store(at);
+  else if (kind == RENO_SKIP_HETRD_ARRIVAL) g_skip_hetrd_column.store(at);
+  else return RENO_ERR_INVALID;
+  return RENO_OK;
+}

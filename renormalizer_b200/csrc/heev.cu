@@ -24,7 +24,8 @@
 //   4. back-transformation K = Q Z in blocks of 64 reflectors (compact WY
 //                     form, three FP64 GEMMs per block, last block first).
 //
-// Every grid-barrier wait is bounded (WAIT_NS of wall clock): on timeout the
+// Every grid-barrier wait is bounded (2 s of wall clock by default, see
+// reno_set_wait_limit_ns): on timeout the
 // CTA raises the abort flag and a status word in the caller's workspace and
 // returns; the others return at their next barrier.
 #include <algorithm>
@@ -40,7 +41,6 @@ namespace reno {
 namespace heev {
 
 constexpr int THREADS = 256, WARPS = THREADS / 32;
-constexpr uint64_t WAIT_NS = 2000000000ull;
 constexpr int MAX_N = 4096;
 
 struct Sync {
@@ -98,13 +98,16 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // counter (no reset between columns), released by each CTA's thread 0 after
 // a CTA barrier and acquired by polling, the ordering pattern of CUTLASS's
 // generic barrier.  false when this or another CTA gave up (abort raised).
-__device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& epoch, int* ok_sh) {
+// skip_arrival (test hook only): this CTA does not arrive, so every wait of
+// this barrier runs out after wait_ns.
+__device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& epoch, int* ok_sh, uint64_t wait_ns,
+                          bool skip_arrival) {
   __syncthreads();
   if (threadIdx.x == 0) {
     epoch += 1u;
     const unsigned target = epoch * nblocks;
     bool good = true;
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&s->count) : "memory");
+    if (!skip_arrival) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&s->count) : "memory");
     volatile int* va = &s->abort;
     const uint64_t t0 = global_ns();
     for (uint32_t it = 0;; ++it) {
@@ -116,7 +119,7 @@ __device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& epoch, int* ok_sh
           good = false;
           break;
         }
-        if (global_ns() - t0 > WAIT_NS) {
+        if (global_ns() - t0 > wait_ns) {
           atomicExch(&s->abort, 1);
           atomicCAS(&s->status, 0, 1);
           good = false;
@@ -150,6 +153,8 @@ struct HetrdProb {
 };
 struct HetrdTable {
   int count;
+  int skip_column;      // test hook: CTA 0 of matrix 0 skips its arrival after this column (-1: none)
+  uint64_t wait_ns;     // limit of every grid-barrier wait
   HetrdProb p[MAXM];
 };
 
@@ -298,7 +303,7 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
       for (int w = 0; w < HW; ++w) s = cadd(s, redc[w]);
       __stcg(&P[(size_t)(k & 1) * G + bid], s);
     }
-    if (!grid_sync(sync, G, gen, &s_ok)) return;
+    if (!grid_sync(sync, G, gen, &s_ok, tab.wait_ns, pi == 0 && bid == 0 && k == tab.skip_column)) return;
 
     // ---- phase 3 (every CTA): w_k = tau y - (|tau|^2 / 2)(y^H v) v; every
     // warp sums the CTA partials itself
@@ -849,6 +854,8 @@ static int launch_hetrd(reno_ctx* ctx, HetrdTable& tab, int nmax, const char* wh
     tab.p[i].nblk = nb;
     used += nb;
   }
+  tab.wait_ns = g_wait_ns.load(std::memory_order_relaxed);
+  tab.skip_column = g_skip_hetrd_column.exchange(-1);
   void* args[] = {&tab};
   count_launch();
   return check_cuda(ctx, cudaLaunchCooperativeKernel((void*)hetrd_kernel, dim3(used), dim3(HT), args, smem,

@@ -22,6 +22,17 @@ struct reno_ctx {
 
 namespace reno {
 
+// Wall-clock limit of every bounded device wait (pipeline mbarriers of the
+// tensor-core GEMM, grid barriers of the eigensolver reduction), passed to
+// the kernels at launch; reno_set_wait_limit_ns changes it.
+inline std::atomic<unsigned long long> g_wait_ns{2000000000ull};
+// Test hooks of the failure path (reno_test_skip_arrival), consumed by the
+// next launch of the kernel they name: CTA 0 of that launch leaves one wait
+// without its arrival, so the bounded wait runs out and the kernel returns
+// with its error status set.  -1 = none.
+inline std::atomic<int> g_skip_split_stage{-1};
+inline std::atomic<int> g_skip_hetrd_column{-1};
+
 // every kernel launch of the library bumps this (host-side, per process)
 inline std::atomic<long long> g_launches{0};
 inline void count_launch(long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }

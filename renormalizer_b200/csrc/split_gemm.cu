@@ -38,7 +38,6 @@ constexpr int B_TILE = BN * KROW_BYTES;   // 32 KB
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr uint32_t TMEM_COLS = 256;  // one accumulator buffer (two are allocated)
-constexpr uint64_t WAIT_NS = 2000000000ull;  // bounded spin: 2 s of wall clock
 
 // device error word: 0 = ok; otherwise 1000 + site of the first timed-out wait
 __device__ int g_split_error = 0;
@@ -182,14 +181,15 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// bounded wait (WAIT_NS of wall clock): returns false and raises the abort flag on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int site) {
+// bounded wait (wait_ns of wall clock): returns false and raises the abort flag on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int site,
+                                          uint64_t wait_ns) {
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0;; ++it) {
     if (mbar_try(bar, parity)) return true;
     if ((it & 255u) == 255u) {
       if (*abort_flag) return false;
-      if (global_ns() - t0 > WAIT_NS) break;
+      if (global_ns() - t0 > wait_ns) break;
     }
   }
   *abort_flag = 1;
@@ -356,11 +356,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 
 // bounded wait that ignores the abort flag: used only to drain the CTA's own
 // copies and MMAs in flight before it frees TMEM and exits
-__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity, uint64_t wait_ns) {
   const uint64_t t0 = global_ns();
   for (uint32_t it = 0;; ++it) {
     if (mbar_try(bar, parity)) return;
-    if ((it & 255u) == 255u && global_ns() - t0 > WAIT_NS) {
+    if ((it & 255u) == 255u && global_ns() - t0 > wait_ns) {
       atomicCAS(&g_split_error, 0, 1009);
       return;
     }
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                       const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, Epi epi,
                       int num_k_tiles, int k_elems, int a_batched, int b_batched, int m_fast, int mt, int nt,
-                      int ntiles) {
+                      int ntiles, uint64_t wait_ns, int skip_stage) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -428,9 +428,13 @@ __global__ void __launch_bounds__(THREADS, 1)
       for (int kt = 0; kt < num_k_tiles; ++kt) {
         const int s = g % STAGES;
         const uint32_t ph = (g / STAGES) & 1;
-        if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, 1)) {
+        if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, 1, wait_ns)) {
           ok = false;
           break;
+        }
+        if (blockIdx.x == 0 && (int)g == skip_stage) {  // test hook: stage g of CTA 0 stays unloaded
+          ++g;
+          continue;
         }
         unsigned char* st = smem + s * STAGE_BYTES;
         mbar_expect_tx(&full[s], STAGE_BYTES);
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     // land every copy this CTA issued before it can exit (immediate for the
     // ones the MMA thread already consumed)
     for (uint32_t j = (g > (uint32_t)STAGES ? g - STAGES : 0u); j < g; ++j)
-      mbar_drain(&full[j % STAGES], (j / STAGES) & 1);
+      mbar_drain(&full[j % STAGES], (j / STAGES) & 1, wait_ns);
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer
     constexpr uint32_t fmt = ESZ == 2 ? 1u : 2u;  // BF16 : TF32
@@ -457,13 +461,13 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
       const int b = i & 1;
       const uint32_t use = (uint32_t)(i >> 1);
-      if (!mbar_wait(&tmem_empty[b], (use & 1) ^ 1, abort_flag, 4)) break;
+      if (!mbar_wait(&tmem_empty[b], (use & 1) ^ 1, abort_flag, 4, wait_ns)) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t tacc = tmem + (uint32_t)(b * TMEM_COLS);
       for (int kt = 0; kt < num_k_tiles; ++kt) {
         const int s = g % STAGES;
         const uint32_t ph = (g / STAGES) & 1;
-        if (!mbar_wait(&full[s], ph, abort_flag, 2)) {
+        if (!mbar_wait(&full[s], ph, abort_flag, 2, wait_ns)) {
           ok = false;
           break;
         }
@@ -492,7 +496,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     // every MMA this thread issued completes before TMEM is freed
     umma_commit(drain);
-    mbar_drain(drain, 0);
+    mbar_drain(drain, 0, wait_ns);
   } else if (warp >= 2) {
     // ---------------- epilogue
     const int q = warp % 4;                      // TMEM lane quarter this warp may access
@@ -501,7 +505,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
       const int b = i & 1;
       const uint32_t use = (uint32_t)(i >> 1);
-      if (!mbar_wait(&tmem_full[b], use & 1, abort_flag, 3)) break;
+      if (!mbar_wait(&tmem_full[b], use & 1, abort_flag, 3, wait_ns)) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
       if (*abort_flag) break;
       int m_tile, n_tile, bz;
@@ -825,7 +829,9 @@ static cudaError_t launch_split(const SplitPacked& A, const SplitPacked& B, int 
   count_launch();
   split_gemm_kernel<ESZ><<<grid, THREADS, SMEM_BYTES, st>>>(tAh, tAl, tBh, tBl, epi, (int)ceil_div(A.kext, kstep),
                                                             (int)A.kext, A.nb > 1 ? 1 : 0, B.nb > 1 ? 1 : 0, m_fast,
-                                                            (int)mt, (int)nt, (int)ntiles);
+                                                            (int)mt, (int)nt, (int)ntiles,
+                                                            (uint64_t)g_wait_ns.load(std::memory_order_relaxed),
+                                                            g_skip_split_stage.exchange(-1));
   return cudaGetLastError();
 }
 
