@@ -25,6 +25,11 @@
  *                         svd_qn.py:89-96 blockrecover, lib.py:302-316
  *                         select_basis column copy
  *  - reno_heff_diag    <- renormalizer/mps/gs.py:419-445 hdiag einsums
+ *  - reno_lanczos_expm <- renormalizer/lib/krylov/krylov.py:27-84 expm_krylov
+ *                         with the hop_expr operator
+ *  - reno_qr_blocks    <- renormalizer/mps/svd_qn.py:195-204 (QR per QN block)
+ *  - reno_heev_*       <- svd_qn.py:12-49 / mp.py:693-778 (the truncation's
+ *                         per-block factorisation, as a Gram eigenproblem)
  *  - reno_heff_backward   (no counterpart: gradients of the matvec)
  */
 #ifndef RENO_B200_H
@@ -232,6 +237,21 @@ int reno_qr_workspace_bytes(int32_t count, const reno_qr_block* blocks,
                             size_t* bytes);
 int reno_qr_blocks(reno_ctx* ctx, int32_t count, const reno_qr_block* blocks,
                    void* workspace, size_t ws_bytes);
+
+/* Lanczos exponential psi <- exp(dt H_eff) psi, krylov.py:27-84 expm_krylov
+ * with the matvec of reno_heff_apply (desc, L, W1, W2, R as there; psi
+ * complex128, dt = dt_re + i dt_im): the reference's stopping rule (results
+ * of successive even steps j > 3 allclose at rtol 1e-5 / atol 1e-8, or a
+ * breakdown beta_j < 100 n eps) and count, returned in out_k.  The host
+ * synchronises at those checks only.  Fails with RENO_ERR_WORKSPACE when more
+ * than kmax Krylov vectors would be needed.  Workspace from
+ * reno_lanczos_workspace_bytes(desc, kmax). */
+int reno_lanczos_workspace_bytes(const reno_heff_desc* desc, int32_t kmax,
+                                 size_t* bytes);
+int reno_lanczos_expm(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
+                      const void* W1, const void* W2, const void* R,
+                      double dt_re, double dt_im, void* psi, int32_t kmax,
+                      int32_t* out_k, void* ws, size_t ws_bytes);
 
 /* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
  *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]

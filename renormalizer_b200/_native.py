@@ -66,6 +66,9 @@ _SIGS = {
     "reno_gemm": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _c_i64, _c_i64, _c_int, _vp, _c_int, _c_i64,
                            _c_i64, _c_int, _vp, _c_i64, _c_int, _vp, _c_sz]),
     "reno_device_error": (_c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "reno_lanczos_workspace_bytes": (_c_int, [ctypes.POINTER(HeffDesc), _c_int, ctypes.POINTER(_c_sz)]),
+    "reno_lanczos_expm": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                   _vp, _c_int, ctypes.POINTER(ctypes.c_int32), _vp, _c_sz]),
     "reno_set_wait_limit_ns": (_c_int, [ctypes.c_uint64]),
     "reno_test_skip_arrival": (_c_int, [ctypes.c_int32, ctypes.c_int32]),
     "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
