@@ -28,6 +28,9 @@
  *  - reno_lanczos_expm <- renormalizer/lib/krylov/krylov.py:27-84 expm_krylov
  *                         with the hop_expr operator
  *  - reno_qr_blocks    <- renormalizer/mps/svd_qn.py:195-204 (QR per QN block)
+ *  - reno_qn_svd_truncate <- svd_qn.py:99-240 + lib.py:253-322 select_basis
+ *                         + configs.py:196-219 compute_m_trunc (the sweeps'
+ *                         truncation, mp.py:693-778)
  *  - reno_heev_*       <- svd_qn.py:12-49 / mp.py:693-778 (the truncation's
  *                         per-block factorisation, as a Gram eigenproblem)
  *  - reno_heff_backward   (no counterpart: gradients of the matvec)
@@ -252,6 +255,45 @@ int reno_lanczos_expm(reno_ctx* ctx, const reno_heff_desc* desc, const void* L,
                       const void* W1, const void* W2, const void* R,
                       double dt_re, double dt_im, void* psi, int32_t kmax,
                       int32_t* out_k, void* ws, size_t ws_bytes);
+
+/* QN-blocked truncation of one coefficient matrix (rows x cols, row-major):
+ * svd_qn.py:99-240 with select_basis lib.py:253-322 (percent 0) and
+ * compute_m_trunc configs.py:196-219, as the sweeps use them (mp.py:693-778).
+ * Per QN sector (left label nl, right label qntot - nl) the block's Gram
+ * matrix of its smaller side goes through the device eigensolver (all blocks
+ * in one batched call), Householder QR and the back-transformation; the
+ * singular values are the norms of the projected vectors.  The kept triplets
+ * are chosen like the reference: every block's values in block order, a
+ * stable descending sort, then the count from the rule -- FIXED: min(m_max,
+ * number of values); THRESHOLD: values with sigma / ||sigma|| > threshold;
+ * BOTH: the smaller.  Outputs: left (rows x ldm) and right (ldm x cols), the
+ * first *out_m columns / rows filled and the rest zero; keep_left = 1 gives
+ * left = U (orthonormal columns) and right = sigma V^H, keep_left = 0 gives
+ * left = U sigma and right = V^H (orthonormal rows).  sigma (host, ldm) and
+ * qn_out (host, ldm x qn_size: the kept side's sector label of each column)
+ * describe the kept columns.  Sectors are visited in the caller's order
+ * (sectors, nsectors x qn_size; the reference iterates a Python set) or, with
+ * nsectors = 0, in order of first appearance among the rows.  Zero-sigma
+ * completion columns (full_matrices=True) are not produced.  At most
+ * RENO_HEEV_MAX_BATCH sectors, smaller sides up to 4096; a block whose
+ * eigensolver check fails returns RENO_ERR_UNSUPPORTED.  Workspace from
+ * reno_qn_svd_truncate_workspace_bytes (same descriptor). */
+enum { RENO_TRUNC_FIXED = 0, RENO_TRUNC_THRESHOLD = 1, RENO_TRUNC_BOTH = 2 };
+typedef struct {
+  int32_t rows, cols, qn_size, dtype;
+  int32_t keep_left, mode, m_max, nsectors;
+  double threshold;
+  const int32_t* qn_rows;  /* host, rows x qn_size */
+  const int32_t* qn_cols;  /* host, cols x qn_size */
+  const int32_t* qntot;    /* host, qn_size */
+  const int32_t* sectors;  /* host, nsectors x qn_size, or NULL */
+} reno_trunc_desc;
+int reno_qn_svd_truncate_workspace_bytes(const reno_trunc_desc* desc,
+                                         size_t* bytes);
+int reno_qn_svd_truncate(reno_ctx* ctx, const reno_trunc_desc* desc,
+                         const void* coef, void* left, void* right,
+                         int32_t ldm, double* sigma, int32_t* qn_out,
+                         int32_t* out_m, void* ws, size_t ws_bytes);
 
 /* Diagonal of the 1/2-site effective Hamiltonian, gs.py:419-445:
  *   nsite 1: hdiag[a,c,f]   = sum L[a,b,a] W1[b,c,c,g] R[f,g,f]

@@ -37,6 +37,13 @@ class QrBlock(ctypes.Structure):
 QR_MAX_BLOCKS = 16
 
 
+class TruncDesc(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_int32), ("cols", ctypes.c_int32), ("qn_size", ctypes.c_int32),
+                ("dtype", ctypes.c_int32), ("keep_left", ctypes.c_int32), ("mode", ctypes.c_int32),
+                ("m_max", ctypes.c_int32), ("nsectors", ctypes.c_int32), ("threshold", ctypes.c_double),
+                ("qn_rows", _vp), ("qn_cols", _vp), ("qntot", _vp), ("sectors", _vp)]
+
+
 class HeevProblem(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32), ("kt", ctypes.c_int32), ("a", _vp), ("d", _vp), ("e", _vp), ("tau", _vp),
                 ("w", _vp), ("z", _vp), ("k", _vp)]
@@ -69,6 +76,9 @@ _SIGS = {
     "reno_lanczos_workspace_bytes": (_c_int, [ctypes.POINTER(HeffDesc), _c_int, ctypes.POINTER(_c_sz)]),
     "reno_lanczos_expm": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                    _vp, _c_int, ctypes.POINTER(ctypes.c_int32), _vp, _c_sz]),
+    "reno_qn_svd_truncate_workspace_bytes": (_c_int, [ctypes.POINTER(TruncDesc), ctypes.POINTER(_c_sz)]),
+    "reno_qn_svd_truncate": (_c_int, [_vp, ctypes.POINTER(TruncDesc), _vp, _vp, _vp, _c_int, _vp, _vp,
+                                      ctypes.POINTER(ctypes.c_int32), _vp, _c_sz]),
     "reno_set_wait_limit_ns": (_c_int, [ctypes.c_uint64]),
     "reno_test_skip_arrival": (_c_int, [ctypes.c_int32, ctypes.c_int32]),
     "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
