@@ -92,6 +92,7 @@ def parse():
                          "grouped FP64 matvecs, against the same realisations evolved one by one")
     ap.add_argument("--batch-nmol", type=int, default=8)
     ap.add_argument("--batch-M", type=int, default=64)
+    ap.add_argument("--cpu-worker", default="", help=argparse.SUPPRESS)
     ap.add_argument("--heff-only", action="store_true",
                     help="time only the workload's largest 2-site H_eff matvec (phonon-phonon block, M x 16 x 16 x M)")
     return ap.parse_args()
@@ -237,6 +238,57 @@ def cpu_step_sample(M, nlev, kry2, kry1, n_pairs_pp, n_pairs_ep):
     return step_s, sample_s, t
 
 
+def config1_anchor(nsteps):
+    """Config 1 (10-molecule Holstein chain, one 10-level mode, the
+    reference's hint-expanded start at M = 32) on the host: nsteps of the
+    numpy restatement's one-site TDVP-PS at dt = 0.05, timed directly.
+    Returns steps/s."""
+    from oracle import reno_oracle as O
+    d = np.load(ROOT / "tests" / "golden" / "config_cases.npz")
+    n = int(d["c1/init/nsites"])
+    init = O.OMps([d[f"c1/init/mt_{i}"] for i in range(n)], [d[f"c1/init/qn_{i}"] for i in range(n + 1)],
+                  int(d["c1/init/qnidx"]), d["c1/init/qntot"], bool(d["c1/init/to_right"]),
+                  [d[f"c1/init/sigmaqn_{i}"] for i in range(n)], compress=O.Compress("fixed", max_bonddim=32))
+    mpo = [d[f"c1/mpo/W_{i}"] for i in range(n)]
+    mps = init
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        mps = O.evolve_tdvp_ps(mps, mpo, 0.05)
+    return nsteps / (time.perf_counter() - t0)
+
+
+def cpu_worker(spec):
+    """Internal (--cpu-worker): run the CPU samples in this process, whose
+    BLAS thread count the parent set, and print them as one JSON line."""
+    M, nlev, kry2, kry1, npp, nep, c1_steps = json.loads(spec)
+    st, ss, _ = cpu_step_sample(M, nlev, kry2, kry1, npp, nep)
+    out = {"threads": threads(), "m256_step_s": st, "m256_sample_s": ss}
+    if c1_steps:
+        out["config1_steps_per_s"] = config1_anchor(c1_steps)
+    print(json.dumps(out), flush=True)
+
+
+def cpu_baselines(M, nlev, kry2, kry1, npp, nep, thread_counts=(1, 4, 8), c1_steps=10):
+    """The host baseline at several BLAS thread counts (one subprocess each:
+    the thread count is fixed when numpy loads its BLAS).  Per count: the
+    modelled M-site step (per-operation timings assembled into one step) and
+    a directly timed config-1 anchor."""
+    out = {}
+    ncpu = os.cpu_count() or 1
+    for t in thread_counts:
+        if t > ncpu:
+            continue
+        env = dict(os.environ, OPENBLAS_NUM_THREADS=str(t), OMP_NUM_THREADS=str(t), MKL_NUM_THREADS=str(t),
+                   RENO_NUM_THREADS=str(t))
+        spec = json.dumps([M, nlev, kry2, kry1, npp, nep, c1_steps])
+        r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--cpu-worker", spec], env=env,
+                           capture_output=True, text=True, timeout=900)
+        lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+        if r.returncode == 0 and lines:
+            out[t] = json.loads(lines[-1])
+    return out
+
+
 def threads():
     try:
         from threadpoolctl import threadpool_info
@@ -269,15 +321,21 @@ def run_reference(args, rank, world):
     step_s = float(np.mean(steps))
     value = 1.0 / step_s
     cores = threads()
+    c1 = config1_anchor(10)
     sample = (f"per-operation timings at M={args.M} (2-site matvecs, QN SVDs, 1-site matvecs, env updates, QR) "
               f"with the numpy oracle, {np.mean(samples):.1f} s of CPU work per step, assembled into one step "
-              f"with {KRY2_DEFAULT}/{KRY1_DEFAULT} Krylov vectors per 2-/1-site exponential")
+              f"with {KRY2_DEFAULT}/{KRY1_DEFAULT} Krylov vectors per 2-/1-site exponential (modelled: a full "
+              f"CPU step takes about half an hour); beside it, config 1 timed directly")
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "nsites": 3 * args.nmol, "M": args.M, "nlev": args.nlev,
                        "dt": args.dt, "parallelism": "replicas" if world > 1 else "single"},
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample,
+                             "modelled": True, "host_cpus": os.cpu_count(),
+                             "RENO_NUM_THREADS": os.environ.get("RENO_NUM_THREADS", "unset"),
+                             "config1_anchor": {"steps_per_s": c1, "steps": 10, "measured": True,
+                                                "workload": "holstein10_nlev10_M32_tdvp_ps_dt0.05"}},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -383,6 +441,25 @@ def fp64_peak_tflops(dev):
     return best
 
 
+def tf32_peak_tflops(dev):
+    import torch
+    a = torch.randn(8192, 8192, dtype=torch.float32, device=dev)
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ a
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a
+    return best
+
+
 def reduce_max_ms(t_ms: float, dist, device) -> float:
     """The multi-GPU timing rule: every rank's device time, max over ranks
     (one all-reduce; identity without a process group)."""
@@ -404,7 +481,7 @@ def run_engine(args, rank, world, dist):
     backend.prec = args.prec
     model = holstein_2mode(args.nmol, args.nlev)
     mpo = Mpo(model)
-    mps0 = initial_state(model, args.M)
+    mps0 = initial_state(model, args.M, args.start, mpo)
     mps = mps0
     pops_first = None
     for i in range(args.warmup):
@@ -425,6 +502,7 @@ def run_engine(args, rank, world, dist):
     import importlib
     svdmod = importlib.import_module("renormalizer_b200.svd_qn")
     sub0 = (svdmod.subspace.calls, svdmod.subspace.fallbacks, svdmod.subspace.retries)
+    svdmod.flop_log = []
     with ClockSampler(local) as clocks:
         s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s_ev.record()
@@ -433,7 +511,10 @@ def run_engine(args, rank, world, dist):
         e_ev.record()
         barrier()
     launches = launch_count() - l0
-    trunc = {"subspace_blocks": svdmod.subspace.calls - sub0[0], "retries": svdmod.subspace.retries - sub0[2],
+    trunc_fl = float(sum(svdmod.flop_log))
+    svdmod.flop_log = None
+    heev_mod = importlib.import_module("renormalizer_b200.heev")
+    trunc = {"device_eigensolver_fallbacks": heev_mod.heev_opts.fallbacks,"subspace_blocks": svdmod.subspace.calls - sub0[0], "retries": svdmod.subspace.retries - sub0[2],
              "fallbacks": svdmod.subspace.fallbacks - sub0[1],
              "options": {"min_dim": svdmod.subspace.min_dim, "iters": svdmod.subspace.iters,
                          "oversample": svdmod.subspace.oversample, "rtol": svdmod.subspace.rtol}}
@@ -452,7 +533,7 @@ def run_engine(args, rank, world, dist):
         barrier()
         s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s2.record()
-        ne2e = 1
+        ne2e = min(args.steps, 3)
         for _ in range(ne2e):
             m = mps.metacopy()
             m._mp = [t.to(dev, non_blocking=True) for t in host_sites]
@@ -464,23 +545,40 @@ def run_engine(args, rank, world, dist):
         e2e = {"value": world * ne2e / (te * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(pops.size * 8)}
 
-    # plain FP64 engine on the same start state (speed ratio and accuracy)
+    # plain FP64 engine from the same start state: population difference after
+    # the first step, and its steps/s over several steps
     fp64 = None
     if args.prec != "fp64":
         backend.prec = "fp64"
+        nfp = max(1, min(args.steps, 4))
         barrier()
         s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s3.record()
         ref = mps0.evolve(mpo, args.dt)
+        pops_ref = ref.e_occupations
+        for _ in range(nfp - 1):
+            ref = ref.evolve(mpo, args.dt)
         e3.record()
         barrier()
-        pops_ref = ref.e_occupations
-        fp64 = {"steps_per_s": 1.0 / (s3.elapsed_time(e3) * 1e-3),
+        t_fp = reduce_max_ms(s3.elapsed_time(e3), dist, dev)
+        fp64 = {"steps_per_s": world * nfp / (t_fp * 1e-3), "steps_timed": nfp,
                 "max_abs_dpop_after_1_step": float(np.abs(pops_ref - pops_first).max())}
         backend.prec = args.prec
 
+    peaks = None
+    if rank == 0:
+        peaks = {"fp64_dgemm_tflops": fp64_peak_tflops(dev), "tf32_tflops": tf32_peak_tflops(dev),
+                 "source": "cuBLAS 8192^3 GEMMs measured in this run (best of 4)"}
+        try:
+            mp = json.load(open(ROOT / "MEASURED_PEAKS.json"))
+            peaks["bf16_tflops_sustained"] = mp.get("bf16_tflops_sustained")
+            peaks["hbm_gbs"] = mp.get("hbm_gbs")
+        except Exception:
+            pass
+
     if args.prec == "fp64":
-        peak, peak_src = fp64_peak_tflops(dev), "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)"
+        peak, peak_src = peaks["fp64_dgemm_tflops"] if peaks else fp64_peak_tflops(dev), \
+            "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)"
     else:
         peak, peak_src = None, "MEASURED_PEAKS.json bf16_tflops_sustained"
         try:
@@ -506,26 +604,51 @@ def run_engine(args, rank, world, dist):
                 "all_2site_matvecs": {"achieved": achieved_all, "launches_timed": nheff},
                 "peak_source": peak_src}
 
+    # truncation: algorithmic FP64 flops of its block factorisations against
+    # the measured DGEMM rate
+    trunc_ms = phases.result().get("svd_truncate", 0.0)
+    trunc_roof = None
+    if trunc_fl and trunc_ms > 0 and peaks:
+        ach = trunc_fl / (trunc_ms * 1e-3) / 1e12
+        trunc_roof = {"bound": "fp64 (latency-bound reduction)", "achieved": ach, "unit": "TFLOP/s",
+                      "peak": peaks["fp64_dgemm_tflops"], "frac": ach / peaks["fp64_dgemm_tflops"],
+                      "ms_per_step": trunc_ms / args.steps, "gflop_per_step": trunc_fl / args.steps / 1e9,
+                      "counted": "per QN block: Gram 8 s^2 l, tridiagonal reduction 16/3 s^3, back-transformation "
+                                 "8 s^2 k, projection 8 s l k (complex; real blocks a quarter), s / l the block's "
+                                 "smaller / larger side, k the eigenvectors used"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         npp, nep = n_pairs(args.nmol)
         k2 = kry_timed["mean"] if kry_timed else KRY2_DEFAULT
-        st, ss, _ = cpu_step_sample(args.M, args.nlev, k2, k2, npp, nep)
-        cpu = {"value": 1.0 / st, "unit": "steps/s", "cores": threads(), "kind": "port",
-               "sample": f"numpy oracle per-operation timings at M={args.M} ({ss:.1f} s of CPU work), assembled "
-                         f"into one TDVP-PS2 step with the engine's measured {k2:.2f} Krylov vectors per exponential"}
+        by_t = cpu_baselines(args.M, args.nlev, k2, k2, npp, nep)
+        if by_t:
+            tmax = max(by_t)
+            cpu = {"value": 1.0 / by_t[tmax]["m256_step_s"], "unit": "steps/s", "cores": by_t[tmax]["threads"],
+                   "kind": "port", "modelled": True, "host_cpus": os.cpu_count(),
+                   "RENO_NUM_THREADS": {str(t): t for t in by_t},
+                   "sample": f"numpy oracle per-operation timings at M={args.M} "
+                             f"({by_t[tmax]['m256_sample_s']:.1f} s of CPU work at {tmax} BLAS threads), assembled "
+                             f"into one TDVP-PS2 step with the engine's measured {k2:.2f} Krylov vectors per "
+                             f"exponential (a full CPU step takes about half an hour)",
+                   "by_threads": {str(t): {"modelled_steps_per_s": 1.0 / v["m256_step_s"],
+                                           "config1_steps_per_s": v.get("config1_steps_per_s")}
+                                  for t, v in by_t.items()},
+                   "config1_anchor": "holstein10_nlev10_M32_tdvp_ps_dt0.05, 10 steps of the numpy restatement "
+                                     "timed directly per thread count"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128" if args.prec == "fp64" else args.prec,
-                "data": "synthetic (Hartree product + seeded random bond expansion to M)",
+                "data": f"synthetic (Hartree product + {'the hint-MPO' if args.start == 'hint' else 'a seeded random'} bond expansion to M)",
                 "config": {"workload": WORKLOAD, "nsites": 3 * args.nmol, "M": args.M, "nlev": args.nlev,
                            "dt": args.dt, "prec": args.prec, "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (MPS ~1.5 GB, environments ~1 GB resident in HBM)"},
                 "tflops_heff2": achieved_all, "heff2_ms": round(heff_ms, 1), "phase_ms": phases.result(),
                 "krylov": kry_timed, "bond_dims_max": max(mps.bond_dims), "truncation": trunc,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline, "truncation_roofline": trunc_roof, "peaks": peaks, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks.summary(), "fp64_engine": fp64}
         print(json.dumps(line), flush=True)
 
@@ -818,6 +941,9 @@ def run_grad(args):
 
 def main():
     args = parse()
+    if args.cpu_worker:
+        cpu_worker(args.cpu_worker)
+        return
     if args.dmrg:
         run_dmrg(args)
         return

@@ -300,6 +300,18 @@ class SubspaceOptions:
 
 
 subspace = SubspaceOptions()
+# when a list, svd_truncate appends the algorithmic FP64 flops of each call's
+# block factorisations (see _block_flops)
+flop_log = None
+
+
+def _block_flops(m, n, k, cplx):
+    """Gram 8 s^2 l, tridiagonal reduction 16/3 s^3, back-transformation
+    8 s^2 k, projection 8 s l k for a block with smaller / larger side s / l
+    and k eigenvectors used (complex counts; a real block a quarter)"""
+    s, l = min(m, n), max(m, n)
+    f = 8.0 * s * s * l + 16.0 / 3.0 * s ** 3 + 8.0 * s * s * k + 8.0 * s * l * k
+    return f if cplx else f / 4.0
 _OMEGA = {}
 
 
@@ -559,6 +571,10 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         blocks.append(blk)
         pending.append(blk)
     if pending:
+        if flop_log is not None:
+            for b in pending:
+                m_, n_ = b["X"].shape
+                flop_log.append(_block_flops(m_, n_, b["ktop"] or min(m_, n_), b["X"].is_complex()))
         fulls = _kept_sides(eng, [b["X"] for b in pending], keep_left, [b["ktop"] for b in pending])
         for b, full in zip(pending, fulls):
             b.update(K=full["K"], P=full["P"], S=full["S"])
