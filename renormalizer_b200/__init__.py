@@ -20,8 +20,9 @@ from .svd_qn import svd_qn
 from .davidson import davidson
 from .gs import optimize_mps
 from .autodiff import heff as heff_autograd
+from .tdmps import TdMpsJob
 
 __all__ = ["backend", "evolve_batch", "compressed_sum", "CompressConfig", "CompressCriteria", "EvolveConfig", "EvolveMethod", "OptimizeConfig",
            "BasisHalfSpin", "BasisSHO", "BasisSimpleElectron", "HolsteinModel", "Model", "Mol", "Op", "Phonon",
            "Quantity", "SpectralDensityFunction", "SpinBosonModel", "Mpo", "Mps", "Environ", "contract_one_site",
-           "hop_expr", "expm_krylov", "svd_qn", "davidson", "optimize_mps", "heff_autograd"]
+           "hop_expr", "expm_krylov", "svd_qn", "davidson", "optimize_mps", "heff_autograd", "TdMpsJob"]

@@ -181,6 +181,8 @@ class Mps:
         mps = cls.from_arrays(model, sites, qn, int(d["qnidx"]), d["qntot"].astype(int), to_right)
         if version in ("0.3", "0.4") and "coeff" in d.files:
             mps.coeff = d["coeff"].item(0)
+        elif version == "0.2" and "tdh_wfns" in d.files:
+            mps.coeff = d["tdh_wfns"][-1]
         return mps
 
     def dump(self, fname, other_attrs=None):
