@@ -47,3 +47,13 @@ def contract_expression(subscripts, *shapes, constants=(), **kwargs):
         return np.einsum(subscripts, *ops, optimize=cache[key])
 
     return expr
+
+
+def contract_path(subscripts, *operands, optimize="auto", **kwargs):
+    """(path, info) like opt_einsum.contract_path, for callers that only plan
+    (torch.einsum consults an importable opt_einsum): numpy's optimal path
+    on shape-only placeholders, as a list of operand-index tuples."""
+    shapes = [tuple(o.shape) for o in operands]
+    ops = [np.lib.stride_tricks.as_strided(np.zeros(1), shape=sh, strides=(0,) * len(sh)) for sh in shapes]
+    path, info = np.einsum_path(subscripts, *ops, optimize=_OPT)
+    return [tuple(p) for p in path[1:]], info

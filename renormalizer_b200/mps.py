@@ -38,7 +38,8 @@ from .krylov import expm_krylov
 from .lib import Environ, contract_one_site
 from .model import Model, Op
 from .mpo import Mpo
-from .svd_qn import qn_sectors, add_outer, get_qn_mask, qr_split, select_basis_indices, svd_truncate
+from .svd_qn import (qn_sectors, add_outer, get_qn_mask, qr_split, select_basis_indices, svd_truncate,
+                     svd_truncate_batch)
 
 logger = logging.getLogger(__name__)
 
@@ -48,6 +49,14 @@ def _krylov_stats(steps):
         return None
     a = np.asarray(steps, dtype=float)
     return {"nobs": int(a.size), "minmax": (int(a.min()), int(a.max())), "mean": float(a.mean())}
+
+
+class TruncRequest:
+    """A truncation a sweep generator yields (svd_truncate's keyword
+    arguments); it receives the TruncatedSplit back."""
+
+    def __init__(self, kwargs: dict):
+        self.kwargs = kwargs
 
 
 class Mps:
@@ -488,13 +497,23 @@ class Mps:
     def _update_mps(self, cstruct: torch.Tensor, cidx: List[int], qnbigl, qnbigr, percent=0):
         """mp.py:651-888, one root, no OFS: QN-blocked SVD truncation of the
         active coefficient and placement of the kept / complementary parts."""
+        res = svd_truncate(**self._truncation_call(cstruct, cidx, qnbigl, qnbigr, percent))
+        self._place_truncation(res, cidx, qnbigl, qnbigr)
+
+    def _truncation_call(self, cstruct: torch.Tensor, cidx: List[int], qnbigl, qnbigr, percent=0) -> dict:
+        """svd_truncate's arguments for the truncation of _update_mps"""
         if self.compress_config.bonddim_should_set:
             self.compress_config.set_bonddim(len(self) + 1)
         left = bool(self.to_right)
         bond_site = cidx[0] if left else cidx[-1]
-        res = svd_truncate(cstruct, qnbigl, qnbigr, self.qntot, keep_left=left,
-                           m_trunc_fn=lambda s: self.compress_config.compute_m_trunc(s, bond_site, left),
-                           percent=percent, kcap=self.compress_config.fixed_cap(bond_site, left))
+        cfg = self.compress_config
+        return dict(coef=cstruct, qnbigl=qnbigl, qnbigr=qnbigr, qntot=self.qntot, keep_left=left,
+                    m_trunc_fn=lambda s: cfg.compute_m_trunc(s, bond_site, left), percent=percent,
+                    kcap=cfg.fixed_cap(bond_site, left))
+
+    def _place_truncation(self, res, cidx: List[int], qnbigl, qnbigr):
+        """the kept / complementary parts of a truncation into the sites (mp.py:779-888)"""
+        left = bool(self.to_right)
         ldims = list(qnbigl.shape[:-1])
         rdims = list(qnbigr.shape[:-1])
         lmat = res.left.reshape(ldims + [res.mdim])
@@ -877,11 +896,15 @@ class Mps:
 
     def _drive(self, steps):
         """Run a sweep generator, serving each local exponential it yields
-        (operator, dt, vector) with expm_krylov; returns the new MPS."""
+        (operator, dt, vector) with expm_krylov and each truncation
+        (TruncRequest) with svd_truncate; returns the new MPS."""
         try:
             req = next(steps)
             while True:
-                req = steps.send(self._krylov(*req))
+                if isinstance(req, TruncRequest):
+                    req = steps.send(svd_truncate(**req.kwargs))
+                else:
+                    req = steps.send(self._krylov(*req))
         except StopIteration as stop:
             return stop.value
 
@@ -967,7 +990,8 @@ class Mps:
                 local_steps.append(j)
                 mps_t = mps_t.reshape(shape2)
                 qnbigl, qnbigr, _ = mps._get_big_qn([cidx0, cidx1], with_mat=False)
-                mps._update_mps(mps_t, [cidx0, cidx1], qnbigl, qnbigr)
+                res = yield TruncRequest(mps._truncation_call(mps_t, [cidx0, cidx1], qnbigl, qnbigr))
+                mps._place_truncation(res, [cidx0, cidx1], qnbigl, qnbigr)
                 if imps == last_idx:
                     continue
                 if mps.to_right:
@@ -1014,7 +1038,9 @@ def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True) -> Li
     own sweep; the local exponentials that are pending at the same time run
     in lockstep (expm_krylov_batch) and their matvecs as grouped launches
     (hop_expr.apply_grouped: one launch per contraction stage for all FP64
-    problems).  Each result equals that instance's own evolve."""
+    problems), and the truncations pending at the same time share one
+    batched eigensolver pass and one host transfer (svd_truncate_batch).
+    Each result equals that instance's own evolve."""
     from .hop_expr import apply_grouped
     from .krylov import expm_krylov_batch
     if isinstance(mpo_list, Mpo):
@@ -1029,17 +1055,28 @@ def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True) -> Li
         except StopIteration as stop:
             out[i] = stop.value
     while pending:
-        idx = sorted(pending)
-        reqs = [pending[i] for i in idx]
-        ops = [r[0] for r in reqs]
-        res = expm_krylov_batch(lambda sub, xs: apply_grouped([ops[k] for k in sub], xs), [r[1] for r in reqs],
-                                [r[2].reshape(-1) for r in reqs])
         nxt = {}
-        for i, r in zip(idx, res):
-            try:
-                nxt[i] = gens[i].send(r)
-            except StopIteration as stop:
-                out[i] = stop.value
+        # truncations of this round: one batched pass over all their QN blocks
+        tidx = sorted(i for i in pending if isinstance(pending[i], TruncRequest))
+        if tidx:
+            res = svd_truncate_batch([pending[i].kwargs for i in tidx])
+            for i, r in zip(tidx, res):
+                try:
+                    nxt[i] = gens[i].send(r)
+                except StopIteration as stop:
+                    out[i] = stop.value
+        # local exponentials of this round in lockstep, grouped matvecs
+        idx = sorted(i for i in pending if not isinstance(pending[i], TruncRequest))
+        if idx:
+            reqs = [pending[i] for i in idx]
+            ops = [r[0] for r in reqs]
+            res = expm_krylov_batch(lambda sub, xs: apply_grouped([ops[k] for k in sub], xs), [r[1] for r in reqs],
+                                    [r[2].reshape(-1) for r in reqs])
+            for i, r in zip(idx, res):
+                try:
+                    nxt[i] = gens[i].send(r)
+                except StopIteration as stop:
+                    out[i] = stop.value
         pending = nxt
     if normalize:
         for m in out:

@@ -537,6 +537,34 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
     (``subspace`` options); its residual norms come to the host with the
     singular values and a block whose Ritz pairs miss the tolerance is redone
     with the full decomposition."""
+    st = _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent, full_matrices, kcap)
+    _trunc_eig([st])
+    host = torch.cat(_trunc_host_tensors(st)).cpu().numpy()
+    return _trunc_end(st, host)
+
+
+def svd_truncate_batch(calls) -> List["TruncatedSplit"]:
+    """svd_truncate for several independent coefficients at once (the
+    truncations of lockstep realisations, evolve_batch): every QN block of
+    every call goes through one batched device eigensolver pass (per kept
+    side) and their singular values and checks reach the host in one
+    transfer.  ``calls`` holds svd_truncate's keyword arguments; each result
+    equals that call's own svd_truncate."""
+    states = [_trunc_begin(**c) for c in calls]
+    _trunc_eig(states)
+    parts = [_trunc_host_tensors(st) for st in states]
+    lens = [sum(t.numel() for t in p) for p in parts]
+    host = torch.cat([t for p in parts for t in p]).cpu().numpy()
+    out, off = [], 0
+    for st, n in zip(states, lens):
+        out.append(_trunc_end(st, host[off:off + n]))
+        off += n
+    return out
+
+
+def _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent=0, full_matrices=True, kcap=None):
+    """Gather the QN blocks of one truncation (the subspace blocks, when that
+    opt-in route applies, are factorised here)."""
     eng = Engine.get(coef.device)
     rows = int(np.prod(qnbigl.shape[:-1]))
     cols = int(np.prod(qnbigr.shape[:-1]))
@@ -570,23 +598,47 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
         blk = dict(nl=nl, nr=nr, lset=lset, rset=rset, dim=dim, npad=npad, X=X, ktop=ktop)
         blocks.append(blk)
         pending.append(blk)
-    if pending:
+    if not blocks:
+        raise ValueError("Invalid quantum number")
+    return dict(eng=eng, coef=coef, rows=rows, cols=cols, keep_left=keep_left, m_trunc_fn=m_trunc_fn,
+                percent=percent, blocks=blocks, pending=pending)
+
+
+def _trunc_eig(states):
+    """Kept sides of the pending blocks of every state: one _kept_sides pass
+    per kept side over all of them."""
+    for keep_left in (True, False):
+        group = [b for st in states if st["keep_left"] == keep_left for b in st["pending"]]
+        if not group:
+            continue
         if flop_log is not None:
-            for b in pending:
+            for b in group:
                 m_, n_ = b["X"].shape
                 flop_log.append(_block_flops(m_, n_, b["ktop"] or min(m_, n_), b["X"].is_complex()))
-        fulls = _kept_sides(eng, [b["X"] for b in pending], keep_left, [b["ktop"] for b in pending])
-        for b, full in zip(pending, fulls):
+        fulls = _kept_sides(states[0]["eng"], [b["X"] for b in group], keep_left, [b["ktop"] for b in group])
+        for b, full in zip(group, fulls):
             b.update(K=full["K"], P=full["P"], S=full["S"])
             if full["chk"] is not None:
                 b["chk"] = full["chk"]
             else:
                 b.pop("X")
-    if not blocks:
-        raise ValueError("Invalid quantum number")
+
+
+def _trunc_host_tensors(st):
+    """The device values the host needs: every block's sigma, the subspace
+    residual pairs and the device eigensolver's check triples."""
+    blocks = st["blocks"]
+    return [b["S"] for b in blocks] + [b["res"] for b in blocks if "res" in b] + \
+        [b["chk"] for b in blocks if "chk" in b]
+
+
+def _trunc_end(st, host):
+    """Checks (redo of failed blocks), the reference's selection and the
+    scatter of the kept columns, from the host copy of _trunc_host_tensors."""
+    eng, coef, rows, cols = st["eng"], st["coef"], st["rows"], st["cols"]
+    keep_left, m_trunc_fn, percent, blocks = st["keep_left"], st["m_trunc_fn"], st["percent"], st["blocks"]
     sub = [b for b in blocks if "res" in b]
     dev_eig = [b for b in blocks if "chk" in b]
-    host = torch.cat([b["S"] for b in blocks] + [b["res"] for b in sub] + [b["chk"] for b in dev_eig]).cpu().numpy()
     off = 0
     for b in blocks:
         b["Sh"] = host[off:off + b["dim"]]
