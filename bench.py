@@ -87,11 +87,13 @@ def parse():
                     help="time the device Hermitian eigensolver (leading 320 eigenpairs, or N/2 below 640) against "
                          "cuSOLVER eigh on a seeded N x N complex Gram matrix")
     ap.add_argument("--batch", type=int, default=0, metavar="B",
-                    help="TDVP-PS2 of B static-disorder realisations (per-molecule couplings g ~ U(0.5, 1.5), "
-                         "--batch-nmol molecules with one 10-level mode, M = --batch-M) advanced in lockstep with "
-                         "grouped FP64 matvecs, against the same realisations evolved one by one")
-    ap.add_argument("--batch-nmol", type=int, default=8)
-    ap.add_argument("--batch-M", type=int, default=64)
+                    help="config 4: TDVP-PS2 of B static-disorder realisations (--batch-nmol molecules with one "
+                         "10-level mode, site energies N(0, 0.5), hoppings 1 + N(0, 0.1), bonds <= --batch-M with "
+                         "the 1e-8 threshold) advanced in lockstep, against the same realisations one by one")
+    ap.add_argument("--batch-nmol", type=int, default=16)
+    ap.add_argument("--batch-M", type=int, default=128)
+    ap.add_argument("--batch-serial", type=int, default=4,
+                    help="--batch mode: realisations timed one by one for the comparison")
     ap.add_argument("--cpu-worker", default="", help=argparse.SUPPRESS)
     ap.add_argument("--heff-only", action="store_true",
                     help="time only the workload's largest 2-site H_eff matvec (phonon-phonon block, M x 16 x 16 x M)")
@@ -836,50 +838,78 @@ def run_heev(args):
                       "max_eigenvalue_diff_rel": float((w - top).abs().max() / top.abs().max())}), flush=True)
 
 
-def run_batch(args):
-    """evolve_batch (lockstep sweeps, grouped FP64 matvecs) vs per-realisation
-    Mps.evolve on the same static-disorder realisations, one warm-up step
-    each, then one timed step; reports realisation-steps per second and the
-    largest population difference between the two."""
-    import torch
+def c4_cases(B, nmol, M, nlev=10, seed=4):
+    """Config 4: B static-disorder realisations of an nmol-molecule Holstein
+    chain (omega = 1, g = 1, nlev levels); site energies eps_i ~ N(0, 0.5)
+    and nearest-neighbour hoppings J (1 + N(0, 0.1)), J = 1, all drawn from
+    one seeded generator; bonds capped at M with the 1e-8 singular-value
+    threshold (CompressCriteria.both), so they truncate unevenly; start:
+    the exciton on molecule 0, bonds expanded with a seeded random expander."""
     from renormalizer_b200 import (CompressConfig, CompressCriteria, EvolveConfig, EvolveMethod, HolsteinModel, Mol,
-                                   Mpo, Mps, Phonon, Quantity, backend, evolve_batch)
-    from renormalizer_b200._native import launch_count
-    torch.cuda.set_device(0)
-    backend.prec = "fp64"
-    B, nmol, M, nlev, dt = args.batch, args.batch_nmol, args.batch_M, 10, 0.05
-    rng = np.random.default_rng(77)
+                                   Mpo, Mps, Phonon, Quantity)
+    rng = np.random.default_rng(seed)
     cases = []
     for b in range(B):
-        g = rng.uniform(0.5, 1.5, nmol)
-        mols = [Mol(Quantity(0), [Phonon.simple_phonon(Quantity(1.0), Quantity(np.sqrt(2.0) * gi), nlev)]) for gi in g]
-        model = HolsteinModel(mols, Quantity(1.0), 3)
+        eps = rng.normal(0.0, 0.5, nmol)
+        hop = 1.0 * (1.0 + rng.normal(0.0, 0.1, nmol - 1))
+        J = np.zeros((nmol, nmol))
+        for i in range(nmol - 1):
+            J[i, i + 1] = J[i + 1, i] = hop[i]
+        ph = [Phonon.simple_phonon(Quantity(1.0), Quantity(np.sqrt(2.0)), nlev)]
+        model = HolsteinModel([Mol(Quantity(float(e)), ph) for e in eps], J, 3)
         np.random.seed(1000 + b)
         mps = Mps.hartree_product_state(model, {0: 1})
-        mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=M)
+        mps.compress_config = CompressConfig(CompressCriteria.both, threshold=1e-8, max_bonddim=M)
         mps = mps.expand_bond_dimension()
         mps.evolve_config = EvolveConfig(EvolveMethod.tdvp_ps2)
         cases.append((mps, Mpo(model)))
+    return cases
+
+
+def run_batch(args):
+    """Config 4 (c4_cases, TDVP-PS2, dt = 0.05): the realisations advanced in
+    lockstep by evolve_batch -- grouped FP64 matvecs, lockstep Lanczos, and
+    every round's truncations in one batched eigensolver pass -- against the
+    same realisations evolved one by one with Mps.evolve.  One warm-up step
+    each, then --steps timed lockstep steps of all realisations and --steps
+    timed steps of the first --batch-serial realisations one by one;
+    realisation-steps per second of both and their populations compared."""
+    import torch
+    from renormalizer_b200 import backend, evolve_batch
+    from renormalizer_b200._native import launch_count
+    torch.cuda.set_device(0)
+    backend.prec = "fp64"
+    B, nmol, M, dt = args.batch, args.batch_nmol, args.batch_M, 0.05
+    cases = c4_cases(B, nmol, M)
     mpos = [mpo for _, mpo in cases]
-    seq = [m.evolve(o, dt) for m, o in cases]
     bat = evolve_batch([m for m, _ in cases], mpos, dt)
+    nser = min(args.batch_serial, B)
+    seq = [m.evolve(o, dt) for (m, _), o in zip(cases[:nser], mpos[:nser])]
     torch.cuda.synchronize()
-    t0 = time.time()
-    seq2 = [m.evolve(o, dt) for m, o in zip(seq, mpos)]
-    torch.cuda.synchronize()
-    t_seq = time.time() - t0
     l0 = launch_count()
     t0 = time.time()
-    bat2 = evolve_batch(bat, mpos, dt)
+    for _ in range(args.steps):
+        bat = evolve_batch(bat, mpos, dt)
     torch.cuda.synchronize()
     t_bat = time.time() - t0
     launches = launch_count() - l0
-    dpop = max(float(np.abs(a.e_occupations - b.e_occupations).max()) for a, b in zip(bat2, seq2))
-    print(json.dumps({"metric": f"TDVP-PS2 realisation-steps/s, {B} static-disorder realisations (lockstep, grouped "
-                                f"FP64 matvecs)", "value": B / t_bat, "unit": "realisation-steps/s",
-                      "sequential_value": B / t_seq, "speedup_vs_sequential": t_seq / t_bat,
-                      "config": {"realisations": B, "nmol": nmol, "nlev": nlev, "M": M, "dt": dt, "prec": "fp64"},
-                      "max_abs_dpop_batch_vs_sequential": dpop, "engine_launches_batch_step": launches}), flush=True)
+    t0 = time.time()
+    for _ in range(args.steps):
+        seq = [m.evolve(o, dt) for m, o in zip(seq, mpos[:nser])]
+    torch.cuda.synchronize()
+    t_seq = time.time() - t0
+    dpop = max(float(np.abs(a.e_occupations - b.e_occupations).max()) for a, b in zip(bat[:nser], seq))
+    v_bat, v_seq = B * args.steps / t_bat, nser * args.steps / t_seq
+    print(json.dumps({"metric": f"TDVP-PS2 realisation-steps/s, {B} static-disorder realisations (config 4)",
+                      "value": v_bat, "unit": "realisation-steps/s", "one_by_one_value": v_seq,
+                      "speedup_vs_one_by_one": v_bat / v_seq,
+                      "config": {"realisations": B, "nmol": nmol, "nlev": 10, "M_cap": M, "threshold": 1e-8,
+                                 "dt": dt, "prec": "fp64", "timed_steps": args.steps,
+                                 "one_by_one_sample": nser},
+                      "bond_dims_max_mean": [int(max(max(m.bond_dims) for m in bat)),
+                                             float(np.mean([np.mean(m.bond_dims) for m in bat]))],
+                      "max_abs_dpop_lockstep_vs_one_by_one": dpop, "engine_launches_lockstep": launches}),
+          flush=True)
 
 
 def run_grad(args):
