@@ -200,7 +200,7 @@ int reno_heev_status_offset(size_t* offset);
  * the grid divided among them in proportion to n^2.  status[i] (device int)
  * receives problem i's status word.  k is used by the back-transformation
  * only.  Workspace from reno_heev_batched_workspace_bytes. */
-#define RENO_HEEV_MAX_BATCH 8
+#define RENO_HEEV_MAX_BATCH 32
 typedef struct {
   int32_t n, kt;
   void* a;      /* n x n complex128, private copy, overwritten */

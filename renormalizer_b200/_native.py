@@ -49,7 +49,7 @@ class HeevProblem(ctypes.Structure):
                 ("w", _vp), ("z", _vp), ("k", _vp)]
 
 
-HEEV_MAX_BATCH = 8
+HEEV_MAX_BATCH = 32
 
 
 class EnvDesc(ctypes.Structure):

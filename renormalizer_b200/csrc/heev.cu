@@ -136,7 +136,7 @@ __device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& epoch, int* ok_sh
 constexpr int HT = 512, HW = HT / 32;  // reduction kernel: 16 warps, one CTA per SM
 constexpr int U1 = 4;                  // loads in flight per thread (rows k, y)
 constexpr int U2 = 8;                  // loads in flight per lane (trailing rows)
-constexpr int MAXM = 8;                // matrices per batched launch
+constexpr int MAXM = 32;               // matrices per batched launch
 
 // One matrix of a batched reduction: CTAs first .. first + nblk - 1 of the
 // cooperative grid work on it, with their own barrier word and buffers.
@@ -151,6 +151,24 @@ struct HetrdProb {
   Sync* sync;
   int first, nblk;
 };
+// One matrix of the batched small-matrix reduction and of the batched
+// eigenvalue / eigenvector stages (blockIdx.y = entry).
+struct EigProb {
+  double2* a;
+  double2* tau;
+  double* d;
+  double* e;
+  int n, kt;
+  double* w;
+  double* z;
+  double* bnd;
+  double* scr;
+};
+struct EigTable {
+  int count;
+  EigProb p[MAXM];
+};
+
 struct HetrdTable {
   int count;
   int skip_column;      // test hook: CTA 0 of matrix 0 skips its arrival after this column (-1: none)
@@ -370,16 +388,16 @@ inline size_t cluster_smem_bytes(int n) {
 }
 
 __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(CT, 1)
-    hetrd_cluster_kernel(const double2* __restrict__ Gin, double2* Aout, int n, double* __restrict__ d,
-                         double* __restrict__ e, double2* __restrict__ tau) {
+    hetrd_cluster_kernel(const __grid_constant__ EigTable tab) {
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
-  const size_t mat = blockIdx.y;
-  Gin += mat * n * n;
-  Aout += mat * n * n;
-  d += mat * n;
-  e += mat * n;
-  tau += mat * n;
+  const EigProb& PR = tab.p[blockIdx.y];
+  const double2* __restrict__ Gin = PR.a;
+  double2* Aout = PR.a;
+  const int n = PR.n;
+  double* __restrict__ d = PR.d;
+  double* __restrict__ e = PR.e;
+  double2* __restrict__ tau = PR.tau;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* rows = reinterpret_cast<double2*>(smem_raw);  // RL x n
   double2* vp = rows + (size_t)RL * n;
@@ -513,8 +531,12 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e2, in
 }
 
 // Gershgorin bounds and pivmin of T into out[0..2] (one block)
-__global__ void __launch_bounds__(THREADS) bounds_kernel(const double* __restrict__ d, const double* __restrict__ e,
-                                                         int n, double* __restrict__ out) {
+__global__ void __launch_bounds__(THREADS) bounds_kernel(const __grid_constant__ EigTable tab) {
+  const EigProb& PR = tab.p[blockIdx.y];
+  const double* __restrict__ d = PR.d;
+  const double* __restrict__ e = PR.e;
+  const int n = PR.n;
+  double* __restrict__ out = PR.bnd;
   __shared__ double rmin[WARPS], rmax[WARPS], re2[WARPS];
   double lo = DBL_MAX, hi = -DBL_MAX, m2 = 0.0;
   for (int i = threadIdx.x; i < n; i += THREADS) {
@@ -553,9 +575,13 @@ __global__ void __launch_bounds__(THREADS) bounds_kernel(const double* __restric
 }
 
 // eigenvalue i0 + j (ascending) of T for j < cnt, one warp each
-__global__ void __launch_bounds__(THREADS) bisect_kernel(const double* __restrict__ d, const double* __restrict__ e,
-                                                         int n, int i0, int cnt, const double* __restrict__ bnd,
-                                                         double* __restrict__ w) {
+__global__ void __launch_bounds__(THREADS) bisect_kernel(const __grid_constant__ EigTable tab) {
+  const EigProb& PR = tab.p[blockIdx.y];
+  const double* __restrict__ d = PR.d;
+  const double* __restrict__ e = PR.e;
+  const int n = PR.n, i0 = PR.n - PR.kt, cnt = PR.kt;
+  const double* __restrict__ bnd = PR.bnd;
+  double* __restrict__ w = PR.w;
   extern __shared__ double sh[];
   double* sd = sh;
   double* se2 = sh + n;
@@ -604,11 +630,15 @@ __device__ __forceinline__ double hash_unit(uint32_t a, uint32_t b) {
 // d, e are staged in shared memory; every sequential loop loads the next CH
 // steps' independent inputs before running their dependent chain.
 constexpr int IV_THREADS = 128, CH = 8;
-__global__ void __launch_bounds__(IV_THREADS) inviter_kernel(const double* __restrict__ d,
-                                                             const double* __restrict__ e, int n, int cnt,
-                                                             const double* __restrict__ w,
-                                                             const double* __restrict__ bnd, double* __restrict__ Z,
-                                                             double* __restrict__ scr) {
+__global__ void __launch_bounds__(IV_THREADS) inviter_kernel(const __grid_constant__ EigTable tab) {
+  const EigProb& PR = tab.p[blockIdx.y];
+  const double* __restrict__ d = PR.d;
+  const double* __restrict__ e = PR.e;
+  const int n = PR.n, cnt = PR.kt;
+  const double* __restrict__ w = PR.w;
+  const double* __restrict__ bnd = PR.bnd;
+  double* __restrict__ Z = PR.z;
+  double* __restrict__ scr = PR.scr;
   extern __shared__ double sh_de[];
   double* sd = sh_de;
   double* se = sh_de + n;
@@ -884,29 +914,36 @@ int heev_attrs(reno_ctx* ctx) {
   return rc;
 }
 
-// tridiagonal reduction of a small matrix (n <= NMAX_C): one thread-block cluster
-int heev_reduce_small(reno_ctx* ctx, int n, void* A, double* d, double* e, void* tau) {
+// tridiagonal reduction of small matrices (n <= NMAX_C): one thread-block
+// cluster per matrix, all in one launch
+int heev_reduce_small(reno_ctx* ctx, const EigTable& tab, int nmax) {
+  if (tab.count == 0) return RENO_OK;
   count_launch();
-  hetrd_cluster_kernel<<<dim3(CL, 1), CT, cluster_smem_bytes(n), ctx->stream>>>(
-      static_cast<const double2*>(A), static_cast<double2*>(A), n, d, e, static_cast<double2*>(tau));
+  hetrd_cluster_kernel<<<dim3(CL, tab.count), CT, cluster_smem_bytes(nmax), ctx->stream>>>(tab);
   RENO_LAUNCH_CHECK(ctx, "reno_heev_top: cluster hetrd");
   return RENO_OK;
 }
 
-// eigenvalues n-kt .. n-1 of T (ascending) and their inverse-iteration vectors
-int heev_eig(reno_ctx* ctx, int n, int kt, const double* d, const double* e, double* w, double* Z, double* bnd,
-             double* scr) {
+// eigenvalues n-kt .. n-1 of every T (ascending) and their inverse-iteration
+// vectors: one launch per stage for all matrices of the table
+int heev_eig(reno_ctx* ctx, const EigTable& tab) {
+  if (tab.count == 0) return RENO_OK;
+  int nmax = 1, ktmax = 1;
+  for (int i = 0; i < tab.count; ++i) {
+    nmax = std::max(nmax, tab.p[i].n);
+    ktmax = std::max(ktmax, tab.p[i].kt);
+  }
   cudaStream_t st = ctx->stream;
   count_launch();
-  bounds_kernel<<<1, THREADS, 0, st>>>(d, e, n, bnd);
+  bounds_kernel<<<dim3(1, tab.count), THREADS, 0, st>>>(tab);
   RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bounds");
   count_launch();
-  bisect_kernel<<<(unsigned)ceil_div(kt, WARPS), THREADS, 2 * (size_t)n * sizeof(double), st>>>(d, e, n, n - kt, kt,
-                                                                                                 bnd, w);
+  bisect_kernel<<<dim3((unsigned)ceil_div(ktmax, WARPS), tab.count), THREADS, 2 * (size_t)nmax * sizeof(double),
+                  st>>>(tab);
   RENO_LAUNCH_CHECK(ctx, "reno_heev_top: bisect");
   count_launch();
-  inviter_kernel<<<(unsigned)ceil_div(kt, IV_THREADS), IV_THREADS, 2 * (size_t)n * sizeof(double), st>>>(
-      d, e, n, kt, w, bnd, Z, scr);
+  inviter_kernel<<<dim3((unsigned)ceil_div(ktmax, IV_THREADS), tab.count), IV_THREADS,
+                   2 * (size_t)nmax * sizeof(double), st>>>(tab);
   RENO_LAUNCH_CHECK(ctx, "reno_heev_top: inverse iteration");
   return RENO_OK;
 }
@@ -942,8 +979,11 @@ extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, doub
   int rc = check_cuda(ctx, cudaMemsetAsync(sync, 0, sizeof(Sync), ctx->stream), "reno_heev_top: memset");
   if (rc == RENO_OK) rc = heev_attrs(ctx);
   if (rc != RENO_OK) return rc;
+  EigTable et{};
+  et.count = 1;
+  et.p[0] = EigProb{static_cast<double2*>(A), static_cast<double2*>(tau), d, e, n, kt, w, Z, bnd, scr};
   if (n <= NMAX_C) {
-    rc = heev_reduce_small(ctx, n, A, d, e, tau);
+    rc = heev_reduce_small(ctx, et, n);
   } else {
     HetrdTable tab{};
     tab.count = 1;
@@ -951,7 +991,7 @@ extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, doub
     rc = launch_hetrd(ctx, tab, n, "reno_heev_top");
   }
   if (rc != RENO_OK) return rc;
-  return heev_eig(ctx, n, kt, d, e, w, Z, bnd, scr);
+  return heev_eig(ctx, et);
 }
 
 extern "C" int reno_heev_batched_workspace_bytes(int32_t count, const reno_heev_problem* probs, size_t* bytes) {
@@ -979,7 +1019,8 @@ extern "C" int reno_heev_top_batched(reno_ctx* ctx, int32_t count, const reno_he
   int rc = heev_attrs(ctx);
   if (rc != RENO_OK) return rc;
   HetrdTable tab{};
-  int nmax = 0;
+  EigTable small{}, all{};
+  int nmax = 0, nsmall = 1;
   for (int i = 0; i < count; ++i) {
     const reno_heev_problem& p = probs[i];
     char* base = static_cast<char*>(ws) + batched_offset(count, probs, i);
@@ -987,9 +1028,12 @@ extern "C" int reno_heev_top_batched(reno_ctx* ctx, int32_t count, const reno_he
     Sync* sync = reinterpret_cast<Sync*>(base + L.sync);
     rc = check_cuda(ctx, cudaMemsetAsync(sync, 0, sizeof(Sync), ctx->stream), "reno_heev_top_batched: memset");
     if (rc != RENO_OK) return rc;
+    const EigProb ep{static_cast<double2*>(p.a), static_cast<double2*>(p.tau), p.d, p.e, p.n, p.kt, p.w, p.z,
+                     reinterpret_cast<double*>(base + L.bnd), reinterpret_cast<double*>(base + L.scr)};
+    all.p[all.count++] = ep;
     if (p.n <= NMAX_C) {
-      rc = heev_reduce_small(ctx, p.n, p.a, p.d, p.e, p.tau);
-      if (rc != RENO_OK) return rc;
+      small.p[small.count++] = ep;
+      nsmall = std::max(nsmall, (int)p.n);
     } else {
       tab.p[tab.count++] = HetrdProb{static_cast<double2*>(p.a), p.n, p.d, p.e, static_cast<double2*>(p.tau),
                                      reinterpret_cast<double2*>(base + L.y), reinterpret_cast<double2*>(base + L.p),
@@ -997,169 +1041,22 @@ extern "C" int reno_heev_top_batched(reno_ctx* ctx, int32_t count, const reno_he
       nmax = std::max(nmax, (int)p.n);
     }
   }
+  rc = heev_reduce_small(ctx, small, nsmall);
+  if (rc != RENO_OK) return rc;
   if (tab.count) {
     rc = launch_hetrd(ctx, tab, nmax, "reno_heev_top_batched");
     if (rc != RENO_OK) return rc;
   }
-  for (int i = 0; i < count; ++i) {
-    const reno_heev_problem& p = probs[i];
-    char* base = static_cast<char*>(ws) + batched_offset(count, probs, i);
-    const HeevLayout L = heev_layout(p.n, p.kt);
-    rc = heev_eig(ctx, p.n, p.kt, p.d, p.e, p.w, p.z, reinterpret_cast<double*>(base + L.bnd),
-                  reinterpret_cast<double*>(base + L.scr));
-    if (rc == RENO_OK)
-      rc = check_cuda(ctx, cudaMemcpyAsync(status + i, base + L.sync + offsetof(Sync, status), sizeof(int32_t),
-                                           cudaMemcpyDeviceToDevice, ctx->stream),
-                      "reno_heev_top_batched: status");
-    if (rc != RENO_OK) return rc;
-  }
-  return RENO_OK;
-}
-
-// K (n x kt complex128, in: eigenvectors of T, out: Q K) after reno_heev_top
-// on the same A, tau and workspace; A's reflector rows are cleaned in place.
-extern "C" int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, void* A, const void* tau, void* K,
-                                       void* ws, size_t ws_bytes) {
-  if (!ctx) return RENO_ERR_INVALID;
-  if (n < 1 || n > MAX_N || kt < 1 || kt > n || !A || !tau || !K || !ws)
-    return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform: invalid arguments");
-  const HeevLayout L = heev_layout(n, kt);
-  if (ws_bytes < L.total) return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heev_backtransform: workspace too small");
-  if (n == 1) return RENO_OK;
-  char* base = static_cast<char*>(ws);
-  double2* Sg = reinterpret_cast<double2*>(base + L.s);
-  double2* Tg = reinterpret_cast<double2*>(base + L.t);
-  double2* W1 = reinterpret_cast<double2*>(base + L.w1);
-  double2* W2 = reinterpret_cast<double2*>(base + L.w2);
-  double2* V = static_cast<double2*>(A);
-  double2* Kc = static_cast<double2*>(K);
-  cudaStream_t st = ctx->stream;
-  const int nblk = (int)ceil_div(n - 1, NB);
-  const int rep = nch_max(n);
-  const size_t nel = (size_t)n * n;
-  count_launch();
-  clean_v_kernel<<<(unsigned)ceil_div((int64_t)nel, 256), 256, 0, st>>>(V, n);
-  RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: clean");
-  int rc = check_cuda(ctx, cudaMemsetAsync(Sg, 0, (size_t)nblk * NB * NB * sizeof(double2), st),
-                      "reno_heev_backtransform: memset");
+  rc = heev_eig(ctx, all);
   if (rc != RENO_OK) return rc;
-  // S_b = V_b^H V_b: the blocks of NB reflectors in one batched GEMM over all
-  // n columns (zeros before each row's reflector), a partial last block apart
-  const int nfull = (n - 1) / NB;
-  if (nfull > 0) {
-    GemmParams p;
-    p.M = NB;
-    p.N = NB;
-    p.K = n;
-    p.batch = nfull;
-    p.A = op(V, n, 1, 1);
-    p.A.s_batch = (int64_t)NB * n;
-    p.B = op(V, n, 1, 0);
-    p.B.s_batch = (int64_t)NB * n;
-    p.C = Sg;
-    p.sCm = NB;
-    p.sCn = 1;
-    p.sCb = (int64_t)NB * NB;
-    count_launch();
-    rc = check_cuda(ctx, gemm_fp64(p, st), "reno_heev_backtransform: gram");
+  for (int i = 0; i < count; ++i) {
+    char* base = static_cast<char*>(ws) + batched_offset(count, probs, i);
+    const HeevLayout L = heev_layout(probs[i].n, probs[i].kt);
+    rc = check_cuda(ctx, cudaMemcpyAsync(status + i, base + L.sync + offsetof(Sync, status), sizeof(int32_t),
+                                         cudaMemcpyDeviceToDevice, ctx->stream),
+                    "reno_heev_top_batched: status");
     if (rc != RENO_OK) return rc;
   }
-  if (nfull < nblk) {
-    const int k0 = nfull * NB, kb = n - 1 - k0;
-    GemmParams p;
-    p.M = kb;
-    p.N = kb;
-    p.K = n;
-    p.A = op(V + (size_t)k0 * n, n, 1, 1);
-    p.B = op(V + (size_t)k0 * n, n, 1, 0);
-    p.C = Sg + (size_t)nfull * NB * NB;
-    p.sCm = NB;
-    p.sCn = 1;
-    count_launch();
-    rc = check_cuda(ctx, gemm_fp64(p, st), "reno_heev_backtransform: gram (last block)");
-    if (rc != RENO_OK) return rc;
-  }
-  count_launch();
-  larft_kernel<<<nblk, NB, 0, st>>>(Sg, static_cast<const double2*>(tau), Tg, n, rep);
-  RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: larft");
-  for (int b = nblk - 1; b >= 0; --b) {
-    const int k0 = b * NB, kb = std::min(NB, n - 1 - k0);
-    const int rows = n - k0 - 1;
-    const int nfc = rows / KCH, rem = rows % KCH, nch = nfc + (rem > 0);
-    const double2* Vb = V + (size_t)k0 * n + k0 + 1;
-    double2* Kb = Kc + (size_t)(k0 + 1) * kt;
-    if (kb < NB) {
-      rc = check_cuda(ctx, cudaMemsetAsync(W1, 0, (size_t)nch * NB * kt * sizeof(double2), st),
-                      "reno_heev_backtransform: memset W1");
-      if (rc != RENO_OK) return rc;
-    }
-    // W1[s] = V_b^H K over row chunk s (split K: one batch entry per full chunk)
-    if (nfc > 0) {
-      GemmParams p1;
-      p1.M = kb;
-      p1.N = kt;
-      p1.K = KCH;
-      p1.batch = nfc;
-      p1.A = op(Vb, n, 1, 1);
-      p1.A.s_batch = KCH;
-      p1.B = op(Kb, 1, kt, 0);
-      p1.B.s_batch = (int64_t)KCH * kt;
-      p1.C = W1;
-      p1.sCm = kt;
-      p1.sCn = 1;
-      p1.sCb = (int64_t)NB * kt;
-      count_launch();
-      rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K");
-      if (rc != RENO_OK) return rc;
-    }
-    if (rem > 0) {
-      GemmParams p1;
-      p1.M = kb;
-      p1.N = kt;
-      p1.K = rem;
-      p1.A = op(Vb + (size_t)nfc * KCH, n, 1, 1);
-      p1.B = op(Kb + (size_t)nfc * KCH * kt, 1, kt, 0);
-      p1.C = W1 + (size_t)nfc * NB * kt;
-      p1.sCm = kt;
-      p1.sCn = 1;
-      count_launch();
-      rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K (last chunk)");
-      if (rc != RENO_OK) return rc;
-    }
-    // W2 = (-T_b) sum_s W1[s]: -T_b replicated along K
-    GemmParams p2;
-    p2.M = kb;
-    p2.N = kt;
-    p2.K = NB * nch;
-    p2.A = op(Tg + (size_t)b * NB * NB * rep, (int64_t)NB * rep, 1, 0);
-    p2.B = op(W1, 1, kt, 0);
-    p2.C = W2;
-    p2.sCm = kt;
-    p2.sCn = 1;
-    // K[k0+1:] += V_b W2
-    GemmParams p3;
-    p3.M = rows;
-    p3.N = kt;
-    p3.K = kb;
-    p3.A = op(Vb, 1, n, 0);
-    p3.B = op(W2, 1, kt, 0);
-    p3.C = Kb;
-    p3.sCm = kt;
-    p3.sCn = 1;
-    p3.accumulate = 1;
-    count_launch(2);
-    rc = check_cuda(ctx, gemm_fp64(p2, st), "reno_heev_backtransform: T W");
-    if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64(p3, st), "reno_heev_backtransform: K += V W");
-    if (rc != RENO_OK) return rc;
-  }
-  return RENO_OK;
-}
-
-// status word of the last reno_heev_top on a workspace: the int at this
-// byte offset of ws (0 = ok, 1 = a grid barrier timed out)
-extern "C" int reno_heev_status_offset(size_t* offset) {
-  if (!offset) return RENO_ERR_INVALID;
-  *offset = offsetof(Sync, status);
   return RENO_OK;
 }
 
