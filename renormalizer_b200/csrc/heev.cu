@@ -1060,6 +1060,153 @@ extern "C" int reno_heev_top_batched(reno_ctx* ctx, int32_t count, const reno_he
   return RENO_OK;
 }
 
+// K (n x kt complex128, in: eigenvectors of T, out: Q K) after reno_heev_top
+// on the same A, tau and workspace; A's reflector rows are cleaned in place.
+extern "C" int reno_heev_backtransform(reno_ctx* ctx, int32_t n, int32_t kt, void* A, const void* tau, void* K,
+                                       void* ws, size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (n < 1 || n > MAX_N || kt < 1 || kt > n || !A || !tau || !K || !ws)
+    return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform: invalid arguments");
+  const HeevLayout L = heev_layout(n, kt);
+  if (ws_bytes < L.total) return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heev_backtransform: workspace too small");
+  if (n == 1) return RENO_OK;
+  char* base = static_cast<char*>(ws);
+  double2* Sg = reinterpret_cast<double2*>(base + L.s);
+  double2* Tg = reinterpret_cast<double2*>(base + L.t);
+  double2* W1 = reinterpret_cast<double2*>(base + L.w1);
+  double2* W2 = reinterpret_cast<double2*>(base + L.w2);
+  double2* V = static_cast<double2*>(A);
+  double2* Kc = static_cast<double2*>(K);
+  cudaStream_t st = ctx->stream;
+  const int nblk = (int)ceil_div(n - 1, NB);
+  const int rep = nch_max(n);
+  const size_t nel = (size_t)n * n;
+  count_launch();
+  clean_v_kernel<<<(unsigned)ceil_div((int64_t)nel, 256), 256, 0, st>>>(V, n);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: clean");
+  int rc = check_cuda(ctx, cudaMemsetAsync(Sg, 0, (size_t)nblk * NB * NB * sizeof(double2), st),
+                      "reno_heev_backtransform: memset");
+  if (rc != RENO_OK) return rc;
+  // S_b = V_b^H V_b: the blocks of NB reflectors in one batched GEMM over all
+  // n columns (zeros before each row's reflector), a partial last block apart
+  const int nfull = (n - 1) / NB;
+  if (nfull > 0) {
+    GemmParams p;
+    p.M = NB;
+    p.N = NB;
+    p.K = n;
+    p.batch = nfull;
+    p.A = op(V, n, 1, 1);
+    p.A.s_batch = (int64_t)NB * n;
+    p.B = op(V, n, 1, 0);
+    p.B.s_batch = (int64_t)NB * n;
+    p.C = Sg;
+    p.sCm = NB;
+    p.sCn = 1;
+    p.sCb = (int64_t)NB * NB;
+    count_launch();
+    rc = check_cuda(ctx, gemm_fp64(p, st), "reno_heev_backtransform: gram");
+    if (rc != RENO_OK) return rc;
+  }
+  if (nfull < nblk) {
+    const int k0 = nfull * NB, kb = n - 1 - k0;
+    GemmParams p;
+    p.M = kb;
+    p.N = kb;
+    p.K = n;
+    p.A = op(V + (size_t)k0 * n, n, 1, 1);
+    p.B = op(V + (size_t)k0 * n, n, 1, 0);
+    p.C = Sg + (size_t)nfull * NB * NB;
+    p.sCm = NB;
+    p.sCn = 1;
+    count_launch();
+    rc = check_cuda(ctx, gemm_fp64(p, st), "reno_heev_backtransform: gram (last block)");
+    if (rc != RENO_OK) return rc;
+  }
+  count_launch();
+  larft_kernel<<<nblk, NB, 0, st>>>(Sg, static_cast<const double2*>(tau), Tg, n, rep);
+  RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform: larft");
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int k0 = b * NB, kb = std::min(NB, n - 1 - k0);
+    const int rows = n - k0 - 1;
+    const int nfc = rows / KCH, rem = rows % KCH, nch = nfc + (rem > 0);
+    const double2* Vb = V + (size_t)k0 * n + k0 + 1;
+    double2* Kb = Kc + (size_t)(k0 + 1) * kt;
+    if (kb < NB) {
+      rc = check_cuda(ctx, cudaMemsetAsync(W1, 0, (size_t)nch * NB * kt * sizeof(double2), st),
+                      "reno_heev_backtransform: memset W1");
+      if (rc != RENO_OK) return rc;
+    }
+    // W1[s] = V_b^H K over row chunk s (split K: one batch entry per full chunk)
+    if (nfc > 0) {
+      GemmParams p1;
+      p1.M = kb;
+      p1.N = kt;
+      p1.K = KCH;
+      p1.batch = nfc;
+      p1.A = op(Vb, n, 1, 1);
+      p1.A.s_batch = KCH;
+      p1.B = op(Kb, 1, kt, 0);
+      p1.B.s_batch = (int64_t)KCH * kt;
+      p1.C = W1;
+      p1.sCm = kt;
+      p1.sCn = 1;
+      p1.sCb = (int64_t)NB * kt;
+      count_launch();
+      rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K");
+      if (rc != RENO_OK) return rc;
+    }
+    if (rem > 0) {
+      GemmParams p1;
+      p1.M = kb;
+      p1.N = kt;
+      p1.K = rem;
+      p1.A = op(Vb + (size_t)nfc * KCH, n, 1, 1);
+      p1.B = op(Kb + (size_t)nfc * KCH * kt, 1, kt, 0);
+      p1.C = W1 + (size_t)nfc * NB * kt;
+      p1.sCm = kt;
+      p1.sCn = 1;
+      count_launch();
+      rc = check_cuda(ctx, gemm_fp64(p1, st), "reno_heev_backtransform: V^H K (last chunk)");
+      if (rc != RENO_OK) return rc;
+    }
+    // W2 = (-T_b) sum_s W1[s]: -T_b replicated along K
+    GemmParams p2;
+    p2.M = kb;
+    p2.N = kt;
+    p2.K = NB * nch;
+    p2.A = op(Tg + (size_t)b * NB * NB * rep, (int64_t)NB * rep, 1, 0);
+    p2.B = op(W1, 1, kt, 0);
+    p2.C = W2;
+    p2.sCm = kt;
+    p2.sCn = 1;
+    // K[k0+1:] += V_b W2
+    GemmParams p3;
+    p3.M = rows;
+    p3.N = kt;
+    p3.K = kb;
+    p3.A = op(Vb, 1, n, 0);
+    p3.B = op(W2, 1, kt, 0);
+    p3.C = Kb;
+    p3.sCm = kt;
+    p3.sCn = 1;
+    p3.accumulate = 1;
+    count_launch(2);
+    rc = check_cuda(ctx, gemm_fp64(p2, st), "reno_heev_backtransform: T W");
+    if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64(p3, st), "reno_heev_backtransform: K += V W");
+    if (rc != RENO_OK) return rc;
+  }
+  return RENO_OK;
+}
+
+// status word of the last reno_heev_top on a workspace: the int at this
+// byte offset of ws (0 = ok, 1 = a grid barrier timed out)
+extern "C" int reno_heev_status_offset(size_t* offset) {
+  if (!offset) return RENO_ERR_INVALID;
+  *offset = offsetof(Sync, status);
+  return RENO_OK;
+}
+
 // reno_heev_backtransform for every problem of a reno_heev_top_batched call
 // (same problems and workspace): K_i <- Q_i K_i.
 extern "C" int reno_heev_backtransform_batched(reno_ctx* ctx, int32_t count, const reno_heev_problem* probs,
