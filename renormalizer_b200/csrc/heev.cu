@@ -30,6 +30,7 @@
 // returns; the others return at their next barrier.
 #include <algorithm>
 #include <cfloat>
+#include <vector>
 #include <cstddef>
 #include "reno_common.cuh"
 #include "gemm_fp64.cuh"
@@ -1208,7 +1209,10 @@ extern "C" int reno_heev_status_offset(size_t* offset) {
 }
 
 // reno_heev_backtransform for every problem of a reno_heev_top_batched call
-// (same problems and workspace): K_i <- Q_i K_i.
+// (same problems and workspace): K_i <- Q_i K_i.  The GEMMs of all problems
+// run as grouped launches: the Grams of the reflector blocks in one launch,
+// then, for the blocks of NB reflectors from the last, one launch each for
+// V_b^H K, (-T_b) W1 and K += V_b W2 over every problem that has block b.
 extern "C" int reno_heev_backtransform_batched(reno_ctx* ctx, int32_t count, const reno_heev_problem* probs,
                                                void* ws, size_t ws_bytes) {
   if (!ctx) return RENO_ERR_INVALID;
@@ -1216,13 +1220,153 @@ extern "C" int reno_heev_backtransform_batched(reno_ctx* ctx, int32_t count, con
     return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform_batched: invalid batch");
   if (ws_bytes < batched_offset(count, probs, count))
     return set_error(ctx, RENO_ERR_WORKSPACE, "reno_heev_backtransform_batched: workspace too small");
+  cudaStream_t st = ctx->stream;
+  struct One {
+    int n, kt, nblk, rep;
+    double2 *V, *K, *Sg, *Tg, *W1, *W2;
+    const double2* tau;
+  };
+  std::vector<One> P;
+  int rc = RENO_OK;
+  static_assert(2 * RENO_HEEV_MAX_BATCH < fp64gemm::MAX_GROUP, "one block step of a batch fits one group");
+  auto flush = [&](fp64gemm::GemmGroup& g, const char* what) -> int {
+    if (g.count == 0) return RENO_OK;
+    const int r = check_cuda(ctx, gemm_fp64_grouped(g, st), what);
+    g.count = 0;
+    return r;
+  };
+  auto add = [&](fp64gemm::GemmGroup& g, const GemmParams& q, const char* what) -> int {
+    g.p[g.count++] = q;
+    return g.count == fp64gemm::MAX_GROUP ? flush(g, what) : RENO_OK;
+  };
   for (int i = 0; i < count; ++i) {
     const reno_heev_problem& p = probs[i];
-    if (!p.k) return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform_batched: null K");
-    const size_t off = batched_offset(count, probs, i);
-    const int rc = reno_heev_backtransform(ctx, p.n, p.kt, p.a, p.tau, p.k, static_cast<char*>(ws) + off,
-                                           heev_layout(p.n, p.kt).total);
+    if (!p.k || !p.a || !p.tau) return set_error(ctx, RENO_ERR_INVALID, "reno_heev_backtransform_batched: null");
+    if (p.n < 2) continue;
+    char* base = static_cast<char*>(ws) + batched_offset(count, probs, i);
+    const HeevLayout L = heev_layout(p.n, p.kt);
+    One o{p.n, p.kt, (int)ceil_div(p.n - 1, NB), nch_max(p.n), static_cast<double2*>(p.a),
+          static_cast<double2*>(p.k), reinterpret_cast<double2*>(base + L.s), reinterpret_cast<double2*>(base + L.t),
+          reinterpret_cast<double2*>(base + L.w1), reinterpret_cast<double2*>(base + L.w2),
+          static_cast<const double2*>(p.tau)};
+    count_launch();
+    clean_v_kernel<<<(unsigned)ceil_div((int64_t)o.n * o.n, 256), 256, 0, st>>>(o.V, o.n);
+    RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform_batched: clean");
+    rc = check_cuda(ctx, cudaMemsetAsync(o.Sg, 0, (size_t)o.nblk * NB * NB * sizeof(double2), st),
+                    "reno_heev_backtransform_batched: memset");
     if (rc != RENO_OK) return rc;
+    P.push_back(o);
+  }
+  if (P.empty()) return RENO_OK;
+  // S_b = V_b^H V_b of every problem (full blocks batched, the partial last block apart)
+  fp64gemm::GemmGroup g1, g2, g3;
+  for (const One& o : P) {
+    const int nfull = (o.n - 1) / NB;
+    if (nfull > 0) {
+      GemmParams q;
+      q.M = NB;
+      q.N = NB;
+      q.K = o.n;
+      q.batch = nfull;
+      q.A = op(o.V, o.n, 1, 1);
+      q.A.s_batch = (int64_t)NB * o.n;
+      q.B = op(o.V, o.n, 1, 0);
+      q.B.s_batch = (int64_t)NB * o.n;
+      q.C = o.Sg;
+      q.sCm = NB;
+      q.sCn = 1;
+      q.sCb = (int64_t)NB * NB;
+      if ((rc = add(g1, q, "reno_heev_backtransform_batched: gram")) != RENO_OK) return rc;
+    }
+    if (nfull < o.nblk) {
+      const int k0 = nfull * NB, kb = o.n - 1 - k0;
+      GemmParams q;
+      q.M = kb;
+      q.N = kb;
+      q.K = o.n;
+      q.A = op(o.V + (size_t)k0 * o.n, o.n, 1, 1);
+      q.B = op(o.V + (size_t)k0 * o.n, o.n, 1, 0);
+      q.C = o.Sg + (size_t)nfull * NB * NB;
+      q.sCm = NB;
+      q.sCn = 1;
+      if ((rc = add(g1, q, "reno_heev_backtransform_batched: gram")) != RENO_OK) return rc;
+    }
+  }
+  if ((rc = flush(g1, "reno_heev_backtransform_batched: gram")) != RENO_OK) return rc;
+  int bmax = 0;
+  for (const One& o : P) {
+    count_launch();
+    larft_kernel<<<o.nblk, NB, 0, st>>>(o.Sg, o.tau, o.Tg, o.n, o.rep);
+    RENO_LAUNCH_CHECK(ctx, "reno_heev_backtransform_batched: larft");
+    bmax = std::max(bmax, o.nblk);
+  }
+  // blocks of reflectors from the last: every problem with block b advances together
+  for (int b = bmax - 1; b >= 0; --b) {
+    for (const One& o : P) {
+      if (b >= o.nblk) continue;
+      const int k0 = b * NB, kb = std::min(NB, o.n - 1 - k0);
+      const int rows = o.n - k0 - 1;
+      const int nfc = rows / KCH, rem = rows % KCH, nch = nfc + (rem > 0);
+      const double2* Vb = o.V + (size_t)k0 * o.n + k0 + 1;
+      double2* Kb = o.K + (size_t)(k0 + 1) * o.kt;
+      if (kb < NB) {
+        rc = check_cuda(ctx, cudaMemsetAsync(o.W1, 0, (size_t)nch * NB * o.kt * sizeof(double2), st),
+                        "reno_heev_backtransform_batched: memset W1");
+        if (rc != RENO_OK) return rc;
+      }
+      if (nfc > 0) {  // W1[s] = V_b^H K over row chunk s
+        GemmParams q;
+        q.M = kb;
+        q.N = o.kt;
+        q.K = KCH;
+        q.batch = nfc;
+        q.A = op(Vb, o.n, 1, 1);
+        q.A.s_batch = KCH;
+        q.B = op(Kb, 1, o.kt, 0);
+        q.B.s_batch = (int64_t)KCH * o.kt;
+        q.C = o.W1;
+        q.sCm = o.kt;
+        q.sCn = 1;
+        q.sCb = (int64_t)NB * o.kt;
+        if ((rc = add(g1, q, "reno_heev_backtransform_batched: V^H K")) != RENO_OK) return rc;
+      }
+      if (rem > 0) {
+        GemmParams q;
+        q.M = kb;
+        q.N = o.kt;
+        q.K = rem;
+        q.A = op(Vb + (size_t)nfc * KCH, o.n, 1, 1);
+        q.B = op(Kb + (size_t)nfc * KCH * o.kt, 1, o.kt, 0);
+        q.C = o.W1 + (size_t)nfc * NB * o.kt;
+        q.sCm = o.kt;
+        q.sCn = 1;
+        if ((rc = add(g1, q, "reno_heev_backtransform_batched: V^H K")) != RENO_OK) return rc;
+      }
+      GemmParams q2;  // W2 = (-T_b) sum_s W1[s]
+      q2.M = kb;
+      q2.N = o.kt;
+      q2.K = NB * nch;
+      q2.A = op(o.Tg + (size_t)b * NB * NB * o.rep, (int64_t)NB * o.rep, 1, 0);
+      q2.B = op(o.W1, 1, o.kt, 0);
+      q2.C = o.W2;
+      q2.sCm = o.kt;
+      q2.sCn = 1;
+      if ((rc = add(g2, q2, "reno_heev_backtransform_batched: T W")) != RENO_OK) return rc;
+      GemmParams q3;  // K[k0+1:] += V_b W2
+      q3.M = rows;
+      q3.N = o.kt;
+      q3.K = kb;
+      q3.A = op(Vb, 1, o.n, 0);
+      q3.B = op(o.W2, 1, o.kt, 0);
+      q3.C = Kb;
+      q3.sCm = o.kt;
+      q3.sCn = 1;
+      q3.accumulate = 1;
+      if ((rc = add(g3, q3, "reno_heev_backtransform_batched: K += V W")) != RENO_OK) return rc;
+    }
+    if ((rc = flush(g1, "reno_heev_backtransform_batched: V^H K")) != RENO_OK) return rc;
+    if ((rc = flush(g2, "reno_heev_backtransform_batched: T W")) != RENO_OK) return rc;
+    if ((rc = flush(g3, "reno_heev_backtransform_batched: K += V W")) != RENO_OK) return rc;
   }
   return RENO_OK;
 }
