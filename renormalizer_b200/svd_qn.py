@@ -300,6 +300,34 @@ class SubspaceOptions:
 
 
 subspace = SubspaceOptions()
+
+
+class RefineOptions:
+    """Second pass for the small singular values of a block.
+
+    The Gram matrix carries absolute rounding errors of about eps ||X||^2, so
+    its eigenvectors for sigma below ~sqrt(eps) ||X|| are mixed within that
+    cluster, and the projected norms ||u^H X|| of such mixtures lie anywhere
+    in the cluster's range.  When the truncation's cut (the smallest selected
+    sigma) lies below ``tau`` times the largest sigma, every block whose
+    projected sigma include values below ``tau`` times its own largest is
+    refined: its cluster rows of P (sigma-scaled singular vectors, mutually
+    orthogonal to within eps sigma_i sigma_j) are projected twice onto the
+    complement of its other rows, the small Gram matrix of what remains
+    (entries of order sigma_cluster^2, accurate to eps relative) goes through
+    the device eigensolver, and its eigenvectors rotate the cluster's kept
+    basis and rows (K P is unchanged).  The refined sigma are accurate to
+    about sqrt(eps) tau ||X|| instead of sqrt(eps) ||X||.  ``tau`` = 0 turns
+    the pass off."""
+
+    def __init__(self, tau=1e-5):
+        env = os.environ.get("RENO_REFINE_TAU")
+        self.tau = float(env) if env else tau
+        self.calls = 0
+        self.blocks = 0
+
+
+refine = RefineOptions()
 # when a list, svd_truncate appends the algorithmic FP64 flops of each call's
 # block factorisations (see _block_flops)
 flop_log = None
@@ -632,6 +660,79 @@ def _trunc_host_tensors(st):
         [b["chk"] for b in blocks if "chk" in b]
 
 
+def _refine_clusters(eng: Engine, blocks, keep_left: bool) -> bool:
+    """The RefineOptions pass over the blocks of one truncation (host sigma
+    ``Sh`` already known): all cluster Gram matrices in one device
+    eigensolver call, their checks and refined sigma in one host transfer.
+    Returns whether any block was refined."""
+    todo = []
+    for b in blocks:
+        kt = b["K"].shape[1]
+        head = np.asarray(b["Sh"][:kt], dtype=np.float64)
+        if kt < 2 or not np.all(np.isfinite(head)) or head.max() <= 0:
+            continue
+        cl = np.nonzero(head < refine.tau * head.max())[0]
+        if len(cl) == 0:
+            continue
+        lg = np.nonzero(head >= refine.tau * head.max())[0]
+        dev = b["S"].device
+        ic, il = _i64(cl, dev), _i64(lg, dev)
+        Z = b["P"] if keep_left else b["P"].transpose(0, 1).conj()
+        Zc, Zl = Z.index_select(0, ic), Z.index_select(0, il)
+        sl2 = b["S"].index_select(0, il) ** 2
+        for _ in range(2):
+            coef = eng.matmul(Zc, Zl.transpose(0, 1), conj_b=True) / sl2[None, :]
+            Zc = Zc - eng.matmul(coef, Zl)
+        C = eng.matmul(Zc, Zc.transpose(0, 1), conj_b=True)
+        scale = torch.clamp(torch.diagonal(C).real.sum(), min=1e-300)
+        todo.append(dict(b=b, cl=cl, ic=ic, C=(C / scale).contiguous(), scale=scale))
+    if not todo:
+        return False
+    refine.calls += 1
+    refine.blocks += len(todo)
+    dev_idx = [i for i, t in enumerate(todo) if _device_eig_ok(t["C"])]
+    if dev_idx:
+        res = heev.heev_top_batched(eng, [todo[i]["C"] for i in dev_idx], [len(todo[i]["cl"]) for i in dev_idx])
+        for i, (w, R, chk) in zip(dev_idx, res):
+            todo[i].update(w=w, R=R if todo[i]["C"].is_complex() else R.real.contiguous(), chk=chk)
+    for t in todo:
+        if "R" not in t:
+            w, V = torch.linalg.eigh(t["C"])
+            t.update(w=torch.flip(w, dims=[0]), R=torch.flip(V, dims=[1]))
+        t["sig"] = torch.sqrt(torch.clamp(t["w"] * t["scale"], min=0.0))
+    host = torch.cat([t["sig"] for t in todo] + [t["chk"] for t in todo if "chk" in t]).cpu().numpy()
+    off = sum(len(t["cl"]) for t in todo)
+    for t in todo:
+        if "chk" in t:
+            if not heev.accepted(host[off:off + 3]):
+                heev.heev_opts.fallbacks += 1
+                w, V = torch.linalg.eigh(t["C"])
+                t.update(R=torch.flip(V, dims=[1]))
+                t["sig"] = torch.sqrt(torch.clamp(torch.flip(w, dims=[0]) * t["scale"], min=0.0))
+                t["sig_h"] = t["sig"].cpu().numpy()
+            off += 3
+    off = 0
+    for t in todo:
+        b, ic, R = t["b"], t["ic"], t["R"]
+        c = len(t["cl"])
+        sig_h = t.get("sig_h", host[off:off + c])
+        off += c
+        b["K"][:, ic] = eng.matmul(b["K"].index_select(1, ic), R)
+        if keep_left:
+            b["P"][ic] = eng.matmul(R.transpose(0, 1), b["P"].index_select(0, ic), conj_a=True)
+        else:
+            b["P"][:, ic] = eng.matmul(b["P"].index_select(1, ic), R)
+        b["S"][ic] = t["sig"]
+        Sh = np.array(b["Sh"], dtype=np.float64, copy=True)
+        Sh[t["cl"]] = sig_h
+        kt = b["K"].shape[1]
+        if len(Sh) > kt:
+            # unprojected tail values stay below every projected one
+            Sh[kt:] = np.minimum(Sh[kt:], Sh[:kt].min())
+        b["Sh"] = Sh
+    return True
+
+
 def _trunc_end(st, host):
     """Checks (redo of failed blocks), the reference's selection and the
     scatter of the kept columns, from the host copy of _trunc_host_tensors."""
@@ -682,22 +783,28 @@ def _trunc_end(st, host):
     # the zero-sigma paddings block by block (svd_qn.py:222-230)
     # (entry -> block bi, position j); block bi's QN is its code: the blocks'
     # sectors are distinct and appear in block order
-    sig = np.concatenate([np.asarray(b["Sh"][:b["dim"]], dtype=np.float64) for b in blocks] +
-                         [np.zeros(b["npad"]) for b in blocks])
     blk = np.concatenate([np.full(b["dim"], bi, dtype=np.int64) for bi, b in enumerate(blocks)] +
                          [np.full(b["npad"], bi, dtype=np.int64) for bi, b in enumerate(blocks)])
     pos = np.concatenate([np.arange(b["dim"], dtype=np.int64) for b in blocks] +
                          [b["dim"] + np.arange(b["npad"], dtype=np.int64) for b in blocks])
     qkey = [tuple(b["nl"] if keep_left else b["nr"]) for b in blocks]
     code_of = {q: bi for bi, q in enumerate(qkey)}
-    mtr = m_trunc_fn(sig)
     # the reference iterates set(qnlist) over the per-entry QN list in entry
     # order, where a block without nonzero entries first appears among the
     # paddings; inserting the distinct QNs in first-occurrence order builds
     # the same set (duplicates leave a set's table unchanged)
     _, first = np.unique(blk, return_index=True)
     visit_set = set(qkey[int(blk[i])] for i in np.sort(first))
-    sidx = _select_by_code(sig, blk, [code_of[q] for q in visit_set], mtr, percent)
+
+    def select():
+        sig = np.concatenate([np.asarray(b["Sh"][:b["dim"]], dtype=np.float64) for b in blocks] +
+                             [np.zeros(b["npad"]) for b in blocks])
+        return sig, _select_by_code(sig, blk, [code_of[q] for q in visit_set], m_trunc_fn(sig), percent)
+
+    sig, sidx = select()
+    if refine.tau > 0 and len(sidx) and sig.max() > 0 and sig[sidx].min() < 2 * refine.tau * sig.max():
+        if _refine_clusters(eng, blocks, keep_left):
+            sig, sidx = select()
     mdim = len(sidx)
     left = torch.zeros((rows, mdim), dtype=coef.dtype, device=coef.device)
     right = torch.zeros((mdim, cols), dtype=coef.dtype, device=coef.device)

@@ -6,9 +6,8 @@ with the shared-environment path (mps.py:527-575, 2103-2169).
 
 Tolerances: RDMs and expectations are contractions (1e-12 relative to the
 largest entry); the bond singular values go through an SVD sweep of a
-re-canonicalised copy, compared as sorted lists to 1e-10 absolute (sigma <= 1:
-values at the rounding floor of the Gram eigendecomposition, ~1e-11, are
-only defined to that level and differ between LAPACK and cuSOLVER);
+re-canonicalised copy, compared as sorted lists to 1e-12 absolute (sigma <= 1;
+the values below sqrt(eps) go through the truncation's cluster refinement);
 entropies to 1e-10."""
 import numpy as np
 import pytest
@@ -36,7 +35,7 @@ def _check(mps, ops):
     sv = mps.calc_bond_singular_values()
     ref = OBS["obs/bond_sv"]
     assert sv.shape == ref.shape
-    np.testing.assert_allclose(np.sort(sv, axis=1), np.sort(ref, axis=1), rtol=0, atol=1e-10)
+    np.testing.assert_allclose(np.sort(sv, axis=1), np.sort(ref, axis=1), rtol=0, atol=1e-12)
     np.testing.assert_allclose(mps.calc_bond_entropy(sv), OBS["obs/bond_entropy"], atol=1e-10)
     ref = OBS["obs/expectations"]
     for opt in (True, False):
