@@ -74,6 +74,9 @@ def parse():
                     help="--accuracy mode: also evolve FP64 from the start state perturbed by one ulp per entry "
                          "and report its distance from the unperturbed FP64 run (the FP64 engine's own envelope)")
     ap.add_argument("--out", default="", help="append the per-step JSON lines of --accuracy mode to this file")
+    ap.add_argument("--accuracy-lockstep", type=int, default=1,
+                    help="--accuracy mode: advance the FP64 reference and every arm together through "
+                         "evolve_batch (1, default) or one after another (0)")
     ap.add_argument("--truncation", default="exact", choices=["exact", "subspace"],
                     help="exact (default): every QN block uses the full Gram eigendecomposition; subspace: blocks "
                          "with at least 1024 rows on the smaller side use the opt-in top-k subspace iteration")
@@ -718,7 +721,7 @@ def run_accuracy(args):
     size of the FP64 engine's own trajectory spread).  Every step prints one
     JSON line (and appends it to --out)."""
     import torch
-    from renormalizer_b200 import Mpo, backend
+    from renormalizer_b200 import Mpo, backend, evolve_batch
     torch.cuda.set_device(0)
     model = holstein_2mode(args.nmol, args.nlev)
     mpo = Mpo(model)
@@ -742,14 +745,30 @@ def run_accuracy(args):
             out.flush()
 
     emit({"start": args.start, "start_s": t_start, "bond_dims": mps0.bond_dims, "nmol": args.nmol, "M": args.M,
-          "dt": args.dt, "arms": list(arms)})
+          "dt": args.dt, "arms": list(arms), "lockstep": bool(args.accuracy_lockstep)})
+    names = list(arms)
     for step in range(args.accuracy):
+        row = {"step": step + 1}
+        if args.accuracy_lockstep:
+            # every arm and the FP64 reference advance together (evolve_batch):
+            # their truncations share the batched eigensolver launches
+            t1 = time.time()
+            res = evolve_batch([ref] + [arms[k] for k in names], mpo, args.dt,
+                               precs=["fp64"] + ["fp64" if k == "fp64_ulp" else k for k in names])
+            ref = res[0]
+            arms = dict(zip(names, res[1:]))
+            step_s["lockstep"] = step_s.get("lockstep", 0.0) + time.time() - t1
+            pref = ref.e_occupations
+            for k in names:
+                row[k] = float(np.abs(arms[k].e_occupations - pref).max())
+                worst[k] = max(worst[k], row[k])
+            emit(row)
+            continue
         backend.prec = "fp64"
         t1 = time.time()
         ref = ref.evolve(mpo, args.dt)
         pref = ref.e_occupations
         step_s["fp64"] += time.time() - t1
-        row = {"step": step + 1}
         for k in arms:
             backend.prec = "fp64" if k == "fp64_ulp" else k
             t1 = time.time()
@@ -762,7 +781,7 @@ def run_accuracy(args):
     backend.prec = args.prec
     emit({"metric": "max |population(arm) - population(fp64)| over the trajectory", "workload": WORKLOAD,
           "nmol": args.nmol, "M": args.M, "dt": args.dt, "start": args.start, "steps": args.accuracy,
-          "max": worst, "s_per_step": {k: v / max(args.accuracy, 1) for k, v in step_s.items()}})
+          "max": worst, "s_per_step": {k: v / max(args.accuracy, 1) for k, v in step_s.items() if v}})
     if out:
         out.close()
 

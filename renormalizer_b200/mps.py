@@ -1031,7 +1031,7 @@ def compressed_sum(mps_list: List[Mps], batchsize=5, temp_m_trunc=None) -> Mps:
     return queue[0]
 
 
-def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True) -> List[Mps]:
+def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True, precs=None) -> List[Mps]:
     """Mps.evolve for many independent MPS at once (static-disorder
     realisations, each with its own MPO and bond dimensions; the reference
     evolves them one by one through mps.py:644-662).  Every instance runs its
@@ -1040,44 +1040,53 @@ def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True) -> Li
     (hop_expr.apply_grouped: one launch per contraction stage for all FP64
     problems), and the truncations pending at the same time share one
     batched eigensolver pass and one host transfer (svd_truncate_batch).
-    Each result equals that instance's own evolve."""
+    Each result equals that instance's own evolve.
+
+    ``precs`` (one contraction precision per instance, default the backend's)
+    runs each instance's matvecs and environment updates in its own
+    precision: every resumption of an instance's sweep runs under it."""
     from .hop_expr import apply_grouped
     from .krylov import expm_krylov_batch
     if isinstance(mpo_list, Mpo):
         mpo_list = [mpo_list] * len(mps_list)
     assert len(mpo_list) == len(mps_list)
+    assert precs is None or len(precs) == len(mps_list)
+    saved_prec = backend.prec
     gens = [m._evolve_steps(o, evolve_dt) for m, o in zip(mps_list, mpo_list)]
     out: List[Mps] = [None] * len(gens)
     pending = {}
-    for i, g in enumerate(gens):
+
+    def resume(i, val, into):
+        if precs is not None:
+            backend.prec = precs[i]
         try:
-            pending[i] = next(g)
+            into[i] = next(gens[i]) if val is None else gens[i].send(val)
         except StopIteration as stop:
             out[i] = stop.value
-    while pending:
-        nxt = {}
-        # truncations of this round: one batched pass over all their QN blocks
-        tidx = sorted(i for i in pending if isinstance(pending[i], TruncRequest))
-        if tidx:
-            res = svd_truncate_batch([pending[i].kwargs for i in tidx])
-            for i, r in zip(tidx, res):
-                try:
-                    nxt[i] = gens[i].send(r)
-                except StopIteration as stop:
-                    out[i] = stop.value
-        # local exponentials of this round in lockstep, grouped matvecs
-        idx = sorted(i for i in pending if not isinstance(pending[i], TruncRequest))
-        if idx:
-            reqs = [pending[i] for i in idx]
-            ops = [r[0] for r in reqs]
-            res = expm_krylov_batch(lambda sub, xs: apply_grouped([ops[k] for k in sub], xs), [r[1] for r in reqs],
-                                    [r[2].reshape(-1) for r in reqs])
-            for i, r in zip(idx, res):
-                try:
-                    nxt[i] = gens[i].send(r)
-                except StopIteration as stop:
-                    out[i] = stop.value
-        pending = nxt
+
+    try:
+        for i in range(len(gens)):
+            resume(i, None, pending)
+        while pending:
+            nxt = {}
+            # truncations of this round: one batched pass over all their QN blocks
+            tidx = sorted(i for i in pending if isinstance(pending[i], TruncRequest))
+            if tidx:
+                res = svd_truncate_batch([pending[i].kwargs for i in tidx])
+                for i, r in zip(tidx, res):
+                    resume(i, r, nxt)
+            # local exponentials of this round in lockstep, grouped matvecs
+            idx = sorted(i for i in pending if not isinstance(pending[i], TruncRequest))
+            if idx:
+                reqs = [pending[i] for i in idx]
+                ops = [r[0] for r in reqs]
+                res = expm_krylov_batch(lambda sub, xs: apply_grouped([ops[k] for k in sub], xs),
+                                        [r[1] for r in reqs], [r[2].reshape(-1) for r in reqs])
+                for i, r in zip(idx, res):
+                    resume(i, r, nxt)
+            pending = nxt
+    finally:
+        backend.prec = saved_prec
     if normalize:
         for m in out:
             m.normalize("mps_and_coeff" if np.iscomplex(evolve_dt) else "mps_only")

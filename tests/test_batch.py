@@ -148,3 +148,30 @@ def test_apply_grouped_dispatch_host_logic(cpu_engine, monkeypatch):
     assert all(len(cl) <= 20 for cl in calls)
     assert all(len({ns for ns, _ in cl}) == 1 and all(p == 0 for _, p in cl) for cl in calls)
     assert sum(len(cl) for cl in calls) == sum(1 for op in ops if op.prec == "fp64")
+
+
+@pytest.mark.parametrize("method", ["tdvp_ps2", "tdvp_ps"])
+def test_evolve_batch_per_instance_precision_host_logic(cpu_engine, monkeypatch, method):
+    """evolve_batch(precs=...) builds every local operator of an instance in
+    that instance's precision (realisations told apart by their phonon
+    dimension, 4 and 3) and leaves the backend's precision as it was"""
+    import importlib
+    from renormalizer_b200 import EvolveMethod, backend, evolve_batch
+    hop_expr = importlib.import_module("renormalizer_b200.hop_expr")
+    seen = []
+    orig = hop_expr.HeffOperator.__init__
+
+    def spy(self, *a, **k):
+        orig(self, *a, **k)
+        seen.append((tuple(self.cshape[1:-1]), self.prec))
+
+    monkeypatch.setattr(hop_expr.HeffOperator, "__init__", spy)
+    m = getattr(EvolveMethod, method)
+    (a, mpo_a), (b, mpo_b) = _realisation(0, m, nlev=4), _realisation(1, m, nlev=3)
+    backend.prec = "fp64"
+    evolve_batch([a, b], [mpo_a, mpo_b], 0.05, precs=["bf16x3", "fp64"])
+    assert backend.prec == "fp64"
+    by_a = [p for d, p in seen if 4 in d]
+    by_b = [p for d, p in seen if 3 in d]
+    assert by_a and by_b
+    assert set(by_a) == {"bf16x3"} and set(by_b) == {"fp64"}
