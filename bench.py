@@ -935,15 +935,22 @@ def run_grad(args):
     """16 molecules x (e, one mode omega = 1, 10 levels), J = 1, g_i ~ U(0.5, 1.5)
     (seed 5), exciton on molecule 0, bonds expanded to M = 64, 1-site TDVP-PS,
     50 steps of dt = 0.05 (t = 2.5), checkpoints every 10 steps.  Times the
-    engine gradient; checks it against torch autograd through FP64 tensordot
-    on the same device and against central differences (h = 1e-5 and 1e-3)
-    for the two largest couplings.  The trajectory itself carries ~1e-9 of
-    rounding amplification (the bond-expansion directions of the start state
-    are set by rounding), which bounds both checks."""
+    engine gradient of the site-0 population with respect to all 16 g_i and
+    checks every component against torch autograd through FP64 tensordot on
+    the same device and against central differences (h = 1e-5 and 1e-4,
+    all 32 perturbed trajectories of each h in one batched FP64 run).
+
+    The start is expand_bond_dimension(coef=1e-2) (the seeded random
+    expander at weight 1e-2): every bond direction then carries weight far
+    above rounding.  With the default coef = 1e-10 the padding directions'
+    orientation is set by rounding, the fixed-M trajectory amplifies that to
+    ~1e-9 in the population, and QR's backward applies R^-1 across those
+    directions; that start is reported beside it (population and the
+    engine-vs-autograd spread only)."""
     import torch
     from renormalizer_b200 import CompressConfig, CompressCriteria, HolsteinModel, Mol, Mpo, Mps, Phonon, Quantity, \
         backend
-    from renormalizer_b200.tdvp_grad import coupling_gradient, trajectory_value
+    from renormalizer_b200.tdvp_grad import coupling_gradient, trajectory_values
     torch.cuda.set_device(0)
     backend.prec = "fp64"
     nmol, nlev, M, dt, nsteps = 16, 10, 64, 0.05, 50
@@ -954,38 +961,54 @@ def run_grad(args):
         return HolsteinModel(mols, Quantity(1.0), 3)
 
     build = lambda g: [Mpo(model(g)).numpy(i) for i in range(2 * nmol)]
-    np.random.seed(2024)
-    mps = Mps.hartree_product_state(model(g0), {0: 1})
-    mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=M)
-    mps = mps.expand_bond_dimension()
-    mps.ensure_right_canonical()
-    sites0 = [mps[i] for i in range(len(mps))]
     op = np.diag([0.0, 1.0])
-    torch.cuda.synchronize()
-    t0 = time.time()
-    val, grad = coupling_gradient(build, g0, sites0, dt, nsteps, 0, op, krylov=8, checkpoint_every=10)
-    torch.cuda.synchronize()
-    t_grad = time.time() - t0
-    t0 = time.time()
-    val_e, grad_e = coupling_gradient(build, g0, sites0, dt, nsteps, 0, op, krylov=8, checkpoint_every=0,
-                                      contract="einsum")
-    torch.cuda.synchronize()
-    t_einsum = time.time() - t0
-    fd = {}
-    for j in (0, 1):
-        for h in (1e-5, 1e-3):
-            e = np.zeros(nmol)
-            e[j] = h
-            fp = trajectory_value(build(g0 + e), sites0, dt, nsteps, 0, op, krylov=8)
-            fm = trajectory_value(build(g0 - e), sites0, dt, nsteps, 0, op, krylov=8)
-            fd[f"g{j}_h{h:g}"] = {"fd": (fp - fm) / (2 * h), "grad": float(grad[j]),
-                                 "rel_diff": abs((fp - fm) / (2 * h) - grad[j]) / abs(grad[j])}
+
+    def start(coef):
+        np.random.seed(2024)
+        mps = Mps.hartree_product_state(model(g0), {0: 1})
+        mps.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=M)
+        mps = mps.expand_bond_dimension(coef=coef)
+        mps.ensure_right_canonical()
+        return [mps[i] for i in range(len(mps))]
+
+    out = {}
+    for coef in (1e-2, 1e-10):
+        sites0 = start(coef)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        val, grad = coupling_gradient(build, g0, sites0, dt, nsteps, 0, op, krylov=8, checkpoint_every=10)
+        torch.cuda.synchronize()
+        t_grad = time.time() - t0
+        t0 = time.time()
+        val_e, grad_e = coupling_gradient(build, g0, sites0, dt, nsteps, 0, op, krylov=8, checkpoint_every=0,
+                                          contract="einsum")
+        torch.cuda.synchronize()
+        t_einsum = time.time() - t0
+        res = {"population": val, "gradient": grad.tolist(), "grad_s": t_grad, "einsum_reference_s": t_einsum,
+               "max_abs_diff_vs_einsum_autograd": float(np.abs(grad - grad_e).max()),
+               "max_rel_diff_vs_einsum_autograd": float(np.abs(grad - grad_e).max() / np.abs(grad_e).max()),
+               "population_vs_einsum": abs(val - val_e)}
+        if coef == 1e-2:
+            fd = {}
+            for h in (1e-5, 1e-4):
+                sets = []
+                for j in range(nmol):
+                    e = np.zeros(nmol)
+                    e[j] = h
+                    sets += [build(g0 + e), build(g0 - e)]
+                t0 = time.time()
+                vals = trajectory_values(sets, sites0, dt, nsteps, 0, op, krylov=8)
+                fdg = (vals[0::2] - vals[1::2]) / (2 * h)
+                fd[f"h{h:g}"] = {"fd": fdg.tolist(), "max_abs_diff": float(np.abs(fdg - grad).max()),
+                                 "max_rel_diff": float(np.abs(fdg - grad).max() / np.abs(grad).max()),
+                                 "seconds": time.time() - t0}
+            res["finite_differences"] = fd
+        out[f"coef{coef:g}"] = res
+    main = out["coef0.01"]
     print(json.dumps({"metric": "d <n_0>(t=2.5) / d g_i through TDVP-PS (16-molecule Holstein, M=64, 50 steps)",
-                      "value": t_grad, "unit": "s per gradient (16 couplings)", "population": val,
-                      "gradient": grad.tolist(), "einsum_reference_s": t_einsum,
-                      "max_rel_diff_vs_einsum_autograd": float(np.abs(grad - grad_e).max() / np.abs(grad_e).max()),
-                      "population_vs_einsum": abs(val - val_e), "finite_differences": fd,
-                      "checkpoint_every": 10, "krylov_vectors": 8}), flush=True)
+                      "value": main["grad_s"], "unit": "s per gradient (16 couplings)",
+                      "start": "expand_bond_dimension(coef=1e-2), seeded random expander",
+                      "runs": out, "checkpoint_every": 10, "krylov_vectors": 8}), flush=True)
 
 
 def main():

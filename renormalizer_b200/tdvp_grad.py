@@ -108,48 +108,96 @@ class _Ops:
         return self.td(t, ms, [1, 3], [2, 1])          # f g h
 
 
-def expm_krylov_fixed(apply: Callable, dt: complex, v: torch.Tensor, k: int) -> torch.Tensor:
+class _BatchedOps(_Ops):
+    """Plain torch FP64 contractions over a leading batch axis (many coupling
+    sets of one trajectory at once: the finite-difference checks).  Tensor
+    indices in ``td`` count the per-instance axes; a batch of one
+    broadcasts."""
+
+    batched = True
+
+    def __init__(self):
+        super().__init__("einsum")
+
+    def td(self, a, b, ia, ib):
+        na, nb = a.dim() - 1, b.dim() - 1
+        la = [chr(97 + i) for i in range(na)]
+        lb = [chr(97 + na + i) for i in range(nb)]
+        for x, y in zip(ia, ib):
+            lb[y] = la[x]
+        out = [c for i, c in enumerate(la) if i not in ia] + [c for i, c in enumerate(lb) if i not in ib]
+        dt = torch.complex128 if (a.is_complex() or b.is_complex()) else torch.float64
+        return torch.einsum(f"...{''.join(la)},...{''.join(lb)}->...{''.join(out)}", a.to(dt), b.to(dt))
+
+    def hop(self, psi, L, Ws, R):
+        if not Ws:
+            t = self.td(L, psi, [2], [0])                               # a b k
+            return self.td(t, R, [1, 2], [1, 2])                        # a l
+        t = self.td(L, psi, [2], [0])                                   # a b e k
+        t = self.td(t, Ws[0], [1, 2], [0, 2])                           # a k d f
+        return self.td(t, R, [3, 1], [1, 2])                            # a d l
+
+
+def _bdot(x, y, nb):
+    """<x, y> over all but the first nb axes"""
+    return (x.conj() * y).reshape(*x.shape[:nb], -1).sum(-1) if nb else torch.vdot(x.reshape(-1), y.reshape(-1))
+
+
+def expm_krylov_fixed(apply: Callable, dt: complex, v: torch.Tensor, k: int, nb: int = 0) -> torch.Tensor:
     """exp(dt A) v from k Lanczos vectors (three-term recurrence as in
     krylov.py:27-84, fixed length; stops early on the reference's breakdown
     test beta < 100 n eps, krylov.py:72-74, which also bounds the local
-    Krylov space by the local dimension)."""
-    nrm = torch.linalg.vector_norm(v)
-    tiny = 100 * v.numel() * np.finfo(np.float64).eps
-    Q = [v / nrm]
+    Krylov space by the local dimension).  With ``nb`` = 1, v carries a
+    leading batch axis and every instance runs the same recurrence; the
+    breakdown test then needs all instances below the threshold (a local
+    dimension exhausts them together) and mixed outcomes are an error."""
+    vol = v[0].numel() if nb else v.numel()
+    red = (lambda x: torch.linalg.vector_norm(x.reshape(x.shape[0], -1), dim=1)) if nb else torch.linalg.vector_norm
+    bshape = (-1,) + (1,) * (v.dim() - 1) if nb else ()
+    nrm = red(v)
+    tiny = 100 * vol * np.finfo(np.float64).eps
+    Q = [v / nrm.reshape(bshape)]
     alphas, betas = [], []
     for j in range(k):
         w = apply(Q[j])
-        a = torch.real(torch.vdot(Q[j].reshape(-1), w.reshape(-1)))
-        w = w - a * Q[j]
+        a = torch.real(_bdot(Q[j], w, nb))
+        w = w - a.reshape(bshape) * Q[j]
         if j > 0:
-            w = w - betas[-1] * Q[j - 1]
+            w = w - betas[-1].reshape(bshape) * Q[j - 1]
         alphas.append(a)
         if j == k - 1:
             break
-        b = torch.linalg.vector_norm(w)
-        if float(b.detach()) < tiny:
+        b = red(w)
+        small = (b.detach() < tiny)
+        if bool(small.all()):
             break
+        if bool(small.any()):
+            raise ArithmeticError("batched Lanczos: the instances broke down at different steps")
         betas.append(b)
-        Q.append(w / b)
+        Q.append(w / b.reshape(bshape))
     m = len(alphas)
-    T = torch.diag(torch.stack(alphas)).to(torch.complex128)
+    T = torch.diag_embed(torch.stack(alphas, dim=-1)).to(torch.complex128)
     if m > 1:
-        off = torch.stack(betas[: m - 1]).to(torch.complex128)
-        T = T + torch.diag(off, 1) + torch.diag(off, -1)
-    e = torch.linalg.matrix_exp(dt * T)[:, 0]
-    out = e[0] * Q[0]
+        off = torch.stack(betas[: m - 1], dim=-1).to(torch.complex128)
+        T = T + torch.diag_embed(off, 1) + torch.diag_embed(off, -1)
+    e = torch.linalg.matrix_exp(dt * T)[..., :, 0]
+    coef = lambda j: e[..., j].reshape(bshape)
+    out = coef(0) * Q[0]
     for j in range(1, m):
-        out = out + e[j] * Q[j]
-    return nrm * out
+        out = out + coef(j) * Q[j]
+    return nrm.reshape(bshape) * out
 
 
 def tdvp_ps_step(sites: List[torch.Tensor], Ws: Sequence[torch.Tensor], dt: float, k: int, ops: _Ops):
     """One TDVP-PS step from a right-canonical MPS (centre on site 0): a
     right half-sweep then a left half-sweep, centre normalised; returns the
-    new right-canonical sites (mps.py:1267-1404)."""
+    new right-canonical sites (mps.py:1267-1404).  With batched ops
+    (_BatchedOps) every tensor carries a leading batch axis."""
     n = len(sites)
     sites = list(sites)
-    one = torch.ones((1, 1, 1), dtype=torch.float64, device=sites[0].device)
+    nb = 1 if getattr(ops, "batched", False) else 0
+    lead = tuple(sites[0].shape[:nb])
+    one = torch.ones(lead + (1, 1, 1), dtype=torch.float64, device=sites[0].device)
     R = [None] * (n + 1)
     R[n] = one
     for i in range(n - 1, 0, -1):
@@ -157,42 +205,51 @@ def tdvp_ps_step(sites: List[torch.Tensor], Ws: Sequence[torch.Tensor], dt: floa
     Ls = [one] + [None] * n
     for i in range(n):
         L = Ls[i]
-        sites[i] = expm_krylov_fixed(lambda x: ops.hop(x, L, [Ws[i]], R[i + 1]), -0.5j * dt, sites[i], k)
+        sites[i] = expm_krylov_fixed(lambda x: ops.hop(x, L, [Ws[i]], R[i + 1]), -0.5j * dt, sites[i], k, nb)
         if i == n - 1:
             break
-        ml, d, mr = sites[i].shape
-        q, r = torch.linalg.qr(sites[i].reshape(ml * d, mr))
-        sites[i] = q.reshape(ml, d, q.shape[1])
+        ml, d, mr = sites[i].shape[nb:]
+        q, r = torch.linalg.qr(sites[i].reshape(lead + (ml * d, mr)))
+        sites[i] = q.reshape(lead + (ml, d, q.shape[-1]))
         Ls[i + 1] = ops.env_L(L, sites[i], Ws[i])
-        c = expm_krylov_fixed(lambda x: ops.hop(x, Ls[i + 1], [], R[i + 1]), 0.5j * dt, r, k)
+        c = expm_krylov_fixed(lambda x: ops.hop(x, Ls[i + 1], [], R[i + 1]), 0.5j * dt, r, k, nb)
         sites[i + 1] = ops.td(c, sites[i + 1], [1], [0])
     Rc = one
     for i in range(n - 1, -1, -1):
-        sites[i] = expm_krylov_fixed(lambda x: ops.hop(x, Ls[i], [Ws[i]], Rc), -0.5j * dt, sites[i], k)
+        sites[i] = expm_krylov_fixed(lambda x: ops.hop(x, Ls[i], [Ws[i]], Rc), -0.5j * dt, sites[i], k, nb)
         if i == 0:
             break
-        ml, d, mr = sites[i].shape
-        q1, r1 = torch.linalg.qr(sites[i].reshape(ml, d * mr).mH)     # site = r1^H q1^H
-        sites[i] = q1.mH.reshape(q1.shape[1], d, mr)
+        ml, d, mr = sites[i].shape[nb:]
+        q1, r1 = torch.linalg.qr(sites[i].reshape(lead + (ml, d * mr)).mH)     # site = r1^H q1^H
+        sites[i] = q1.mH.reshape(lead + (q1.shape[-1], d, mr))
         Rn = ops.env_R(Rc, sites[i], Ws[i])
-        c = expm_krylov_fixed(lambda x: ops.hop(x, Ls[i], [], Rn), 0.5j * dt, r1.mH, k)
+        c = expm_krylov_fixed(lambda x: ops.hop(x, Ls[i], [], Rn), 0.5j * dt, r1.mH, k, nb)
         sites[i - 1] = ops.td(sites[i - 1], c, [2], [0])
         Rc = Rn
-    sites[0] = sites[0] / torch.linalg.vector_norm(sites[0])
+    if nb:
+        s0 = sites[0]
+        sites[0] = s0 / torch.linalg.vector_norm(s0.reshape(s0.shape[0], -1), dim=1).reshape(-1, 1, 1, 1)
+    else:
+        sites[0] = sites[0] / torch.linalg.vector_norm(sites[0])
     return sites
 
 
 def site_expectation(sites: Sequence[torch.Tensor], site: int, op: torch.Tensor, ops: _Ops):
-    """<psi| O_site |psi> / <psi|psi> by a left-environment sweep."""
+    """<psi| O_site |psi> / <psi|psi> by a left-environment sweep (one value
+    per instance with batched ops)."""
     dev = sites[0].device
-    E = torch.ones((1, 1, 1), dtype=torch.float64, device=dev)
+    nb = 1 if getattr(ops, "batched", False) else 0
+    one = (1,) * nb
+    E = torch.ones(one + (1, 1, 1), dtype=torch.float64, device=dev)
     N = E
     for i, ms in enumerate(sites):
-        d = ms.shape[1]
-        eye = torch.eye(d, dtype=torch.float64, device=dev).reshape(1, d, d, 1)
-        W = op.reshape(1, d, d, 1) if i == site else eye
+        d = ms.shape[nb + 1]
+        eye = torch.eye(d, dtype=torch.float64, device=dev).reshape(one + (1, d, d, 1))
+        W = op.reshape(one + (1, d, d, 1)) if i == site else eye
         E = ops.env_L(E, ms, W)
         N = ops.env_L(N, ms, eye)
+    if nb:
+        return torch.real(E.reshape(E.shape[0], -1)[:, 0]) / torch.real(N.reshape(N.shape[0], -1)[:, 0])
     return torch.real(E.reshape(-1)[0]) / torch.real(N.reshape(-1)[0])
 
 
@@ -224,6 +281,23 @@ def trajectory_value(Ws: Sequence[np.ndarray], sites0: Sequence[torch.Tensor], d
         for _ in range(nsteps):
             sites = tdvp_ps_step(sites, Wd, dt, krylov, ops)
         return float(site_expectation(sites, obs_site, torch.as_tensor(op, dtype=torch.float64, device=dev), ops))
+
+
+def trajectory_values(Ws_list: Sequence[Sequence[np.ndarray]], sites0: Sequence[torch.Tensor], dt: float,
+                      nsteps: int, obs_site: int, op: np.ndarray, krylov: int = 8) -> np.ndarray:
+    """trajectory_value(contract="einsum") for many MPOs of one structure at
+    once (batched FP64 torch contractions; used for finite differences)."""
+    ops = _BatchedOps()
+    dev = sites0[0].device
+    B = len(Ws_list)
+    Wd = [torch.stack([torch.as_tensor(np.asarray(Ws[i], dtype=float)) for Ws in Ws_list]).to(dev)
+          for i in range(len(Ws_list[0]))]
+    with torch.no_grad():
+        sites = [s.to(torch.complex128).unsqueeze(0).expand((B,) + tuple(s.shape)).contiguous() for s in sites0]
+        for _ in range(nsteps):
+            sites = tdvp_ps_step(sites, Wd, dt, krylov, ops)
+        opd = torch.as_tensor(op, dtype=torch.float64, device=dev)
+        return site_expectation(sites, obs_site, opd, ops).cpu().numpy()
 
 
 def coupling_gradient(build: Callable[[np.ndarray], Sequence[np.ndarray]], g0, sites0: Sequence[torch.Tensor],

@@ -69,3 +69,17 @@ def test_tdvp_gradient_host_logic(cpu_engine):
 @pytest.mark.gpu
 def test_tdvp_gradient_gpu():
     _run("cuda")
+
+
+def test_batched_trajectory_values_match_single_cpu(cpu_engine):
+    """trajectory_values (batched FP64 torch contractions, the finite-difference
+    helper) equals trajectory_value(contract="einsum") per coupling set"""
+    from renormalizer_b200.tdvp_grad import trajectory_value, trajectory_values
+    _, build, g0, mps = _setup("cpu")
+    sites0 = [mps[i].cpu() for i in range(len(mps))]
+    op = np.diag([0.0, 1.0])
+    gs = [g0, g0 + np.array([1e-3, 0, 0]), g0 - np.array([0, 0, 2e-3])]
+    got = trajectory_values([build(g) for g in gs], sites0, 0.1, 3, 0, op, krylov=8)
+    for g, v in zip(gs, got):
+        ref = trajectory_value(build(g), sites0, 0.1, 3, 0, op, krylov=8, contract="einsum")
+        assert abs(v - ref) < 1e-13, (v, ref)
