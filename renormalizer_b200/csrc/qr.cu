@@ -161,6 +161,8 @@ __global__ void __cluster_dims__(QCL, 1, 1) __launch_bounds__(QT, 1)
   T* wfull = wpart + 2 * NBMAX;                            // NBMAX: the summed w
   T* gram = wfull + NBMAX;                                 // NBMAX x NBMAX partial V^H V
   T* stau = gram + NBMAX * NBMAX;                          // NBMAX
+  T* tsm = stau + NBMAX;                                   // NBMAX x NBMAX: T of the panel (CTA 0)
+  T* xs = tsm + NBMAX * NBMAX;                             // NBMAX: one column's -tau_i (V^H V)[:, i]
   __shared__ double npart[2];                              // this CTA's partial ||x||^2 by column parity
   __shared__ T apart[2];                                   // alpha, written by its owner
   __shared__ double redd[QW];
@@ -266,33 +268,46 @@ __global__ void __cluster_dims__(QCL, 1, 1) __launch_bounds__(QT, 1)
     V[(size_t)(p0 + r) * P.kq + p0 + jj] = (r == jj) ? E::one() : (r > jj ? x : E::zero());
   }
   cluster.sync();
-  if (rank == 0 && tid == 0) {
-    // zlarft (forward, columnwise): T[0:i, i] = -tau_i T[0:i, 0:i] (V^H V)[0:i, i]
+  if (rank == 0) {
+    // the cluster's V^H V: every entry summed over the CTAs (in rank order)
+    // by one thread of CTA 0, in place in CTA 0's partial
+    for (int e = tid; e < nbp * nbp; e += QT) {
+      const int i = e / nbp, j = e % nbp;
+      T g = E::zero();
+      for (int q = 0; q < QCL; ++q) g = E::add(g, cluster.map_shared_rank(gram, q)[i * NBMAX + j]);
+      gram[i * NBMAX + j] = g;
+    }
+    for (int e = tid; e < NBMAX * NBMAX; e += QT) tsm[e] = E::zero();
+    __syncthreads();
+    // zlarft (forward, columnwise): T[0:i, i] = -tau_i T[0:i, 0:i] (V^H V)[0:i, i];
+    // lane l owns row l of T (nb <= 32), columns in order
+    if (warp == 0) {
+      for (int i = 0; i < nbp; ++i) {
+        const T ti = stau[i];
+        if (lane < i) xs[lane] = E::mul(E::neg(ti), gram[lane * NBMAX + i]);
+        __syncwarp();
+        if (lane < i) {
+          T acc = E::zero();
+          for (int c = lane; c < i; ++c) acc = E::add(acc, E::mul(tsm[lane * NBMAX + c], xs[c]));
+          tsm[lane * NBMAX + i] = acc;
+        } else if (lane == i) {
+          tsm[i * NBMAX + i] = ti;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
     const int pi = p0 / nb;
     T* Tm = reinterpret_cast<T*>(P.t) + (size_t)pi * nb * nb;
     T* NT = reinterpret_cast<T*>(P.nt) + (size_t)pi * nb * nb;
     T* NTH = reinterpret_cast<T*>(P.nth) + (size_t)pi * nb * nb;
-    T x[NBMAX];
-    for (int i = 0; i < nb * nb; ++i) Tm[i] = E::zero();
-    for (int i = 0; i < nbp; ++i) {
-      const T ti = stau[i];
-      for (int l = 0; l < i; ++l) {
-        T g = E::zero();
-        for (int q = 0; q < QCL; ++q) g = E::add(g, cluster.map_shared_rank(gram, q)[l * NBMAX + i]);
-        x[l] = E::mul(E::neg(ti), g);
-      }
-      for (int l = 0; l < i; ++l) {
-        T acc = E::zero();
-        for (int c = l; c < i; ++c) acc = E::add(acc, E::mul(Tm[l * nb + c], x[c]));
-        Tm[l * nb + i] = acc;
-      }
-      Tm[i * nb + i] = ti;
+    for (int e = tid; e < nb * nb; e += QT) {
+      const int i = e / nb, j = e % nb;
+      const T t = tsm[i * NBMAX + j];
+      Tm[e] = t;
+      NT[e] = E::neg(t);
+      NTH[e] = E::neg(E::conj(tsm[j * NBMAX + i]));
     }
-    for (int i = 0; i < nb; ++i)
-      for (int j = 0; j < nb; ++j) {
-        NT[i * nb + j] = E::neg(Tm[i * nb + j]);
-        NTH[i * nb + j] = E::neg(E::conj(Tm[j * nb + i]));
-      }
   }
   cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
@@ -444,9 +459,10 @@ extern "C" int reno_qr_blocks(reno_ctx* ctx, int32_t count, const reno_qr_block*
     nmax = std::max(nmax, P.m);
   }
   const int rows = (nmax + qr::QCL - 1) / qr::QCL;
-  const size_t smem = ((size_t)rows * nb + 2 * qr::NBMAX + qr::NBMAX + qr::NBMAX * qr::NBMAX + qr::NBMAX) * es;
+  const size_t smem =
+      ((size_t)rows * nb + 2 * qr::NBMAX + qr::NBMAX + 2 * qr::NBMAX * qr::NBMAX + 2 * qr::NBMAX) * es;
   // the opt-in is made once per device, so it covers the largest panel any call can use
-  const int smem_max = (int)(((size_t)qr::PANEL_ELEMS + 4 * qr::NBMAX + qr::NBMAX * qr::NBMAX) * 16);
+  const int smem_max = (int)(((size_t)qr::PANEL_ELEMS + 5 * qr::NBMAX + 2 * qr::NBMAX * qr::NBMAX) * 16);
   static std::atomic<unsigned long long> set_c{0}, set_r{0};
   cudaError_t e = cplx ? smem_optin_once(qr::qr_panel_kernel<true>, smem_max, set_c)
                        : smem_optin_once(qr::qr_panel_kernel<false>, smem_max, set_r);
