@@ -136,7 +136,7 @@ __device__ bool grid_sync(Sync* s, unsigned nblocks, unsigned& epoch, int* ok_sh
 
 constexpr int HT = 512, HW = HT / 32;  // reduction kernel: 16 warps, one CTA per SM
 constexpr int U1 = 4;                  // loads in flight per thread (rows k, y)
-constexpr int U2 = 8;                  // loads in flight per lane (trailing rows)
+constexpr int U2 = 6;                  // loads in flight per lane per item (trailing rows)
 constexpr int MAXM = 32;               // matrices per batched launch
 
 // One matrix of a batched reduction: CTAs first .. first + nblk - 1 of the
@@ -180,6 +180,41 @@ struct HetrdTable {
 // A: n x n row-major Hermitian (both triangles), overwritten: row k holds
 // reflector k from column k+1 on.  Y: 2n, P: 2 * nblk scratch.  Every
 // matrix of the table is reduced by its own share of the grid.
+//
+// Per column k (lagged: update k-1 is applied while column k is processed):
+//   phase 1 (every CTA)  row k with update k-1 applied, reflector k;
+//   phase 2              the trailing rows r > k are dealt round-robin to the
+//                        matrix's CTAs (r = k + 1 + bid + j G); each CTA splits
+//                        its rows into chunks of HCH columns and spreads the
+//                        (row, chunk) items over its warps, two items in
+//                        flight per warp: update k-1 applied and stored, the
+//                        chunk's share of y_r = (A v_k)_r kept in shared
+//                        memory and summed per row in chunk order;
+//   grid barrier;
+//   phase 3 (every CTA)  w_k from y and the CTA partials of y^H v_k, issued
+//                        together with the loads of row k+1 for the next
+//                        phase 1 (one round trip to L2 for both).
+constexpr int HCH = 32 * U2;    // columns per phase-2 item
+constexpr int PARTS = 1024;     // per-CTA (row, chunk) partial sums held at once
+
+// one phase-2 item: update k-1 on U2 x 32 entries of a row (a: their loaded
+// values), stored back; returns the lane's share of the row's y
+__device__ __forceinline__ double2 hetrd_item(double2* __restrict__ row, int cbase, int n, double2 vpr, double2 wpr,
+                                              const double2* vp, const double2* wp, const double2* vc,
+                                              const double2 (&a)[U2]) {
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int u = 0; u < U2; ++u) {
+    const int c = cbase + 32 * u;
+    if (c < n) {
+      const double2 x = csub(csub(a[u], cmulc(vpr, wp[c])), cmulc(wpr, vp[c]));
+      __stcg(&row[c], x);
+      acc = cadd(acc, cmul(x, vc[c]));
+    }
+  }
+  return acc;
+}
+
 __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ HetrdTable tab) {
   int pi = 0;
   while (pi + 1 < tab.count && (int)blockIdx.x >= tab.p[pi + 1].first) ++pi;
@@ -197,17 +232,25 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
   double2* vp = reinterpret_cast<double2*>(smem_raw);  // v of step k-1 (pending update)
   double2* wp = vp + n;                                // w of step k-1
   double2* vc = wp + n;                                // v of step k
+  double2* parts = vc + n;                             // PARTS (row, chunk) partial sums of y
   __shared__ double red[HW];
   __shared__ double2 redc[HW];
   __shared__ double s_akk;
   __shared__ int s_ok;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const unsigned G = (unsigned)PR.nblk;
+  const int G = PR.nblk;
   unsigned gen = 0;
   for (int i = tid; i < n; i += HT) {
     vp[i] = make_double2(0.0, 0.0);
     wp[i] = make_double2(0.0, 0.0);
     vc[i] = make_double2(0.0, 0.0);
+  }
+  // row 0, the part phase 1 reads in its first pass (c = tid + u HT)
+  double2 pre[U1];
+#pragma unroll
+  for (int u = 0; u < U1; ++u) {
+    const int c = tid + u * HT;
+    pre[u] = c < n ? __ldcg(&A[c]) : make_double2(0.0, 0.0);
   }
   __syncthreads();
   // Shared-memory discipline: in phases 1 and 3 thread t owns the entries
@@ -217,22 +260,27 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
   // recomputes the scalars that more than one thread needs (the Householder
   // scalars, the dot y^H v and the pending pivot entries v_{k-1}[k] = 1,
   // w_{k-1}[k]) with the same operations, so they agree bit for bit.
-  double2 tk_prev = make_double2(0.0, 0.0), alph_prev = make_double2(0.0, 0.0);
+  double2 tk_prev = make_double2(0.0, 0.0), alph_prev = make_double2(0.0, 0.0), yk_prev = make_double2(0.0, 0.0);
   for (int k = 0; k < n - 1; ++k) {
     // ---- phase 1 (every CTA): row k with update k-1 applied, reflector k
     double2 vpk = make_double2(0.0, 0.0), wpk = make_double2(0.0, 0.0);
     if (k > 0) {
       vpk = make_double2(1.0, 0.0);
-      wpk = cadd(cmul(tk_prev, __ldcg(&Y[(size_t)((k - 1) & 1) * n + k])), cmul(alph_prev, vpk));
+      wpk = cadd(cmul(tk_prev, yk_prev), cmul(alph_prev, vpk));
     }
     const double2* rowk = A + (size_t)k * n;
     double ss = 0.0;
     for (int base = k + tid; base < n; base += U1 * HT) {
       double2 a[U1];
+      if (base == k + tid) {
 #pragma unroll
-      for (int u = 0; u < U1; ++u) {
-        const int c = base + u * HT;
-        a[u] = c < n ? __ldcg(&rowk[c]) : make_double2(0.0, 0.0);
+        for (int u = 0; u < U1; ++u) a[u] = pre[u];
+      } else {
+#pragma unroll
+        for (int u = 0; u < U1; ++u) {
+          const int c = base + u * HT;
+          a[u] = c < n ? __ldcg(&rowk[c]) : make_double2(0.0, 0.0);
+        }
       }
 #pragma unroll
       for (int u = 0; u < U1; ++u) {
@@ -285,36 +333,61 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
     }
     __syncthreads();
 
-    // ---- phase 2 (rows split over all warps of the grid): update k-1, y = A v_k
-    const int gw = bid * HW + warp, tw = (int)G * HW;
+    // ---- phase 2: update k-1 on this CTA's trailing rows, y = A v_k
+    const int nrow = n - k - 1;
+    const int nr_c = nrow > bid ? (nrow - bid + G - 1) / G : 0;
+    const int nch = (nrow + HCH - 1) / HCH;
+    const int rb = max(1, PARTS / nch);
     double2 pdot = make_double2(0.0, 0.0);
-    for (int r = k + 1 + gw; r < n; r += tw) {
-      const double2 vpr = vp[r], wpr = wp[r];
-      double2* row = A + (size_t)r * n;
-      double2 acc = make_double2(0.0, 0.0);
-      for (int base = k + 1 + lane; base < n; base += 32 * U2) {
-        double2 a[U2];
+    for (int j0 = 0; j0 < nr_c; j0 += rb) {
+      const int jn = min(rb, nr_c - j0);
+      const int nit = jn * nch;
+      for (int it = warp; it < nit; it += 2 * HW) {
+        const int it2 = it + HW;
+        const int jl1 = it / nch, ch1 = it - jl1 * nch;
+        const int r1 = k + 1 + bid + (j0 + jl1) * G;
+        const int cb1 = k + 1 + ch1 * HCH + lane;
+        double2* row1 = A + (size_t)r1 * n;
+        double2 a1[U2], a2[U2];
 #pragma unroll
         for (int u = 0; u < U2; ++u) {
-          const int c = base + 32 * u;
-          a[u] = c < n ? __ldcg(&row[c]) : make_double2(0.0, 0.0);
+          const int c = cb1 + 32 * u;
+          a1[u] = c < n ? __ldcg(&row1[c]) : make_double2(0.0, 0.0);
         }
+        int jl2 = 0, ch2 = 0, r2 = 0, cb2 = 0;
+        double2* row2 = row1;
+        if (it2 < nit) {
+          jl2 = it2 / nch;
+          ch2 = it2 - jl2 * nch;
+          r2 = k + 1 + bid + (j0 + jl2) * G;
+          cb2 = k + 1 + ch2 * HCH + lane;
+          row2 = A + (size_t)r2 * n;
 #pragma unroll
-        for (int u = 0; u < U2; ++u) {
-          const int c = base + 32 * u;
-          if (c < n) {
-            const double2 x = csub(csub(a[u], cmulc(vpr, wp[c])), cmulc(wpr, vp[c]));
-            __stcg(&row[c], x);
-            acc = cadd(acc, cmul(x, vc[c]));
+          for (int u = 0; u < U2; ++u) {
+            const int c = cb2 + 32 * u;
+            a2[u] = c < n ? __ldcg(&row2[c]) : make_double2(0.0, 0.0);
           }
         }
+        double2 acc = hetrd_item(row1, cb1, n, vp[r1], wp[r1], vp, wp, vc, a1);
+        acc = warp_sum(acc);
+        if (lane == 0) parts[jl1 * nch + ch1] = acc;
+        if (it2 < nit) {
+          acc = hetrd_item(row2, cb2, n, vp[r2], wp[r2], vp, wp, vc, a2);
+          acc = warp_sum(acc);
+          if (lane == 0) parts[jl2 * nch + ch2] = acc;
+        }
       }
-      acc = warp_sum(acc);
-      if (lane == 0) {
-        __stcg(&Y[(size_t)(k & 1) * n + r], acc);
-        pdot = cadd(pdot, cmulc(vc[r], acc));  // conj(y_r) v_r
+      __syncthreads();
+      for (int jl = tid; jl < jn; jl += HT) {
+        double2 y = make_double2(0.0, 0.0);
+        for (int ch = 0; ch < nch; ++ch) y = cadd(y, parts[jl * nch + ch]);
+        const int r = k + 1 + bid + (j0 + jl) * G;
+        __stcg(&Y[(size_t)(k & 1) * n + r], y);
+        pdot = cadd(pdot, cmulc(vc[r], y));  // v_r conj(y_r)
       }
+      __syncthreads();  // parts is refilled by the next row group
     }
+    pdot = warp_sum(pdot);
     if (lane == 0) redc[warp] = pdot;
     __syncthreads();
     if (tid == 0) {
@@ -322,30 +395,46 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
       for (int w = 0; w < HW; ++w) s = cadd(s, redc[w]);
       __stcg(&P[(size_t)(k & 1) * G + bid], s);
     }
-    if (!grid_sync(sync, G, gen, &s_ok, tab.wait_ns, pi == 0 && bid == 0 && k == tab.skip_column)) return;
+    if (!grid_sync(sync, (unsigned)G, gen, &s_ok, tab.wait_ns, pi == 0 && bid == 0 && k == tab.skip_column)) return;
 
     // ---- phase 3 (every CTA): w_k = tau y - (|tau|^2 / 2)(y^H v) v; every
-    // warp sums the CTA partials itself
+    // warp sums the CTA partials itself.  The loads of y, of the partials, of
+    // y_{k+1} and of row k+1 (phase 1 of the next column) go out together.
+    const bool next = k + 2 < n;
+    const double2* rown = A + (size_t)(k + 1) * n;
+    double2 yv[U1];
+#pragma unroll
+    for (int u = 0; u < U1; ++u) {
+      const int c = k + 1 + tid + u * HT;
+      yv[u] = c < n ? __ldcg(&Y[(size_t)(k & 1) * n + c]) : make_double2(0.0, 0.0);
+      pre[u] = (next && c < n) ? __ldcg(&rown[c]) : make_double2(0.0, 0.0);
+    }
+    const double2 yk1 = __ldcg(&Y[(size_t)(k & 1) * n + k + 1]);
     double2 dot = make_double2(0.0, 0.0);
-    for (int base = lane; base < (int)G; base += 32 * U1) {
-      double2 p[U1];
+    for (int base = lane; base < G; base += 32 * U1) {
+      double2 pp[U1];
 #pragma unroll
       for (int u = 0; u < U1; ++u) {
         const int b = base + 32 * u;
-        p[u] = b < (int)G ? __ldcg(&P[(size_t)(k & 1) * G + b]) : make_double2(0.0, 0.0);
+        pp[u] = b < G ? __ldcg(&P[(size_t)(k & 1) * G + b]) : make_double2(0.0, 0.0);
       }
 #pragma unroll
-      for (int u = 0; u < U1; ++u) dot = cadd(dot, p[u]);
+      for (int u = 0; u < U1; ++u) dot = cadd(dot, pp[u]);
     }
     dot = warp_sum(dot);
     const double t2 = tk.x * tk.x + tk.y * tk.y;
     const double2 alph = make_double2(-0.5 * t2 * dot.x, -0.5 * t2 * dot.y);
     for (int base = k + 1 + tid; base < n; base += U1 * HT) {
       double2 y[U1];
+      if (base == k + 1 + tid) {
 #pragma unroll
-      for (int u = 0; u < U1; ++u) {
-        const int c = base + u * HT;
-        y[u] = c < n ? __ldcg(&Y[(size_t)(k & 1) * n + c]) : make_double2(0.0, 0.0);
+        for (int u = 0; u < U1; ++u) y[u] = yv[u];
+      } else {
+#pragma unroll
+        for (int u = 0; u < U1; ++u) {
+          const int c = base + u * HT;
+          y[u] = c < n ? __ldcg(&Y[(size_t)(k & 1) * n + c]) : make_double2(0.0, 0.0);
+        }
       }
 #pragma unroll
       for (int u = 0; u < U1; ++u) {
@@ -359,6 +448,7 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
     }
     tk_prev = tk;
     alph_prev = alph;
+    yk_prev = yk1;
   }
   if (bid == 0 && tid == 0) {
     if (n == 1) {
@@ -862,10 +952,10 @@ GemmOperand op(const void* p, int64_t s_outer, int64_t s_k, int conj) {
 // one CTA per SM, the SMs shared out in proportion to each matrix's n^2.
 static int launch_hetrd(reno_ctx* ctx, HetrdTable& tab, int nmax, const char* what) {
   static std::atomic<unsigned long long> hetrd_set{0};
-  int rc = check_cuda(ctx, smem_optin_once(hetrd_kernel, 3 * MAX_N * 16, hetrd_set),
+  int rc = check_cuda(ctx, smem_optin_once(hetrd_kernel, (3 * MAX_N + PARTS) * 16, hetrd_set),
                       (std::string(what) + ": hetrd smem attribute").c_str());
   if (rc != RENO_OK) return rc;
-  const size_t smem = 3 * (size_t)nmax * sizeof(double2);
+  const size_t smem = (3 * (size_t)nmax + PARTS) * sizeof(double2);
   int per_sm = 0;
   rc = check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_kernel, HT, smem),
                   (std::string(what) + ": occupancy").c_str());
