@@ -506,7 +506,8 @@ def run_engine(args, rank, world, dist):
     l0 = launch_count()
     import importlib
     svdmod = importlib.import_module("renormalizer_b200.svd_qn")
-    sub0 = (svdmod.subspace.calls, svdmod.subspace.fallbacks, svdmod.subspace.retries)
+    sub0 = (svdmod.subspace.calls, svdmod.subspace.fallbacks, svdmod.subspace.retries, svdmod.refine.calls,
+            svdmod.refine.blocks)
     svdmod.flop_log = []
     with ClockSampler(local) as clocks:
         s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -519,7 +520,10 @@ def run_engine(args, rank, world, dist):
     trunc_fl = float(sum(svdmod.flop_log))
     svdmod.flop_log = None
     heev_mod = importlib.import_module("renormalizer_b200.heev")
-    trunc = {"device_eigensolver_fallbacks": heev_mod.heev_opts.fallbacks,"subspace_blocks": svdmod.subspace.calls - sub0[0], "retries": svdmod.subspace.retries - sub0[2],
+    trunc = {"device_eigensolver_fallbacks": heev_mod.heev_opts.fallbacks,
+             "small_sigma_refinements": {"truncations": svdmod.refine.calls - sub0[3],
+                                         "blocks": svdmod.refine.blocks - sub0[4], "tau": svdmod.refine.tau},
+             "subspace_blocks": svdmod.subspace.calls - sub0[0], "retries": svdmod.subspace.retries - sub0[2],
              "fallbacks": svdmod.subspace.fallbacks - sub0[1],
              "options": {"min_dim": svdmod.subspace.min_dim, "iters": svdmod.subspace.iters,
                          "oversample": svdmod.subspace.oversample, "rtol": svdmod.subspace.rtol}}
