@@ -318,11 +318,22 @@ class RefineOptions:
     the device eigensolver, and its eigenvectors rotate the cluster's kept
     basis and rows (K P is unchanged).  The refined sigma are accurate to
     about sqrt(eps) tau ||X|| instead of sqrt(eps) ||X||.  ``tau`` = 0 turns
-    the pass off."""
+    the pass off.
 
-    def __init__(self, tau=1e-5):
+    ``always`` False (default): only truncations that keep every entry (the
+    singular values a caller reports, compress with an unbounded cap as in
+    calc_bond_singular_values) are refined.  In a sweep the cut of a nearly
+    product state falls among directions of weight ~1e-20 (the bond
+    expansion's 1e-10 padding), where every block would need a second
+    eigensolver pass of its whole cluster; those directions carry no weight
+    an observable can see, and their choice is rounding-sensitive in the
+    reference's LAPACK path as well.  ``always`` True refines wherever the cut
+    reaches a cluster."""
+
+    def __init__(self, tau=1e-5, always=False):
         env = os.environ.get("RENO_REFINE_TAU")
         self.tau = float(env) if env else tau
+        self.always = always
         self.calls = 0
         self.blocks = 0
 
@@ -802,7 +813,9 @@ def _trunc_end(st, host):
         return sig, _select_by_code(sig, blk, [code_of[q] for q in visit_set], m_trunc_fn(sig), percent)
 
     sig, sidx = select()
-    if refine.tau > 0 and len(sidx) and sig.max() > 0 and sig[sidx].min() < 2 * refine.tau * sig.max():
+    keeps_all = len(sidx) >= sum(b["dim"] for b in blocks)
+    if refine.tau > 0 and (keeps_all or refine.always) and len(sidx) and sig.max() > 0 and \
+            sig[sidx].min() < 2 * refine.tau * sig.max():
         if _refine_clusters(eng, blocks, keep_left):
             sig, sidx = select()
     mdim = len(sidx)
