@@ -74,6 +74,9 @@ def parse():
                     help="--accuracy mode: also evolve FP64 from the start state perturbed by one ulp per entry "
                          "and report its distance from the unperturbed FP64 run (the FP64 engine's own envelope)")
     ap.add_argument("--out", default="", help="append the per-step JSON lines of --accuracy mode to this file")
+    ap.add_argument("--krylov-tol", default="",
+                    help="rtol,atol of the Lanczos convergence test for every arm (default: the reference's "
+                         "numpy allclose defaults 1e-5,1e-8)")
     ap.add_argument("--accuracy-lockstep", type=int, default=1,
                     help="--accuracy mode: advance the FP64 reference and every arm together through "
                          "evolve_batch (1, default) or one after another (0)")
@@ -532,7 +535,7 @@ def run_engine(args, rank, world, dist):
     t_ms = reduce_max_ms(s_ev.elapsed_time(e_ev), dist, dev)
     value = world * args.steps / (t_ms * 1e-3)
     fl, heff_ms, nheff = timer.result()
-    kry_timed = mps.evolve_config.stat
+    kry_timed = {k: v for k, v in (mps.evolve_config.stat or {}).items() if k != "counts"} or None
 
     # e2e: host-resident MPS (pinned), copied in, evolved, populations copied out
     e2e = None
@@ -749,7 +752,8 @@ def run_accuracy(args):
             out.flush()
 
     emit({"start": args.start, "start_s": t_start, "bond_dims": mps0.bond_dims, "nmol": args.nmol, "M": args.M,
-          "dt": args.dt, "arms": list(arms), "lockstep": bool(args.accuracy_lockstep)})
+          "dt": args.dt, "arms": list(arms), "lockstep": bool(args.accuracy_lockstep),
+          "krylov_tol": args.krylov_tol or "1e-5,1e-8"})
     names = list(arms)
     for step in range(args.accuracy):
         row = {"step": step + 1}
@@ -763,9 +767,14 @@ def run_accuracy(args):
             arms = dict(zip(names, res[1:]))
             step_s["lockstep"] = step_s.get("lockstep", 0.0) + time.time() - t1
             pref = ref.e_occupations
+            kref = (ref.evolve_config.stat or {}).get("counts", [])
             for k in names:
                 row[k] = float(np.abs(arms[k].e_occupations - pref).max())
                 worst[k] = max(worst[k], row[k])
+                # local exponentials of this step whose Lanczos stopped at another
+                # length than the FP64 reference's
+                ka = (arms[k].evolve_config.stat or {}).get("counts", [])
+                row[k + "_krylov_mismatch"] = sum(a != b for a, b in zip(ka, kref)) + abs(len(ka) - len(kref))
             emit(row)
             continue
         backend.prec = "fp64"
@@ -1042,6 +1051,9 @@ def main():
         return
     import importlib
     importlib.import_module("renormalizer_b200.svd_qn").subspace.min_dim = 1024 if args.truncation == "subspace" else 0
+    if args.krylov_tol:
+        tol = importlib.import_module("renormalizer_b200.krylov").tolerance
+        tol.rtol, tol.atol = (float(x) for x in args.krylov_tol.split(","))
     if args.accuracy:
         run_accuracy(args)
         return

@@ -48,7 +48,8 @@ def _krylov_stats(steps):
     if not steps:
         return None
     a = np.asarray(steps, dtype=float)
-    return {"nobs": int(a.size), "minmax": (int(a.min()), int(a.max())), "mean": float(a.mean())}
+    return {"nobs": int(a.size), "minmax": (int(a.min()), int(a.max())), "mean": float(a.mean()),
+            "counts": [int(x) for x in steps]}
 
 
 class TruncRequest:
