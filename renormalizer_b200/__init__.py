@@ -21,8 +21,11 @@ from .davidson import davidson
 from .gs import optimize_mps
 from .autodiff import heff as heff_autograd
 from .tdmps import TdMpsJob
+from .mpdm import MpDm
+from .thermalprop import ThermalProp, load_thermal_state
 
 __all__ = ["backend", "evolve_batch", "compressed_sum", "CompressConfig", "CompressCriteria", "EvolveConfig", "EvolveMethod", "OptimizeConfig",
            "BasisHalfSpin", "BasisSHO", "BasisSimpleElectron", "HolsteinModel", "Model", "Mol", "Op", "Phonon",
            "Quantity", "SpectralDensityFunction", "SpinBosonModel", "Mpo", "Mps", "Environ", "contract_one_site",
-           "hop_expr", "expm_krylov", "svd_qn", "davidson", "optimize_mps", "heff_autograd", "TdMpsJob"]
+           "hop_expr", "expm_krylov", "svd_qn", "davidson", "optimize_mps", "heff_autograd", "TdMpsJob", "MpDm",
+           "ThermalProp", "load_thermal_state"]

@@ -39,6 +39,10 @@ class Quantity:
     def as_au(self) -> float:
         return self.value / _RATIO[self.unit]
 
+    def to_beta(self) -> float:
+        """quantity.py:53-56: 1 / (k_B T) in atomic units for a temperature"""
+        return np.inf if self.value == 0 else 1.0 / self.as_au()
+
     def __repr__(self):
         return f"Quantity({self.value}, {self.unit!r})"
 

@@ -200,7 +200,12 @@ class Mpo:
         from ._native import Engine
         dt = new.dtype
         sites = []
-        for W, ms in zip(self._dev, new._mp):
+        # on a density operator the MPO acts on the physical index (mpo.py:331-389 via MpDm)
+        Ws = self._dev
+        if getattr(mp, "is_mpdm", False):
+            from .mpdm import ancilla_mpo
+            Ws = ancilla_mpo(self)._dev
+        for W, ms in zip(Ws, new._mp):
             a, p, q, b = W.shape
             c, q2, d = ms.shape
             assert q == q2

@@ -61,6 +61,10 @@ class TruncRequest:
 
 
 class Mps:
+    is_mps = True
+    is_mpo = False
+    is_mpdm = False
+
     # ------------------------------------------------------------ construction
     def __init__(self):
         self._mp: List[torch.Tensor] = []
@@ -198,8 +202,8 @@ class Mps:
     def dump(self, fname, other_attrs=None):
         """npz protocol 0.4 writer (mp.py:1085-1113)."""
         data = {"version": "0.4", "nsites": len(self)}
-        for i, mt in enumerate(self._mp):
-            data[f"mt_{i}"] = mt.cpu().numpy()
+        for i in range(len(self._mp)):
+            data[f"mt_{i}"] = self._site_for_file(i).cpu().numpy()
         data["qnidx"] = self.qnidx
         data["qntot"] = self.qntot
         arr = np.empty(len(self.qn), object)
@@ -212,6 +216,9 @@ class Mps:
         for a in other_attrs or []:
             data[a] = getattr(self, a)
         np.savez(fname, **data)
+
+    def _site_for_file(self, i) -> torch.Tensor:
+        return self._mp[i]
 
     # ------------------------------------------------------------ container
     def _to_dev(self, array) -> torch.Tensor:
@@ -226,7 +233,7 @@ class Mps:
         t = self._to_dev(array)
         if self._mp:
             assert t.shape[0] == self._mp[-1].shape[-1]
-        if t.shape[1] != self.model.pbond_list[len(self._mp)]:
+        if t.shape[1] != self.pbond_list[len(self._mp)]:
             raise ValueError("Matrix physical bond dimension does not match system information")
         self._mp.append(t)
 
@@ -242,7 +249,7 @@ class Mps:
 
     def __setitem__(self, i, array):
         t = self._to_dev(array)
-        if t.shape[1] != self.model.pbond_list[i if i >= 0 else len(self) + i]:
+        if t.shape[1] != self.pbond_list[i if i >= 0 else len(self) + i]:
             raise ValueError("Matrix physical bond dimension does not match system information")
         self._mp[i] = t
 
@@ -808,18 +815,30 @@ class Mps:
 
     # ------------------------------------------------------------ bond expansion
     @classmethod
-    def ground_state(cls, model: Model, max_entangled: bool = False) -> "Mps":
-        """mps.py:259-350 for max_entangled=False: every site in its basis
-        state 0 (electrons empty, SHO modes in their ground state), QN 0."""
-        if max_entangled:
-            raise NotImplementedError("the maximally entangled (T = infinity) state belongs to the MPDM path")
+    def ground_state(cls, model: Model, max_entangled: bool = False, normalize: bool = True) -> "Mps":
+        """mps.py:259-350: electrons empty; SHO modes (and spins) in their
+        ground state, or with ``max_entangled`` in the uniform T = infinity
+        state (1 / sqrt(d) per level, 1 without ``normalize``); QN 0."""
         sites = []
         for b in model.basis:
             ms = np.zeros((1, b.nbas, 1))
-            ms[0, 0, 0] = 1.0
+            if max_entangled and (b.is_phonon or b.is_spin):
+                ms[0, :, 0] = 1.0 / np.sqrt(b.nbas) if normalize else 1.0
+            elif b.is_phonon or b.is_spin or b.is_electron:
+                ms[0, 0, 0] = 1.0
+            else:
+                raise NotImplementedError(f"ground state of basis {type(b).__name__}")
             sites.append(ms)
         qn = [np.zeros((1, model.qn_size), dtype=int) for _ in range(model.nsite + 1)]
         return cls.from_arrays(model, sites, qn, model.nsite - 1, np.zeros(model.qn_size, dtype=int), False)
+
+    def _expansion_ex_state(self) -> "Mps":
+        """mps.py:1943-1949: the excited product state of the hint expander"""
+        assert self.model.qn_size == 1, "the excited expander state supports one QN only"
+        ex = Mps.ground_state(self.model, False)
+        for _ in range(int(self.qntot[0])):
+            ex = Mpo.onsite(self.model, r"a^\dagger") @ ex
+        return ex
 
     @property
     def bond_dims_exact(self) -> np.ndarray:
@@ -842,13 +861,10 @@ class Mps:
         m_target = np.minimum(np.array(self.compress_config.max_dims) - np.array(self.bond_dims),
                               self.bond_dims_exact).astype(int)
         if hint_mpo is None:
-            expander = Mps.random(self.model, self.qntot, np.maximum(m_target, 1))
+            expander = self.__class__.random(self.model, self.qntot, np.maximum(m_target, 1))
         else:
             if include_ex:
-                assert self.model.qn_size == 1, "the excited expander state supports one QN only"
-                ex = Mps.ground_state(self.model, False)
-                for _ in range(int(self.qntot[0])):
-                    ex = Mpo.onsite(self.model, r"a^\dagger") @ ex
+                ex = self._expansion_ex_state()
                 ex.compress_config = self.compress_config
                 ex.move_qnidx(self.qnidx)
                 ex.to_right = self.to_right

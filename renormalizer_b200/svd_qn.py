@@ -309,7 +309,7 @@ class RefineOptions:
     its eigenvectors for sigma below ~sqrt(eps) ||X|| are mixed within that
     cluster, and the projected norms ||u^H X|| of such mixtures lie anywhere
     in the cluster's range.  When the truncation's cut (the smallest selected
-    sigma) lies below ``tau`` times the largest sigma, every block whose
+    sigma) lies below 2 ``tau`` times the largest sigma, every block whose
     projected sigma include values below ``tau`` times its own largest is
     refined: its cluster rows of P (sigma-scaled singular vectors, mutually
     orthogonal to within eps sigma_i sigma_j) are projected twice onto the
@@ -317,23 +317,21 @@ class RefineOptions:
     (entries of order sigma_cluster^2, accurate to eps relative) goes through
     the device eigensolver, and its eigenvectors rotate the cluster's kept
     basis and rows (K P is unchanged).  The refined sigma are accurate to
-    about sqrt(eps) tau ||X|| instead of sqrt(eps) ||X||.  ``tau`` = 0 turns
-    the pass off.
+    about sqrt(eps) tau ||X|| instead of sqrt(eps) ||X||, and the kept
+    vectors at such a cut are the true singular vectors (the reference's
+    gesdd choice): without the pass, an imaginary-time TDVP-PS2 step of a
+    density operator whose cut sits at 1e-7 moved its energy by 4e-8 against
+    the reference, with it by 3e-14.
 
-    ``always`` False (default): only truncations that keep every entry (the
-    singular values a caller reports, compress with an unbounded cap as in
-    calc_bond_singular_values) are refined.  In a sweep the cut of a nearly
-    product state falls among directions of weight ~1e-20 (the bond
-    expansion's 1e-10 padding), where every block would need a second
-    eigensolver pass of its whole cluster; those directions carry no weight
-    an observable can see, and their choice is rounding-sensitive in the
-    reference's LAPACK path as well.  ``always`` True refines wherever the cut
-    reaches a cluster."""
+    The pass runs however small the cut's weight: which directions a
+    truncation keeps at a cut of weight 1e-20 (the 1e-10 bond expansion of a
+    start state) sets the bond space that one-site TDVP then evolves in, and
+    with the Gram eigenvectors' choice there a TDVP-PS density-operator
+    trajectory left the reference's by 2e-4.  ``tau`` = 0 turns the pass off."""
 
-    def __init__(self, tau=1e-5, always=False):
+    def __init__(self, tau=1e-6):
         env = os.environ.get("RENO_REFINE_TAU")
         self.tau = float(env) if env else tau
-        self.always = always
         self.calls = 0
         self.blocks = 0
 
@@ -813,9 +811,7 @@ def _trunc_end(st, host):
         return sig, _select_by_code(sig, blk, [code_of[q] for q in visit_set], m_trunc_fn(sig), percent)
 
     sig, sidx = select()
-    keeps_all = len(sidx) >= sum(b["dim"] for b in blocks)
-    if refine.tau > 0 and (keeps_all or refine.always) and len(sidx) and sig.max() > 0 and \
-            sig[sidx].min() < 2 * refine.tau * sig.max():
+    if refine.tau > 0 and len(sidx) and sig.max() > 0 and sig[sidx].min() < 2 * refine.tau * sig.max():
         if _refine_clusters(eng, blocks, keep_left):
             sig, sidx = select()
     mdim = len(sidx)

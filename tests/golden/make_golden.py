@@ -451,6 +451,36 @@ def gen_obs(out):
     np.savez_compressed(out / "obs_cases.npz", **cases)
 
 
+def gen_mpdm(out):
+    """Finite temperature (mps/thermalprop.py, mps/mpdm.py): the T = infinity
+    one-exciton density operator of a 3-molecule Holstein chain, bonds
+    expanded with the Hamiltonian hint (ThermalProp's auto_expand), then
+    imaginary-time TDVP-PS / TDVP-PS2 steps towards beta / 2 at 298 K.  Stored:
+    the expanded start (4-index sites), and after every step the energy,
+    electronic and phonon occupations and bond entropies ThermalProp records."""
+    from renormalizer.mps import MpDm, ThermalProp
+    from renormalizer.utils import CompressConfig, CompressCriteria, EvolveConfig, EvolveMethod, Quantity
+    cases = {}
+    model = _holstein(3, 3, [(1.0, 1.0)])
+    beta = Quantity(298, "K").to_beta()
+    for tag, method, m in (("ps", EvolveMethod.tdvp_ps, 10), ("ps2", EvolveMethod.tdvp_ps2, 10)):
+        np.random.seed(7)
+        init = MpDm.max_entangled_ex(model)
+        init.compress_config = CompressConfig(CompressCriteria.fixed, max_bonddim=m)
+        tp = ThermalProp(init, evolve_config=EvolveConfig(method))
+        _dump_mps(f"{tag}/init", tp.latest_mps, cases)
+        nsteps, dbeta = 6, beta / 2j / 2000
+        tp.evolve(evolve_dt=dbeta, nsteps=nsteps)
+        cases[f"{tag}/dbeta"] = np.array(dbeta)
+        cases[f"{tag}/mmax"] = np.array(m)
+        cases[f"{tag}/energies"] = np.array(tp.energies)
+        cases[f"{tag}/e_occ"] = tp.e_occupations_array
+        cases[f"{tag}/ph_occ"] = tp.ph_occupations_array
+        cases[f"{tag}/entropy"] = tp.vn_entropy_array
+        cases[f"{tag}/bond_dims_final"] = np.array(tp.latest_mps.bond_dims)
+    np.savez_compressed(out / "mpdm_cases.npz", **cases)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -463,7 +493,7 @@ def main():
         gen_c1_traj(int(args.c1_traj[0]), args.c1_traj[1])
         return
     gens = dict(heff=gen_heff, env=gen_env, krylov=gen_krylov, svd=gen_svd, mpo=gen_mpo, tdvp=gen_tdvp,
-                dmrg=gen_dmrg, obs=gen_obs, configs=gen_configs)
+                dmrg=gen_dmrg, obs=gen_obs, configs=gen_configs, mpdm=gen_mpdm)
     for name, fn in gens.items():
         if args.only and name not in args.only.split(","):
             continue
