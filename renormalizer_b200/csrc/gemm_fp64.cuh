@@ -9,6 +9,8 @@
 // Operands are staged global -> shared with cp.async (zero-filled tails) in a
 // 3-stage ring; each warp owns a 32x32 output tile = 4x4 m8n8 fragments.
 #pragma once
+#include <algorithm>
+#include <type_traits>
 #include "reno_common.cuh"
 
 namespace reno {
@@ -294,6 +296,160 @@ inline cudaError_t gemm_fp64_grouped(fp64gemm::GemmGroup& g, cudaStream_t st) {
   if (ac) return fp64gemm::launch_grouped_t<true, false>(g, st);
   if (bc) return fp64gemm::launch_grouped_t<false, true>(g, st);
   return fp64gemm::launch_grouped_t<false, false>(g, st);
+}
+
+namespace fp64gemm {
+
+// Split-K for groups whose output tiles alone cannot fill the GPU (a few
+// rows by a few hundred columns summed over thousands of rows, as in the
+// V^H C products of blocked Householder QR): each such product is cut into
+// S chunks of its K range, the chunks run as separate group entries into
+// partial buffers, and one reduction launch sums the partials in chunk order
+// (deterministic), adding the old C when the product accumulates.
+constexpr int SPLITK_MAX = 16;
+constexpr int SPLITK_CHUNK = 256;  // smallest K range of a chunk
+
+struct SplitReduce {
+  int count;
+  struct Entry {
+    void* C;
+    const void* part;
+    int M, N, batch, S;
+    int64_t sCm, sCn, sCb;
+    int accumulate;
+  } e[MAX_GROUP];
+};
+
+template <bool CC>
+__global__ void splitk_reduce_kernel(const __grid_constant__ SplitReduce r) {
+  using T = typename std::conditional<CC, double2, double>::type;
+  const SplitReduce::Entry& E = r.e[blockIdx.y];
+  const int64_t n = (int64_t)E.M * E.N * E.batch;
+  const T* part = reinterpret_cast<const T*>(E.part);
+  T* C = reinterpret_cast<T*>(E.C);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int nn = (int)(i % E.N);
+    const int64_t rest = i / E.N;
+    const int m = (int)(rest % E.M);
+    const int64_t b = rest / E.M;
+    T acc = part[i];
+    for (int s = 1; s < E.S; ++s) {
+      const T x = part[(int64_t)s * n + i];
+      if constexpr (CC) {
+        acc.x += x.x;
+        acc.y += x.y;
+      } else {
+        acc += x;
+      }
+    }
+    T* c = C + b * E.sCb + (int64_t)m * E.sCm + (int64_t)nn * E.sCn;
+    if (E.accumulate) {
+      if constexpr (CC) {
+        acc.x += c->x;
+        acc.y += c->y;
+      } else {
+        acc += *c;
+      }
+    }
+    *c = acc;
+  }
+}
+
+// chunks per entry (1 = unsplit); returns the partial-buffer bytes
+inline size_t splitk_plan(const GemmGroup& g, int target_ctas, int* S) {
+  int64_t tiles = 0;
+  for (int i = 0; i < g.count; ++i) {
+    const GemmParams& p = g.p[i];
+    tiles += (p.M > 0 && p.N > 0) ? ceil_div(p.N, BN) * ceil_div(p.M, BM) * p.batch : 0;
+  }
+  const int want = tiles > 0 ? (int)std::min<int64_t>(SPLITK_MAX, ceil_div(target_ctas, tiles)) : 1;
+  for (int cap = want;; cap = std::max(1, cap / 2)) {
+    int total = 0;
+    for (int i = 0; i < g.count; ++i) {
+      const GemmParams& p = g.p[i];
+      S[i] = (p.M > 0 && p.N > 0 && tiles < target_ctas) ? std::max(1, std::min(cap, p.K / SPLITK_CHUNK)) : 1;
+      total += S[i];
+    }
+    if (total <= MAX_GROUP || cap == 1) break;
+  }
+  size_t bytes = 0;
+  for (int i = 0; i < g.count; ++i) {
+    const GemmParams& p = g.p[i];
+    const size_t es = (p.A.is_complex || p.B.is_complex) ? 16 : 8;
+    if (S[i] > 1) bytes += (size_t)S[i] * p.M * p.N * p.batch * es;
+  }
+  return bytes;
+}
+
+// upper bound of splitk_plan's bytes for a group of `count` entries of at most
+// M x N x batch outputs
+inline size_t splitk_bytes_bound(int count, int64_t mn_batch, bool complex_out) {
+  return (size_t)count * SPLITK_MAX * (size_t)mn_batch * (complex_out ? 16 : 8);
+}
+
+}  // namespace fp64gemm
+
+// gemm_fp64_grouped with split-K where the group's output tiles are fewer
+// than about two per SM; ws holds the partials (fp64gemm::splitk_plan bytes).
+inline cudaError_t gemm_fp64_grouped_splitk(fp64gemm::GemmGroup& g, void* ws, size_t ws_bytes, cudaStream_t st) {
+  using namespace fp64gemm;
+  if (g.count < 1 || g.count > MAX_GROUP) return cudaErrorInvalidValue;
+  int S[MAX_GROUP];
+  const size_t need = splitk_plan(g, 2 * sm_count_current_device(), S);
+  bool any = false;
+  for (int i = 0; i < g.count; ++i) any = any || S[i] > 1;
+  if (!any) return gemm_fp64_grouped(g, st);
+  if (need > ws_bytes || !ws) return cudaErrorInvalidValue;
+  GemmGroup x;
+  SplitReduce red{};
+  char* part = reinterpret_cast<char*>(ws);
+  const bool cc = g.p[0].A.is_complex || g.p[0].B.is_complex;
+  for (int i = 0; i < g.count; ++i) {
+    const GemmParams& p = g.p[i];
+    if (S[i] == 1) {
+      x.p[x.count++] = p;
+      continue;
+    }
+    const size_t esA = p.A.is_complex ? 16 : 8, esB = p.B.is_complex ? 16 : 8, esC = cc ? 16 : 8;
+    const int kc = (int)ceil_div(p.K, S[i]);
+    const int64_t n = (int64_t)p.M * p.N * p.batch;
+    int used = 0;
+    for (int s = 0; s < S[i]; ++s) {
+      const int k0 = s * kc, k1 = std::min(p.K, k0 + kc);
+      GemmParams q = p;
+      q.K = std::max(0, k1 - k0);
+      q.A.ptr = reinterpret_cast<const char*>(p.A.ptr) + (int64_t)k0 * p.A.s_k * (int64_t)esA;
+      q.B.ptr = reinterpret_cast<const char*>(p.B.ptr) + (int64_t)k0 * p.B.s_k * (int64_t)esB;
+      q.C = part + (size_t)s * n * esC;
+      q.sCm = p.N;
+      q.sCn = 1;
+      q.sCb = (int64_t)p.M * p.N;
+      q.accumulate = 0;
+      x.p[x.count++] = q;
+      ++used;
+    }
+    SplitReduce::Entry& e = red.e[red.count++];
+    e.C = p.C;
+    e.part = part;
+    e.M = p.M;
+    e.N = p.N;
+    e.batch = p.batch;
+    e.S = used;
+    e.sCm = p.sCm;
+    e.sCn = p.sCn;
+    e.sCb = p.sCb;
+    e.accumulate = p.accumulate;
+    part += (size_t)used * n * esC;
+  }
+  cudaError_t err = gemm_fp64_grouped(x, st);
+  if (err != cudaSuccess) return err;
+  int64_t nmax = 1;
+  for (int i = 0; i < red.count; ++i) nmax = std::max<int64_t>(nmax, (int64_t)red.e[i].M * red.e[i].N * red.e[i].batch);
+  const unsigned bx = (unsigned)std::min<int64_t>(ceil_div(nmax, 256), 64);
+  count_launch();
+  if (cc) splitk_reduce_kernel<true><<<dim3(bx, red.count), 256, 0, st>>>(red);
+  else splitk_reduce_kernel<false><<<dim3(bx, red.count), 256, 0, st>>>(red);
+  return cudaGetLastError();
 }
 
 // Launch the FP64 GEMM; returns a CUDA error code.

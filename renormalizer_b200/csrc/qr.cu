@@ -358,6 +358,7 @@ int panel_width(int mmax) {
 
 struct Layout {
   size_t off[RENO_QR_MAX_BLOCKS][7];
+  size_t split = 0, split_bytes = 0;  // split-K partials of the V^H products
   size_t total = 0;
   int nb = 0;
 };
@@ -394,6 +395,12 @@ int plan(int32_t count, const reno_qr_block* b, Layout& L, std::string& why) {
       o = al256(o + std::max<size_t>(sz[s], 1) * es);
     }
   }
+  size_t wmax = 1;
+  for (int i = 0; i < count; ++i)
+    wmax = std::max<size_t>(wmax, std::max<size_t>(std::max(b[i].k, std::min(b[i].m, b[i].k)), 1));
+  L.split = o;
+  L.split_bytes = fp64gemm::splitk_bytes_bound(count, (int64_t)L.nb * (int64_t)wmax, es == 16);
+  o = al256(o + L.split_bytes);
   L.total = o;
   return RENO_OK;
 }
@@ -506,7 +513,7 @@ extern "C" int reno_qr_blocks(reno_ctx* ctx, int32_t count, const reno_qr_block*
       g3.p[g3.count++] = c3;
     }
     if (g1.count) {
-      rc = check_cuda(ctx, gemm_fp64_grouped(g1, st), "reno_qr_blocks: V^H C");
+      rc = check_cuda(ctx, gemm_fp64_grouped_splitk(g1, ws + L.split, L.split_bytes, st), "reno_qr_blocks: V^H C");
       if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64_grouped(g2, st), "reno_qr_blocks: T^H W");
       if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64_grouped(g3, st), "reno_qr_blocks: C += V W");
       if (rc != RENO_OK) return rc;
@@ -555,7 +562,7 @@ extern "C" int reno_qr_blocks(reno_ctx* ctx, int32_t count, const reno_qr_block*
       g3.p[g3.count++] = c3;
     }
     if (!g1.count) continue;
-    rc = check_cuda(ctx, gemm_fp64_grouped(g1, st), "reno_qr_blocks: V^H Q");
+    rc = check_cuda(ctx, gemm_fp64_grouped_splitk(g1, ws + L.split, L.split_bytes, st), "reno_qr_blocks: V^H Q");
     if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64_grouped(g2, st), "reno_qr_blocks: T W");
     if (rc == RENO_OK) rc = check_cuda(ctx, gemm_fp64_grouped(g3, st), "reno_qr_blocks: Q += V W");
     if (rc != RENO_OK) return rc;

@@ -148,9 +148,10 @@ def expm_krylov_fixed(apply: Callable, dt: complex, v: torch.Tensor, k: int, nb:
     krylov.py:27-84, fixed length; stops early on the reference's breakdown
     test beta < 100 n eps, krylov.py:72-74, which also bounds the local
     Krylov space by the local dimension).  With ``nb`` = 1, v carries a
-    leading batch axis and every instance runs the same recurrence; the
-    breakdown test then needs all instances below the threshold (a local
-    dimension exhausts them together) and mixed outcomes are an error."""
+    leading batch axis and every instance runs the same recurrence; an
+    instance that breaks down while others go on gets beta_j = 0 and zero
+    vectors from there on, which decouples the rest of its tridiagonal matrix
+    (exp of a block-diagonal T), so its result is that of its own run."""
     vol = v[0].numel() if nb else v.numel()
     red = (lambda x: torch.linalg.vector_norm(x.reshape(x.shape[0], -1), dim=1)) if nb else torch.linalg.vector_norm
     bshape = (-1,) + (1,) * (v.dim() - 1) if nb else ()
@@ -171,8 +172,12 @@ def expm_krylov_fixed(apply: Callable, dt: complex, v: torch.Tensor, k: int, nb:
         small = (b.detach() < tiny)
         if bool(small.all()):
             break
-        if bool(small.any()):
-            raise ArithmeticError("batched Lanczos: the instances broke down at different steps")
+        if nb and bool(small.any()):
+            b = torch.where(small, torch.zeros_like(b), b)
+            safe = torch.where(small, torch.ones_like(b), b)
+            betas.append(b)
+            Q.append(torch.where(small.reshape(bshape), torch.zeros_like(w), w / safe.reshape(bshape)))
+            continue
         betas.append(b)
         Q.append(w / b.reshape(bshape))
     m = len(alphas)

@@ -83,3 +83,21 @@ def test_batched_trajectory_values_match_single_cpu(cpu_engine):
     for g, v in zip(gs, got):
         ref = trajectory_value(build(g), sites0, 0.1, 3, 0, op, krylov=8, contract="einsum")
         assert abs(v - ref) < 1e-13, (v, ref)
+
+
+def test_batched_lanczos_mixed_breakdown():
+    """an instance whose Krylov space is exhausted earlier than the others'
+    gets the result of its own run"""
+    from renormalizer_b200.tdvp_grad import expm_krylov_fixed
+    rng = np.random.default_rng(2)
+    h = rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6))
+    H = torch.as_tensor(h + h.conj().T)
+    low = torch.zeros((6, 6), dtype=torch.complex128)
+    low[:2, :2] = H[:2, :2]                       # Krylov space of dimension 2 from e_0
+    v = torch.zeros(6, dtype=torch.complex128)
+    v[0], v[1] = 1.0, 0.5j
+    Hs = torch.stack([H, low])
+    out = expm_krylov_fixed(lambda x: torch.einsum("bij,bj->bi", Hs, x), -0.3j, torch.stack([v, v]), 5, nb=1)
+    for i, M in enumerate((H, low)):
+        ref = expm_krylov_fixed(lambda x: M @ x, -0.3j, v, 5)
+        assert float((out[i] - ref).abs().max()) < 1e-13
