@@ -46,6 +46,13 @@ WORKLOAD = "holstein32x2modes_nlev16_M256_tdvp_ps2_dt0.025"
 # the engine on B200 (evolve_config.stat); used by the CPU extrapolation
 KRY2_DEFAULT = 8.0
 KRY1_DEFAULT = 8.0
+# the metric's accuracy gate, measured over 200 steps of this workload at 8
+# molecules by `bench.py --accuracy 200 --nmol 8 --start hint --accuracy-precs
+# bf16x3,tf32x3 --envelope` (52 min of B200 time: too long for this run);
+# per-step table in profiles/accuracy_tdvp_ps2_holstein24_M256.md
+ACCURACY_200 = {"steps": 200, "nmol": 8, "max_abs_dpop": {"bf16x3": 1.074e-5, "tf32x3": 7.99e-6},
+                "fp64_envelope": 1.63e-9, "first_step_above_1e-6": {"bf16x3": 24, "tf32x3": 29},
+                "holds_1e-6": False, "record": "profiles/accuracy_tdvp_ps2_holstein24_M256.md"}
 
 
 def parse():
@@ -661,7 +668,7 @@ def run_engine(args, rank, world, dist):
                 "krylov": kry_timed, "bond_dims_max": max(mps.bond_dims), "truncation": trunc,
                 "roofline": roofline, "truncation_roofline": trunc_roof, "peaks": peaks, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks.summary(), "fp64_engine": fp64}
+                "clocks": clocks.summary(), "fp64_engine": fp64, "accuracy": ACCURACY_200}
         print(json.dumps(line), flush=True)
 
 
