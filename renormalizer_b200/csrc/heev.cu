@@ -151,6 +151,7 @@ struct HetrdProb {
   double2* P;
   Sync* sync;
   int first, nblk;
+  double2* YP;  // lower-triangle reduction: YP_G x n partial sums of y (nullptr: not available)
 };
 // One matrix of the batched small-matrix reduction and of the batched
 // eigenvalue / eigenvector stages (blockIdx.y = entry).
@@ -408,6 +409,303 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
       const int c = k + 1 + tid + u * HT;
       yv[u] = c < n ? __ldcg(&Y[(size_t)(k & 1) * n + c]) : make_double2(0.0, 0.0);
       pre[u] = (next && c < n) ? __ldcg(&rown[c]) : make_double2(0.0, 0.0);
+    }
+    const double2 yk1 = __ldcg(&Y[(size_t)(k & 1) * n + k + 1]);
+    double2 dot = make_double2(0.0, 0.0);
+    for (int base = lane; base < G; base += 32 * U1) {
+      double2 pp[U1];
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int b = base + 32 * u;
+        pp[u] = b < G ? __ldcg(&P[(size_t)(k & 1) * G + b]) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < U1; ++u) dot = cadd(dot, pp[u]);
+    }
+    dot = warp_sum(dot);
+    const double t2 = tk.x * tk.x + tk.y * tk.y;
+    const double2 alph = make_double2(-0.5 * t2 * dot.x, -0.5 * t2 * dot.y);
+    for (int base = k + 1 + tid; base < n; base += U1 * HT) {
+      double2 y[U1];
+      if (base == k + 1 + tid) {
+#pragma unroll
+        for (int u = 0; u < U1; ++u) y[u] = yv[u];
+      } else {
+#pragma unroll
+        for (int u = 0; u < U1; ++u) {
+          const int c = base + u * HT;
+          y[u] = c < n ? __ldcg(&Y[(size_t)(k & 1) * n + c]) : make_double2(0.0, 0.0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int c = base + u * HT;
+        if (c < n) {
+          const double2 v = vc[c];
+          wp[c] = cadd(cmul(tk, y[u]), cmul(alph, v));
+          vp[c] = v;
+        }
+      }
+    }
+    tk_prev = tk;
+    alph_prev = alph;
+    yk_prev = yk1;
+  }
+  if (bid == 0 && tid == 0) {
+    if (n == 1) {
+      d[0] = __ldcg(&A[0]).x;
+    } else {
+      double2 a = __ldcg(&A[(size_t)(n - 1) * n + (n - 1)]);
+      a = csub(csub(a, cmulc(vp[n - 1], wp[n - 1])), cmulc(wp[n - 1], vp[n - 1]));
+      d[n - 1] = a.x;
+      __stcg(&A[(size_t)(n - 2) * n + (n - 1)], vp[n - 1]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- large matrices, lower triangle
+// The same lagged one-column-at-a-time reduction for large n, reading and
+// updating only the lower triangle of A: half the bytes per column, and a
+// 3584^2 complex matrix (205 MB in full) then stays in the 126 MB L2 instead
+// of streaming from HBM twice per column.  Element (r, c), c < r, adds
+// x v_c to y_r and conj(x) v_r to y_c; the diagonal adds x v_r to y_r.
+//   phase 1 (every CTA)  "row" k is column k of the lower triangle (strided
+//                        loads), update k-1 applied, reflector k;
+//   phase 2              the trailing rows dealt round-robin to the CTAs; each
+//                        warp owns column chunks of LCH columns (assigned in a
+//                        snake order for balance) and walks the CTA's rows
+//                        through them, two rows in flight: update k-1 stored,
+//                        the row's chunk share of y kept in shared memory and
+//                        the column contributions in the lanes' registers;
+//                        the CTA writes its partial y (columns, plus its rows'
+//                        sums in chunk order) to YP[bid][.];
+//   grid barrier;
+//   phase 2b             CTA b sums YP[0..G-1][i] for its slice of i (one warp
+//                        per entry, lanes over the CTAs, fixed shuffle tree),
+//                        writes y and its share of y^H v;
+//   grid barrier;
+//   phase 3 (every CTA)  w_k as before, with column k+1 loaded for phase 1.
+// Every reduction has a fixed order, so the result is the same on every run.
+constexpr int LU2 = 4;                 // loads in flight per lane per row of a chunk
+constexpr int LCH = 32 * LU2;          // columns per chunk
+constexpr int LPARTS = 2048;           // (row, chunk) partial sums per CTA
+constexpr int YP_G = 256;              // largest CTA count per matrix (YP rows)
+constexpr int LOWER_MIN_N = 1536;      // the lower-triangle kernel runs when the batch's largest n reaches this
+
+// one row of a phase-2 chunk: update k-1 on its lower-triangle entries
+// (a: their loaded values), stored back; the row's y share (warp-summed) is
+// returned and the column contributions added to col
+__device__ __forceinline__ double2 lower_row(double2* __restrict__ A, int r, int cs, int lane, int n,
+                                             const double2* vp, const double2* wp, const double2* vc,
+                                             const double2 (&a)[LU2], double2 (&col)[LU2]) {
+  const double2 vpr = vp[r], wpr = wp[r], vr = vc[r];
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int u = 0; u < LU2; ++u) {
+    const int c = cs + lane + 32 * u;
+    if (c <= r && c < n) {
+      const double2 x = csub(csub(a[u], cmulc(vpr, wp[c])), cmulc(wpr, vp[c]));
+      __stcg(&A[(size_t)r * n + c], x);
+      acc = cadd(acc, cmul(x, vc[c]));
+      if (c < r) col[u] = cadd(col[u], cmul(conjg(x), vr));
+    }
+  }
+  return warp_sum(acc);
+}
+
+__global__ void __launch_bounds__(HT, 1) hetrd_lower_kernel(const __grid_constant__ HetrdTable tab) {
+  int pi = 0;
+  while (pi + 1 < tab.count && (int)blockIdx.x >= tab.p[pi + 1].first) ++pi;
+  const HetrdProb& PR = tab.p[pi];
+  double2* __restrict__ A = PR.A;
+  const int n = PR.n;
+  double* __restrict__ d = PR.d;
+  double* __restrict__ e = PR.e;
+  double2* __restrict__ tau = PR.tau;
+  double2* __restrict__ Y = PR.Y;
+  double2* __restrict__ P = PR.P;
+  double2* __restrict__ YP = PR.YP;
+  Sync* sync = PR.sync;
+  const int bid = (int)blockIdx.x - PR.first;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* vp = reinterpret_cast<double2*>(smem_raw);  // v of step k-1 (pending update)
+  double2* wp = vp + n;                                // w of step k-1
+  double2* vc = wp + n;                                // v of step k
+  double2* parts = vc + n;                             // LPARTS (row, chunk) partial sums of y
+  __shared__ double red[HW];
+  __shared__ double2 redc[HW];
+  __shared__ double s_akk;
+  __shared__ int s_ok;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int G = PR.nblk;
+  unsigned gen = 0;
+  for (int i = tid; i < n; i += HT) {
+    vp[i] = make_double2(0.0, 0.0);
+    wp[i] = make_double2(0.0, 0.0);
+    vc[i] = make_double2(0.0, 0.0);
+  }
+  // column 0 of the lower triangle, the part phase 1 reads in its first pass
+  double2 pre[U1];
+#pragma unroll
+  for (int u = 0; u < U1; ++u) {
+    const int c = tid + u * HT;
+    pre[u] = c < n ? conjg(__ldcg(&A[(size_t)c * n])) : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  double2 tk_prev = make_double2(0.0, 0.0), alph_prev = make_double2(0.0, 0.0), yk_prev = make_double2(0.0, 0.0);
+  for (int k = 0; k < n - 1; ++k) {
+    // ---- phase 1 (every CTA): row k = conj(column k) with update k-1, reflector k
+    double2 vpk = make_double2(0.0, 0.0), wpk = make_double2(0.0, 0.0);
+    if (k > 0) {
+      vpk = make_double2(1.0, 0.0);
+      wpk = cadd(cmul(tk_prev, yk_prev), cmul(alph_prev, vpk));
+    }
+    double ss = 0.0;
+    for (int base = k + tid; base < n; base += U1 * HT) {
+      double2 a[U1];
+      if (base == k + tid) {
+#pragma unroll
+        for (int u = 0; u < U1; ++u) a[u] = pre[u];
+      } else {
+#pragma unroll
+        for (int u = 0; u < U1; ++u) {
+          const int c = base + u * HT;
+          a[u] = c < n ? conjg(__ldcg(&A[(size_t)c * n + k])) : make_double2(0.0, 0.0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int c = base + u * HT;
+        if (c < n) {
+          const double2 x = csub(csub(a[u], cmulc(vpk, wp[c])), cmulc(wpk, vp[c]));
+          if (c == k) {
+            s_akk = x.x;
+          } else {
+            const double2 xc = conjg(x);
+            vc[c] = xc;
+            if (c >= k + 2) ss += xc.x * xc.x + xc.y * xc.y;
+          }
+        }
+      }
+    }
+    ss = warp_sum(ss);
+    __syncthreads();
+    if (lane == 0) red[warp] = ss;
+    const double2 alpha = vc[k + 1];
+    __syncthreads();
+    ss = 0.0;
+#pragma unroll
+    for (int w = 0; w < HW; ++w) ss += red[w];
+    double beta;
+    double2 tk, sc;
+    if (ss == 0.0 && alpha.y == 0.0) {
+      tk = make_double2(0.0, 0.0);
+      sc = make_double2(0.0, 0.0);
+      beta = alpha.x;
+    } else {
+      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+      tk = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+      const double2 den = make_double2(alpha.x - beta, alpha.y);
+      const double m2 = den.x * den.x + den.y * den.y;
+      sc = make_double2(den.x / m2, -den.y / m2);
+    }
+    if (bid == 0 && tid == 0) {
+      d[k] = s_akk;
+      e[k] = beta;
+      tau[k] = tk;
+    }
+    // own entries of vc: v_k; reflector k-1 into row k-1 (upper triangle, which
+    // this kernel never reads)
+    for (int c = k + tid; c < n; c += HT) {
+      if (c > k) vc[c] = (c == k + 1) ? make_double2(1.0, 0.0) : cmul(vc[c], sc);
+      if (bid == 0 && k > 0) __stcg(&A[(size_t)(k - 1) * n + c], vp[c]);
+    }
+    __syncthreads();
+
+    // ---- phase 2: update k-1 on the lower triangle of this CTA's rows; partial y
+    const int nrow = n - k - 1;
+    const int nr_c = nrow > bid ? (nrow - bid + G - 1) / G : 0;
+    const int nch = (nrow + LCH - 1) / LCH;
+    double2* yp = YP + (size_t)bid * n;
+    // chunk ch of warp w: ch = w + 2 HW t or 2 HW - 1 - w + 2 HW t
+    for (int t = 0; 2 * HW * t + warp < nch; ++t) {
+#pragma unroll 1
+      for (int q = 0; q < 2; ++q) {
+        const int ch = q == 0 ? 2 * HW * t + warp : 2 * HW * t + 2 * HW - 1 - warp;
+        if (ch >= nch) continue;
+        const int cs = k + 1 + ch * LCH;
+        double2 col[LU2];
+#pragma unroll
+        for (int u = 0; u < LU2; ++u) col[u] = make_double2(0.0, 0.0);
+        // first own row reaching this chunk: r_j >= cs
+        const int j0 = cs - (k + 1 + bid) > 0 ? (cs - (k + 1 + bid) + G - 1) / G : 0;
+        for (int j = j0; j < nr_c; j += 2) {
+          const int r1 = k + 1 + bid + j * G;
+          const bool two = j + 1 < nr_c;
+          const int r2 = two ? r1 + G : r1;
+          double2 a1[LU2], a2[LU2];
+#pragma unroll
+          for (int u = 0; u < LU2; ++u) {
+            const int c = cs + lane + 32 * u;
+            a1[u] = (c <= r1 && c < n) ? __ldcg(&A[(size_t)r1 * n + c]) : make_double2(0.0, 0.0);
+            a2[u] = (two && c <= r2 && c < n) ? __ldcg(&A[(size_t)r2 * n + c]) : make_double2(0.0, 0.0);
+          }
+          double2 acc = lower_row(A, r1, cs, lane, n, vp, wp, vc, a1, col);
+          if (lane == 0) parts[j * nch + ch] = acc;
+          if (two) {
+            acc = lower_row(A, r2, cs, lane, n, vp, wp, vc, a2, col);
+            if (lane == 0) parts[(j + 1) * nch + ch] = acc;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < LU2; ++u) {
+          const int c = cs + lane + 32 * u;
+          if (c < n) __stcg(&yp[c], col[u]);
+        }
+      }
+    }
+    __syncthreads();
+    // this CTA's rows: add their sums over the chunks they reach, in chunk order
+    for (int j = tid; j < nr_c; j += HT) {
+      const int r = k + 1 + bid + j * G;
+      const int chmax = (r - k - 1) / LCH;
+      double2 s = __ldcg(&yp[r]);
+      double2 rs = make_double2(0.0, 0.0);
+      for (int ch = 0; ch <= chmax; ++ch) rs = cadd(rs, parts[j * nch + ch]);
+      __stcg(&yp[r], cadd(s, rs));
+    }
+    if (!grid_sync(sync, (unsigned)G, gen, &s_ok, tab.wait_ns, pi == 0 && bid == 0 && k == tab.skip_column)) return;
+
+    // ---- phase 2b: y_i = sum over the CTAs' partials, one warp per entry of this CTA's slice
+    const int sl = (nrow + G - 1) / G;
+    const int i0 = k + 1 + bid * sl, i1 = min(n, i0 + sl);
+    double2 pdot = make_double2(0.0, 0.0);
+    for (int i = i0 + warp; i < i1; i += HW) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int b = lane; b < G; b += 32) acc = cadd(acc, __ldcg(&YP[(size_t)b * n + i]));
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        __stcg(&Y[(size_t)(k & 1) * n + i], acc);
+        pdot = cadd(pdot, cmulc(vc[i], acc));
+      }
+    }
+    if (lane == 0) redc[warp] = pdot;
+    __syncthreads();
+    if (tid == 0) {
+      double2 sum = make_double2(0.0, 0.0);
+      for (int w = 0; w < HW; ++w) sum = cadd(sum, redc[w]);
+      __stcg(&P[(size_t)(k & 1) * G + bid], sum);
+    }
+    if (!grid_sync(sync, (unsigned)G, gen, &s_ok, tab.wait_ns, false)) return;
+
+    // ---- phase 3 (every CTA): w_k; column k+1 loaded for the next phase 1
+    const bool next = k + 2 < n;
+    double2 yv[U1];
+#pragma unroll
+    for (int u = 0; u < U1; ++u) {
+      const int c = k + 1 + tid + u * HT;
+      yv[u] = c < n ? __ldcg(&Y[(size_t)(k & 1) * n + c]) : make_double2(0.0, 0.0);
+      pre[u] = (next && c < n) ? conjg(__ldcg(&A[(size_t)c * n + k + 1])) : make_double2(0.0, 0.0);
     }
     const double2 yk1 = __ldcg(&Y[(size_t)(k & 1) * n + k + 1]);
     double2 dot = make_double2(0.0, 0.0);
@@ -909,7 +1207,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 namespace {
 struct HeevLayout {
-  size_t sync, y, p, bnd, scr, s, t, w1, w2, total;
+  size_t sync, y, p, yp, bnd, scr, s, t, w1, w2, total;
 };
 HeevLayout heev_layout(int n, int kt) {
   HeevLayout L{};
@@ -921,6 +1219,8 @@ HeevLayout heev_layout(int n, int kt) {
   off += align256(2 * (size_t)n * sizeof(double2));
   L.p = off;
   off += align256(2 * 1024 * sizeof(double2));
+  L.yp = off;  // partial sums of the lower-triangle reduction (grid path only)
+  off += n > NMAX_C ? align256((size_t)YP_G * n * sizeof(double2)) : 0;
   L.bnd = off;
   off += align256(4 * sizeof(double));
   L.scr = off;
@@ -949,28 +1249,54 @@ GemmOperand op(const void* p, int64_t s_outer, int64_t s_k, int conj) {
 }  // namespace
 
 // Cooperative launch of the reduction over the matrices of tab (n > NMAX_C):
-// one CTA per SM, the SMs shared out in proportion to each matrix's n^2.
+// one CTA per SM, the SMs shared out in proportion to each matrix's n^2.  When
+// the largest matrix has at least LOWER_MIN_N rows the lower-triangle kernel
+// runs (each matrix then needs enough CTAs that its rows' (row, chunk)
+// partials fit LPARTS, and at most YP_G); otherwise the full-row kernel.
 static int launch_hetrd(reno_ctx* ctx, HetrdTable& tab, int nmax, const char* what) {
-  static std::atomic<unsigned long long> hetrd_set{0};
+  static std::atomic<unsigned long long> hetrd_set{0}, lower_set{0};
   int rc = check_cuda(ctx, smem_optin_once(hetrd_kernel, (3 * MAX_N + PARTS) * 16, hetrd_set),
                       (std::string(what) + ": hetrd smem attribute").c_str());
+  if (rc == RENO_OK)
+    rc = check_cuda(ctx, smem_optin_once(hetrd_lower_kernel, (3 * MAX_N + LPARTS) * 16, lower_set),
+                    (std::string(what) + ": hetrd smem attribute").c_str());
   if (rc != RENO_OK) return rc;
-  const size_t smem = (3 * (size_t)nmax + PARTS) * sizeof(double2);
+  const int G = std::min(sm_count_current_device(), 1024);
+  if (tab.count > G) return set_error(ctx, RENO_ERR_INVALID, std::string(what) + ": more matrices than SMs");
+  // CTAs a matrix needs under the lower-triangle kernel
+  auto gmin_lower = [](int n) {
+    const int nch = (int)ceil_div(n - 1, LCH);
+    const int rows = std::max(1, LPARTS / std::max(nch, 1));
+    return (int)ceil_div(n - 1, rows);
+  };
+  bool lower = nmax >= LOWER_MIN_N;
+  int need = 0;
+  for (int i = 0; i < tab.count; ++i) {
+    if (!tab.p[i].YP) lower = false;
+    need += gmin_lower(tab.p[i].n);
+  }
+  if (need > G) lower = false;
+  void* kfn = lower ? (void*)hetrd_lower_kernel : (void*)hetrd_kernel;
+  const size_t smem = (3 * (size_t)nmax + (lower ? LPARTS : PARTS)) * sizeof(double2);
   int per_sm = 0;
-  rc = check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_kernel, HT, smem),
+  rc = check_cuda(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, HT, smem),
                   (std::string(what) + ": occupancy").c_str());
   if (rc != RENO_OK) return rc;
   if (per_sm < 1) return set_error(ctx, RENO_ERR_INVALID, std::string(what) + ": hetrd kernel does not fit on an SM");
-  const int G = std::min(sm_count_current_device(), 1024);
-  if (tab.count > G) return set_error(ctx, RENO_ERR_INVALID, std::string(what) + ": more matrices than SMs");
   double work = 0.0;
   for (int i = 0; i < tab.count; ++i) work += (double)tab.p[i].n * tab.p[i].n;
-  int used = 0;
+  int used = 0, reserved = 0;
+  if (lower)
+    for (int i = 0; i < tab.count; ++i) reserved += gmin_lower(tab.p[i].n);
   for (int i = 0; i < tab.count; ++i) {
     const int left = tab.count - 1 - i;  // at least one CTA for every later matrix
+    const int floor_i = lower ? gmin_lower(tab.p[i].n) : 1;
+    if (lower) reserved -= floor_i;
+    const int later = lower ? reserved : left;
     int nb = i == tab.count - 1 ? G - used
                                 : (int)std::lround(G * (double)tab.p[i].n * tab.p[i].n / std::max(work, 1.0));
-    nb = std::max(1, std::min(nb, G - used - left));
+    nb = std::max(floor_i, std::min(nb, G - used - later));
+    if (lower) nb = std::min(nb, YP_G);
     tab.p[i].first = used;
     tab.p[i].nblk = nb;
     used += nb;
@@ -979,8 +1305,7 @@ static int launch_hetrd(reno_ctx* ctx, HetrdTable& tab, int nmax, const char* wh
   tab.skip_column = g_skip_hetrd_column.exchange(-1);
   void* args[] = {&tab};
   count_launch();
-  return check_cuda(ctx, cudaLaunchCooperativeKernel((void*)hetrd_kernel, dim3(used), dim3(HT), args, smem,
-                                                     ctx->stream),
+  return check_cuda(ctx, cudaLaunchCooperativeKernel(kfn, dim3(used), dim3(HT), args, smem, ctx->stream),
                     (std::string(what) + ": hetrd launch").c_str());
 }
 
@@ -1078,7 +1403,8 @@ extern "C" int reno_heev_top(reno_ctx* ctx, int32_t n, int32_t kt, void* A, doub
   } else {
     HetrdTable tab{};
     tab.count = 1;
-    tab.p[0] = HetrdProb{static_cast<double2*>(A), n, d, e, static_cast<double2*>(tau), Y, P, sync, 0, 0};
+    tab.p[0] = HetrdProb{static_cast<double2*>(A), n, d, e, static_cast<double2*>(tau), Y, P, sync, 0, 0,
+                         reinterpret_cast<double2*>(base + L.yp)};
     rc = launch_hetrd(ctx, tab, n, "reno_heev_top");
   }
   if (rc != RENO_OK) return rc;
@@ -1128,7 +1454,7 @@ extern "C" int reno_heev_top_batched(reno_ctx* ctx, int32_t count, const reno_he
     } else {
       tab.p[tab.count++] = HetrdProb{static_cast<double2*>(p.a), p.n, p.d, p.e, static_cast<double2*>(p.tau),
                                      reinterpret_cast<double2*>(base + L.y), reinterpret_cast<double2*>(base + L.p),
-                                     sync, 0, 0};
+                                     sync, 0, 0, reinterpret_cast<double2*>(base + L.yp)};
       nmax = std::max(nmax, (int)p.n);
     }
   }

@@ -100,3 +100,27 @@ def test_svd_truncate_device_eigensolver_matches_cusolver(keep_left):
     kept = got.left if keep_left else got.right.mH
     eye = torch.eye(kcap, dtype=kept.dtype, device=kept.device)
     assert float((kept.mH @ kept - eye).abs().max()) < 1e-12
+
+
+@pytest.mark.gpu
+def test_heev_batched_mixed_sizes_lower_triangle_reduction():
+    """a batch whose largest matrix takes the lower-triangle reduction kernel
+    (n >= 1536) with smaller ones sharing the launch: every matrix meets the
+    single-matrix bounds, and the batch is reproducible bit for bit"""
+    from renormalizer_b200._native import Engine
+    from renormalizer_b200.heev import accepted, heev_top_batched
+    sizes, kts = (1700, 400, 2100, 300), (320, 100, 320, 64)
+    Gs = [_gram(n, True, "generic" if i % 2 == 0 else "nearly_product", seed=31 + i) for i, n in enumerate(sizes)]
+    eng = Engine.get(Gs[0].device)
+    res = heev_top_batched(eng, Gs, list(kts))
+    res2 = heev_top_batched(eng, Gs, list(kts))
+    torch.cuda.synchronize()
+    for G, kt, (w, K, chk), (w2, K2, _) in zip(Gs, kts, res, res2):
+        assert accepted(chk.cpu().numpy()), chk.cpu().numpy()
+        assert torch.equal(w, w2) and torch.equal(K, K2)
+        ref = torch.flip(torch.linalg.eigvalsh(G), dims=[0])[:kt]
+        scale = float(ref.abs().max())
+        assert float((w - ref).abs().max()) <= 1e-13 * scale
+        assert float((G @ K - K * w).abs().max()) <= 1e-12 * scale
+        eye = torch.eye(kt, dtype=torch.complex128, device="cuda")
+        assert float((K.mH @ K - eye).abs().max()) <= 1e-12

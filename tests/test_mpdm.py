@@ -7,12 +7,13 @@ The T = infinity one-exciton density operator of a 3-molecule Holstein chain
 at 298 K, TDVP-PS and TDVP-PS2, energy offset updated every step as
 ThermalProp does).  From the reference's expanded start the engine must give
 the same energies, electronic and phonon occupations and bond entropies
-after every step: 1e-10 for TDVP-PS2, and for TDVP-PS 5e-8, the size of the
+after every step: 1e-10 for TDVP-PS2, and for TDVP-PS 2e-7, twice the
 reference's own spread on this run (the reference against itself from a
-start perturbed by one ulp per entry: 9.4e-9 in the energies, 2.4e-8 in the
-occupations after 6 steps; 3e-15 for TDVP-PS2: the one-site sweep keeps the
-start's 1e-10-weight expansion directions, whose rounding the imaginary-time
-steps amplify).  The engine's own start (MpDm.max_entangled_ex, ThermalProp's
+start perturbed by one ulp per entry, three draws: up to 1.1e-8 in the
+energies, 2.7e-8 in the electronic and 1.0e-7 in the phonon occupations after
+6 steps; 3e-15 for TDVP-PS2: the one-site sweep keeps the start's
+1e-10-weight expansion directions, whose rounding the imaginary-time steps
+amplify).  The engine's own start (MpDm.max_entangled_ex, ThermalProp's
 canonicalisation and Hamiltonian-hint bond expansion) must reproduce the
 reference's TDVP-PS2 trajectory to 1e-10.
 
@@ -134,7 +135,7 @@ def _ancilla_contractions(dev):
 def test_mpdm_host_logic(cpu_engine):
     _ancilla_contractions("cpu")
     _run("ps2", 1e-10)
-    _run("ps", 5e-8)
+    _run("ps", 2e-7)
     _own_start(1e-10)
 
 
@@ -146,7 +147,7 @@ def test_ancilla_contractions_gpu():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tag,tol", [("ps", 5e-8), ("ps2", 1e-10)])
+@pytest.mark.parametrize("tag,tol", [("ps", 2e-7), ("ps2", 1e-10)])
 def test_thermal_prop_matches_reference_gpu(tag, tol):
     from renormalizer_b200 import backend
     backend.prec = "fp64"
