@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
   }
 }
 
-// ---------------------------------------------------------------- large matrices, lower triangle
+// ---------------------------------------------------------------- large matrices (n >= 3072), lower triangle
 // The same lagged one-column-at-a-time reduction for large n, reading and
 // updating only the lower triangle of A: half the bytes per column, and a
 // 3584^2 complex matrix (205 MB in full) then stays in the 126 MB L2 instead
@@ -490,7 +490,7 @@ constexpr int LU2 = 4;                 // loads in flight per lane per row of a 
 constexpr int LCH = 32 * LU2;          // columns per chunk
 constexpr int LPARTS = 2048;           // (row, chunk) partial sums per CTA
 constexpr int YP_G = 256;              // largest CTA count per matrix (YP rows)
-constexpr int LOWER_MIN_N = 1536;      // the lower-triangle kernel runs when the batch's largest n reaches this
+constexpr int LOWER_MIN_N = 3072;      // the lower-triangle kernel runs when the batch's largest n reaches this
 
 // one row of a phase-2 chunk: update k-1 on its lower-triangle entries
 // (a: their loaded values), stored back; the row's y share (warp-summed) is
@@ -681,8 +681,16 @@ __global__ void __launch_bounds__(HT, 1) hetrd_lower_kernel(const __grid_constan
     const int i0 = k + 1 + bid * sl, i1 = min(n, i0 + sl);
     double2 pdot = make_double2(0.0, 0.0);
     for (int i = i0 + warp; i < i1; i += HW) {
+      // G <= YP_G = 8 x 32: every lane's partials are loaded before any is summed
+      double2 part[YP_G / 32];
+#pragma unroll
+      for (int u = 0; u < YP_G / 32; ++u) {
+        const int b = lane + 32 * u;
+        part[u] = b < G ? __ldcg(&YP[(size_t)b * n + i]) : make_double2(0.0, 0.0);
+      }
       double2 acc = make_double2(0.0, 0.0);
-      for (int b = lane; b < G; b += 32) acc = cadd(acc, __ldcg(&YP[(size_t)b * n + i]));
+#pragma unroll
+      for (int u = 0; u < YP_G / 32; ++u) acc = cadd(acc, part[u]);
       acc = warp_sum(acc);
       if (lane == 0) {
         __stcg(&Y[(size_t)(k & 1) * n + i], acc);

@@ -40,6 +40,7 @@ from .model import Model, Op
 from .mpo import Mpo
 from .svd_qn import (qn_sectors, add_outer, get_qn_mask, qr_split, select_basis_indices, svd_truncate,
                      svd_truncate_batch)
+from .svd_qn import refine as svd_refine
 
 logger = logging.getLogger(__name__)
 
@@ -517,7 +518,7 @@ class Mps:
         cfg = self.compress_config
         return dict(coef=cstruct, qnbigl=qnbigl, qnbigr=qnbigr, qntot=self.qntot, keep_left=left,
                     m_trunc_fn=lambda s: cfg.compute_m_trunc(s, bond_site, left), percent=percent,
-                    kcap=cfg.fixed_cap(bond_site, left))
+                    kcap=cfg.fixed_cap(bond_site, left), refine_floor=svd_refine.sweep_floor)
 
     def _place_truncation(self, res, cidx: List[int], qnbigl, qnbigr):
         """the kept / complementary parts of a truncation into the sites (mp.py:779-888)"""

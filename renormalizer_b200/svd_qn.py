@@ -323,15 +323,21 @@ class RefineOptions:
     density operator whose cut sits at 1e-7 moved its energy by 4e-8 against
     the reference, with it by 3e-14.
 
-    The pass runs however small the cut's weight: which directions a
-    truncation keeps at a cut of weight 1e-20 (the 1e-10 bond expansion of a
-    start state) sets the bond space that one-site TDVP then evolves in, and
-    with the Gram eigenvectors' choice there a TDVP-PS density-operator
-    trajectory left the reference's by 2e-4.  ``tau`` = 0 turns the pass off."""
+    Compressions (bond expansion, canonical compress) refine however small
+    the cut's weight: which directions they keep at a cut of weight 1e-20
+    (the 1e-10 bond expansion of a start state) sets the bond space that
+    one-site TDVP then evolves in, and with the Gram eigenvectors' choice
+    there a TDVP-PS density-operator trajectory left the reference's by 2e-4.
+    The two-site sweeps pass ``sweep_floor``: a cut below 1e-9 of the largest
+    sigma (weight below 1e-18, the early steps from a bond-expanded start,
+    where nearly every truncation would otherwise run the pass) is left as
+    the Gram eigenvectors give it; the next step's two-site tensor chooses
+    those directions anew.  ``tau`` = 0 turns the pass off."""
 
-    def __init__(self, tau=1e-6):
+    def __init__(self, tau=1e-6, sweep_floor=1e-9):
         env = os.environ.get("RENO_REFINE_TAU")
         self.tau = float(env) if env else tau
+        self.sweep_floor = sweep_floor
         self.calls = 0
         self.blocks = 0
 
@@ -557,7 +563,7 @@ def _full_kept_side(eng: Engine, X: torch.Tensor, keep_left: bool, ktop: Optiona
 
 
 def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_trunc_fn, percent=0,
-                 full_matrices=True, kcap: Optional[int] = None):
+                 full_matrices=True, kcap: Optional[int] = None, refine_floor: float = 0.0):
     """Fused svd_qn + compute_m_trunc + select_basis of mp.py:693-778.
 
     keep_left=True keeps U (left-to-right sweep: left = U, right = sigma Vh);
@@ -573,8 +579,12 @@ def svd_truncate(coef: torch.Tensor, qnbigl, qnbigr, qntot, keep_left: bool, m_t
     is threshold-based) lets large blocks use the top-k subspace solver
     (``subspace`` options); its residual norms come to the host with the
     singular values and a block whose Ritz pairs miss the tolerance is redone
-    with the full decomposition."""
-    st = _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent, full_matrices, kcap)
+    with the full decomposition.
+
+    ``refine_floor``: a cut below this fraction of the largest sigma skips the
+    small-sigma refinement (RefineOptions) unless every entry is kept."""
+    st = _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent, full_matrices, kcap,
+                      refine_floor)
     _trunc_eig([st])
     host = torch.cat(_trunc_host_tensors(st)).cpu().numpy()
     return _trunc_end(st, host)
@@ -599,7 +609,8 @@ def svd_truncate_batch(calls) -> List["TruncatedSplit"]:
     return out
 
 
-def _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent=0, full_matrices=True, kcap=None):
+def _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent=0, full_matrices=True, kcap=None,
+                 refine_floor=0.0):
     """Gather the QN blocks of one truncation (the subspace blocks, when that
     opt-in route applies, are factorised here)."""
     eng = Engine.get(coef.device)
@@ -638,6 +649,7 @@ def _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent=0, 
     if not blocks:
         raise ValueError("Invalid quantum number")
     return dict(eng=eng, coef=coef, rows=rows, cols=cols, keep_left=keep_left, m_trunc_fn=m_trunc_fn,
+                refine_floor=refine_floor,
                 percent=percent, blocks=blocks, pending=pending)
 
 
@@ -811,7 +823,9 @@ def _trunc_end(st, host):
         return sig, _select_by_code(sig, blk, [code_of[q] for q in visit_set], m_trunc_fn(sig), percent)
 
     sig, sidx = select()
-    if refine.tau > 0 and len(sidx) and sig.max() > 0 and sig[sidx].min() < 2 * refine.tau * sig.max():
+    keeps_all = len(sidx) >= sum(b["dim"] for b in blocks)
+    if refine.tau > 0 and len(sidx) and sig.max() > 0 and sig[sidx].min() < 2 * refine.tau * sig.max() and \
+            (keeps_all or sig[sidx].min() >= st["refine_floor"] * sig.max()):
         if _refine_clusters(eng, blocks, keep_left):
             sig, sidx = select()
     mdim = len(sidx)

@@ -105,11 +105,11 @@ def test_svd_truncate_device_eigensolver_matches_cusolver(keep_left):
 @pytest.mark.gpu
 def test_heev_batched_mixed_sizes_lower_triangle_reduction():
     """a batch whose largest matrix takes the lower-triangle reduction kernel
-    (n >= 1536) with smaller ones sharing the launch: every matrix meets the
+    (n >= 3072) with smaller ones sharing the launch: every matrix meets the
     single-matrix bounds, and the batch is reproducible bit for bit"""
     from renormalizer_b200._native import Engine
     from renormalizer_b200.heev import accepted, heev_top_batched
-    sizes, kts = (1700, 400, 2100, 300), (320, 100, 320, 64)
+    sizes, kts = (3200, 400, 2100, 300), (320, 100, 320, 64)
     Gs = [_gram(n, True, "generic" if i % 2 == 0 else "nearly_product", seed=31 + i) for i, n in enumerate(sizes)]
     eng = Engine.get(Gs[0].device)
     res = heev_top_batched(eng, Gs, list(kts))
