@@ -38,8 +38,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 # DRAM bytes (read + write) of one phonon-phonon 2-site matvec at M = 256,
-# d = 16 x 16, from an ncu capture of the four split_gemm_kernel launches
-TRAFFIC_PH_PH = {"bf16x3": 3.998e9}
+# d = 16 x 16, from ncu captures of the four split_gemm_kernel launches (the
+# same 4.00 GB in both captures recorded in
+# profiles/split_gemm_fused_heff2_ph_ph_M256_bf16x3.md); ncu cannot run
+# inside this timed region
+TRAFFIC_PH_PH = {"bf16x3": 4.00e9}
 METRIC = "TDVP steps/s at M=256 (2-site TDVP-PS, 32-site two-mode Holstein, split-prec vs FP64)"
 WORKLOAD = "holstein32x2modes_nlev16_M256_tdvp_ps2_dt0.025"
 # average Krylov vectors per local exponential of this workload, measured by
