@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(HT, 1) hetrd_kernel(const __grid_constant__ He
   }
 }
 
-// ---------------------------------------------------------------- large matrices (n >= 1536), lower triangle
+// ---------------------------------------------------------------- large matrices (n >= 3072), lower triangle
 // The same lagged one-column-at-a-time reduction for large n, reading and
 // updating only the lower triangle of A: half the bytes per column, and a
 // 3584^2 complex matrix (205 MB in full) then stays in the 126 MB L2 instead
@@ -491,7 +491,7 @@ constexpr int LU2 = 4;                 // loads in flight per lane per row of a 
 constexpr int LCH = 32 * LU2;          // columns per chunk
 constexpr int LPARTS = 2048;           // (row, chunk) partial sums per CTA
 constexpr int YP_G = 256;              // largest CTA count per matrix (YP rows)
-constexpr int LOWER_MIN_N = 1536;      // the lower-triangle kernel runs when the batch's largest n reaches this
+constexpr int LOWER_MIN_N = 3072;      // the lower-triangle kernel runs when the batch's largest n reaches this
 
 // one row of a phase-2 chunk: update k-1 on its lower-triangle entries
 // (a: their loaded values), stored back; the row's y share (warp-summed) is

@@ -105,7 +105,7 @@ def test_svd_truncate_device_eigensolver_matches_cusolver(keep_left):
 @pytest.mark.gpu
 def test_heev_batched_mixed_sizes_lower_triangle_reduction():
     """a batch whose largest matrix takes the lower-triangle reduction kernel
-    (n >= 1536) with smaller ones sharing the launch: every matrix meets the
+    (n >= 3072) with smaller ones sharing the launch: every matrix meets the
     single-matrix bounds, and the batch is reproducible bit for bit"""
     from renormalizer_b200._native import Engine
     from renormalizer_b200.heev import accepted, heev_top_batched
