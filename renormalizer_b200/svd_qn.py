@@ -346,6 +346,10 @@ class RefineOptions:
 
 
 refine = RefineOptions()
+# eigenpairs computed beyond a block's fixed cap k (a block contributes at most
+# k entries to the selection; the others only fill the list the rule reads).
+# RENO_TOP_MARGIN overrides it.
+TOP_MARGIN = int(os.environ.get("RENO_TOP_MARGIN", "64"))
 # when a list, svd_truncate appends the algorithmic FP64 flops of each call's
 # block factorisations (see _block_flops)
 flop_log = None
@@ -645,7 +649,7 @@ def _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent=0, 
             blocks.append(dict(nl=nl, nr=nr, lset=lset, rset=rset, K=K, P=P, S=S, dim=ksub, npad=npad, res=chk,
                                X=X, Q=Q))
             continue
-        ktop = kcap + 64 if kcap is not None and kcap + 64 < dim else None
+        ktop = kcap + TOP_MARGIN if kcap is not None and kcap + TOP_MARGIN < dim else None
         blk = dict(nl=nl, nr=nr, lset=lset, rset=rset, dim=dim, npad=npad, X=X, ktop=ktop)
         blocks.append(blk)
         pending.append(blk)
