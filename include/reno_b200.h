@@ -396,6 +396,51 @@ int reno_vec_precond(reno_ctx* ctx, int64_t n, int32_t dtype, const void* r,
                      void* out);
 
 /* ------------------------------------------------------------------------
+ * Grouped vector kernels: one operation on up to RENO_VEC_GROUP_MAX
+ * independent vectors of their own lengths and types in one or two launches
+ * (the Lanczos exponentials of many static-disorder realisations advanced
+ * in lockstep; the reference runs krylov.py:27-84 once per realisation).
+ * Every item's result is bitwise the one of the single call above: the same
+ * per-item block partition and summation order.
+ *   RENO_VOP_NORM      scalars[0] = ||x||                 (reno_vec_norm)
+ *   RENO_VOP_ALPHA     scalars[2j] = Re vdot(x, y)        (reno_krylov_alpha,
+ *                      x = w, y = v, scalars = ab)
+ *   RENO_VOP_ORTH      out -= ab[2j] x + ab[2j-1] y;  ab[2j+1] = ||out||
+ *                      (reno_krylov_orth, out = w, x = v, y = vprev,
+ *                      scalars = ab)
+ *   RENO_VOP_SCALE_INV out = x / s[0]                     (reno_vec_scale_inv)
+ *   RENO_VOP_LINCOMB   out = sum_{i<j} s[2i..2i+1] x[i ldv ..] (reno_vec_lincomb,
+ *                      k = j vectors)
+ *   RENO_VOP_ALLCLOSE  scalars[0] = allclose(x, y, rtol, atol)
+ *                      (reno_vec_allclose)
+ * workspace: reno_vec_grouped_workspace_bytes(count) bytes.
+ * ---------------------------------------------------------------------- */
+enum {
+  RENO_VOP_NORM = 0,
+  RENO_VOP_ALPHA = 1,
+  RENO_VOP_ORTH = 2,
+  RENO_VOP_SCALE_INV = 3,
+  RENO_VOP_LINCOMB = 4,
+  RENO_VOP_ALLCLOSE = 5
+};
+#define RENO_VEC_GROUP_MAX 128
+typedef struct {
+  int64_t n;           /* elements of each vector of this item */
+  int32_t dtype;       /* RENO_F64 or RENO_C128 */
+  int32_t j;           /* Krylov index (ALPHA, ORTH); vector count (LINCOMB) */
+  const void* x;
+  const void* y;
+  void* out;
+  double* scalars;
+  const double* s;
+  int64_t ldv;         /* LINCOMB: row stride of x in elements */
+} reno_vec_item;
+int reno_vec_grouped_workspace_bytes(int32_t count, size_t* bytes);
+int reno_vec_grouped(reno_ctx* ctx, int32_t op, int32_t count,
+                     const reno_vec_item* items, double rtol, double atol,
+                     void* workspace, size_t ws_bytes);
+
+/* ------------------------------------------------------------------------
  * Quantum-number block movers (svd_qn.py:177-213, 89-96; lib.py:302-316).
  * reno_qn_gather: out[i, j] = src[rows[i] * ld + cols[j]]   (nr x nc, dense out)
  * reno_qn_scatter: dst[rows[i] * dst_rs + dcols[j] * dst_cs] =

@@ -52,6 +52,15 @@ class HeevProblem(ctypes.Structure):
 HEEV_MAX_BATCH = 32
 
 
+class VecItem(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("dtype", ctypes.c_int32), ("j", ctypes.c_int32), ("x", _vp), ("y", _vp),
+                ("out", _vp), ("scalars", _vp), ("s", _vp), ("ldv", ctypes.c_int64)]
+
+
+VEC_GROUP_MAX = 128
+VOP_NORM, VOP_ALPHA, VOP_ORTH, VOP_SCALE_INV, VOP_LINCOMB, VOP_ALLCLOSE = range(6)
+
+
 class EnvDesc(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in
                 ("side", "d", "w_in", "w_out", "mk_in", "mk_out", "mb_in", "mb_out", "env_dtype", "ket_dtype",
@@ -112,6 +121,9 @@ _SIGS = {
                                    _c_sz]),
     "reno_vec_axpy": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, ctypes.c_double]),
     "reno_vec_precond": (_c_int, [_vp, _c_i64, _c_int, _vp, _vp, _vp, ctypes.c_double, _vp]),
+    "reno_vec_grouped_workspace_bytes": (_c_int, [_c_int, ctypes.POINTER(_c_sz)]),
+    "reno_vec_grouped": (_c_int, [_vp, _c_int, _c_int, ctypes.POINTER(VecItem), ctypes.c_double, ctypes.c_double,
+                                  _vp, _c_sz]),
     "reno_qn_gather": (_c_int, [_vp, _c_int, _vp, _c_i64, _vp, _c_i64, _vp, _c_i64, _vp]),
     "reno_qn_scatter": (_c_int, [_vp, _c_int, _vp, _c_i64, _c_i64, _vp, _c_i64, _vp, _vp, _c_i64, _vp, _vp, _c_i64,
                                  _c_i64]),
@@ -223,6 +235,7 @@ class Engine:
         self._stream_handle = None
         self._ws = None
         self._vec_ws = None
+        self._vec_gws = None
         self.scalars = torch.zeros(4096, dtype=torch.float64, device=f"cuda:{device}")
         self.launches = 0
 
@@ -457,6 +470,23 @@ class Engine:
     def precond(self, r, hdiag, e, shift, out):
         self.check(self.lib.reno_vec_precond(self.ctx, r.numel(), dtype_code(r), ptr(r), ptr(hdiag), ptr(e), shift,
                                              ptr(out)), "reno_vec_precond")
+
+    def vec_grouped(self, op, items, rtol=0.0, atol=0.0):
+        """One vector operation on many problems (reno_vec_grouped), in chunks
+        of VEC_GROUP_MAX.  items: tuples (n, dtype, j, x, y, out, scalars, s,
+        ldv) of sizes and tensors (None where the operation has no operand)."""
+        for c0 in range(0, len(items), VEC_GROUP_MAX):
+            chunk = items[c0:c0 + VEC_GROUP_MAX]
+            arr = (VecItem * len(chunk))()
+            for k, (n, dt, j, x, y, out, sc, sv, ldv) in enumerate(chunk):
+                arr[k] = VecItem(n, dt, j, ptr(x), ptr(y), ptr(out), ptr(sc), ptr(sv), ldv)
+            nbytes = _c_sz()
+            self.check(self.lib.reno_vec_grouped_workspace_bytes(len(chunk), ctypes.byref(nbytes)),
+                       "reno_vec_grouped_workspace_bytes")
+            if self._vec_gws is None or self._vec_gws.numel() < nbytes.value:
+                self._vec_gws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=f"cuda:{self.device}")
+            self.check(self.lib.reno_vec_grouped(self.ctx, op, len(chunk), arr, rtol, atol, ptr(self._vec_gws),
+                                                 self._vec_gws.numel()), "reno_vec_grouped")
 
     # quantum-number block movers
     def qn_gather(self, mat, rows, cols, out):

@@ -51,32 +51,113 @@ __device__ __forceinline__ double2 block_sum(double2 v) {
   return r;  // valid in thread 0
 }
 
+// Per-block bodies shared by the single and the grouped kernels: block b of
+// the nb blocks that cover one vector walks i = b VT + t, stepping nb VT.
+// Their arithmetic is written with explicitly rounded operations, so no
+// kernel that inlines them can contract it into FMAs differently: a grouped
+// call rounds exactly like the single one.
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // mode 0: sum conj(x) y ; mode 1: sum |x|^2 (in .x)
-__global__ void dot_partial(int64_t n, bool cplx, const void* x, const void* y, int mode, double2* part) {
+__device__ __forceinline__ double2 dot_body(int64_t n, bool cplx, const void* x, const void* y, int mode, int64_t b,
+                                            int64_t nb) {
   double2 acc = make_double2(0.0, 0.0);
-  for (int64_t i = blockIdx.x * (int64_t)VT + threadIdx.x; i < n; i += (int64_t)gridDim.x * VT) {
+  for (int64_t i = b * VT + threadIdx.x; i < n; i += nb * VT) {
     const double2 a = ld2(x, i, cplx);
     if (mode == 0) {
-      const double2 b = ld2(y, i, cplx);
-      acc.x += a.x * b.x + a.y * b.y;
-      acc.y += a.x * b.y - a.y * b.x;
+      const double2 c = ld2(y, i, cplx);
+      acc.x = add_(acc.x, fma_(a.x, c.x, mul_(a.y, c.y)));
+      acc.y = add_(acc.y, fma_(a.x, c.y, -mul_(a.y, c.x)));
     } else {
-      acc.x += a.x * a.x + a.y * a.y;
+      acc.x = add_(acc.x, fma_(a.x, a.x, mul_(a.y, a.y)));
     }
   }
-  const double2 r = block_sum(acc);
+  return acc;
+}
+
+// w -= ab[2j] * v + ab[2j-1] * vprev ; partial |w|^2
+__device__ __forceinline__ double2 orth_body(int64_t n, bool cplx, void* w, const void* v, const void* vprev,
+                                             const double* ab, int j, int64_t b, int64_t nb) {
+  const double alpha = ab[2 * j];
+  const double beta = j > 0 ? ab[2 * j - 1] : 0.0;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int64_t i = b * VT + threadIdx.x; i < n; i += nb * VT) {
+    const double2 vi = ld2(v, i, cplx);
+    double2 t = make_double2(mul_(alpha, vi.x), mul_(alpha, vi.y));
+    if (j > 0) {
+      const double2 pi = ld2(vprev, i, cplx);
+      t.x = fma_(beta, pi.x, t.x);
+      t.y = fma_(beta, pi.y, t.y);
+    }
+    double2 wi = ld2(w, i, cplx);
+    wi.x = add_(wi.x, -t.x);
+    wi.y = add_(wi.y, -t.y);
+    st2(w, i, cplx, wi);
+    acc.x = add_(acc.x, fma_(wi.x, wi.x, mul_(wi.y, wi.y)));
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void scale_inv_body(int64_t n, bool cplx, const void* x, const double* s, void* out,
+                                               int64_t b, int64_t nb) {
+  const double inv = s[0];
+  for (int64_t i = b * VT + threadIdx.x; i < n; i += nb * VT) {
+    double2 v = ld2(x, i, cplx);
+    v.x /= inv;
+    v.y /= inv;
+    st2(out, i, cplx, v);
+  }
+}
+
+__device__ __forceinline__ void lincomb_body(int64_t n, int k, bool cplx, const void* V, int64_t ldv,
+                                             const double* coef, void* out, int64_t b, int64_t nb) {
+  for (int64_t i = b * VT + threadIdx.x; i < n; i += nb * VT) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int j = 0; j < k; ++j) {
+      const double2 v = ld2(V, (int64_t)j * ldv + i, cplx);
+      const double cr = coef[2 * j], ci = coef[2 * j + 1];
+      acc.x = add_(acc.x, fma_(cr, v.x, -mul_(ci, v.y)));
+      acc.y = add_(acc.y, fma_(cr, v.y, mul_(ci, v.x)));
+    }
+    st2(out, i, cplx, acc);
+  }
+}
+
+// count of elements violating |a-b| <= atol + rtol |b|
+__device__ __forceinline__ double2 allclose_body(int64_t n, bool cplx, const void* a, const void* b_, double rtol,
+                                                 double atol, int64_t b, int64_t nb) {
+  double2 acc = make_double2(0.0, 0.0);
+  for (int64_t i = b * VT + threadIdx.x; i < n; i += nb * VT) {
+    const double2 x = ld2(a, i, cplx), y = ld2(b_, i, cplx);
+    const double dx = x.x - y.x, dy = x.y - y.y;
+    const double diff = cplx ? hypot(dx, dy) : fabs(dx);
+    const double mag = cplx ? hypot(y.x, y.y) : fabs(y.x);
+    if (!(diff <= fma_(rtol, mag, atol))) acc.x += 1.0;
+  }
+  return acc;
+}
+
+// second pass: the nb partials in a fixed order (valid in thread 0)
+__device__ __forceinline__ double2 final_sum(int nb, const double2* part) {
+  double2 acc = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < nb; i += VT) {
+    acc.x = add_(acc.x, part[i].x);
+    acc.y = add_(acc.y, part[i].y);
+  }
+  return block_sum(acc);
+}
+
+__global__ void dot_partial(int64_t n, bool cplx, const void* x, const void* y, int mode, double2* part) {
+  const double2 r = block_sum(dot_body(n, cplx, x, y, mode, blockIdx.x, gridDim.x));
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
 
 // finalize: mode 0 -> out[0..1] = sum ; mode 1 -> out[0] = sqrt(sum) ;
 // mode 2 -> out[0] = sum.x (real part of a dot)
 __global__ void dot_final(int nb, const double2* part, int mode, double* out) {
-  double2 acc = make_double2(0.0, 0.0);
-  for (int i = threadIdx.x; i < nb; i += VT) {
-    acc.x += part[i].x;
-    acc.y += part[i].y;
-  }
-  const double2 r = block_sum(acc);
+  const double2 r = final_sum(nb, part);
   if (threadIdx.x == 0) {
     if (mode == 0) {
       out[0] = r.x;
@@ -89,74 +170,95 @@ __global__ void dot_final(int nb, const double2* part, int mode, double* out) {
   }
 }
 
-// w -= ab[2j] * v + ab[2j-1] * vprev ; partial |w|^2
 __global__ void orth_partial(int64_t n, bool cplx, void* w, const void* v, const void* vprev, const double* ab,
                              int j, double2* part) {
-  const double alpha = ab[2 * j];
-  const double beta = j > 0 ? ab[2 * j - 1] : 0.0;
-  double2 acc = make_double2(0.0, 0.0);
-  for (int64_t i = blockIdx.x * (int64_t)VT + threadIdx.x; i < n; i += (int64_t)gridDim.x * VT) {
-    const double2 vi = ld2(v, i, cplx);
-    double2 t = make_double2(alpha * vi.x, alpha * vi.y);
-    if (j > 0) {
-      const double2 pi = ld2(vprev, i, cplx);
-      t.x += beta * pi.x;
-      t.y += beta * pi.y;
-    }
-    double2 wi = ld2(w, i, cplx);
-    wi.x -= t.x;
-    wi.y -= t.y;
-    st2(w, i, cplx, wi);
-    acc.x += wi.x * wi.x + wi.y * wi.y;
-  }
-  const double2 r = block_sum(acc);
+  const double2 r = block_sum(orth_body(n, cplx, w, v, vprev, ab, j, blockIdx.x, gridDim.x));
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
 
 __global__ void scale_inv_kernel(int64_t n, bool cplx, const void* x, const double* s, void* out) {
-  const double inv = s[0];
-  for (int64_t i = blockIdx.x * (int64_t)VT + threadIdx.x; i < n; i += (int64_t)gridDim.x * VT) {
-    double2 v = ld2(x, i, cplx);
-    v.x /= inv;
-    v.y /= inv;
-    st2(out, i, cplx, v);
-  }
+  scale_inv_body(n, cplx, x, s, out, blockIdx.x, gridDim.x);
 }
 
 __global__ void lincomb_kernel(int64_t n, int k, bool cplx, const void* V, int64_t ldv, const double* coef,
                                void* out) {
-  for (int64_t i = blockIdx.x * (int64_t)VT + threadIdx.x; i < n; i += (int64_t)gridDim.x * VT) {
-    double2 acc = make_double2(0.0, 0.0);
-    for (int j = 0; j < k; ++j) {
-      const double2 v = ld2(V, (int64_t)j * ldv + i, cplx);
-      const double cr = coef[2 * j], ci = coef[2 * j + 1];
-      acc.x += cr * v.x - ci * v.y;
-      acc.y += cr * v.y + ci * v.x;
-    }
-    st2(out, i, cplx, acc);
-  }
+  lincomb_body(n, k, cplx, V, ldv, coef, out, blockIdx.x, gridDim.x);
 }
 
-// count of elements violating |a-b| <= atol + rtol |b|
 __global__ void allclose_partial(int64_t n, bool cplx, const void* a, const void* b, double rtol, double atol,
                                  double2* part) {
-  double2 acc = make_double2(0.0, 0.0);
-  for (int64_t i = blockIdx.x * (int64_t)VT + threadIdx.x; i < n; i += (int64_t)gridDim.x * VT) {
-    const double2 x = ld2(a, i, cplx), y = ld2(b, i, cplx);
-    const double dx = x.x - y.x, dy = x.y - y.y;
-    const double diff = cplx ? hypot(dx, dy) : fabs(dx);
-    const double mag = cplx ? hypot(y.x, y.y) : fabs(y.x);
-    if (!(diff <= atol + rtol * mag)) acc.x += 1.0;
-  }
-  const double2 r = block_sum(acc);
+  const double2 r = block_sum(allclose_body(n, cplx, a, b, rtol, atol, blockIdx.x, gridDim.x));
   if (threadIdx.x == 0) part[blockIdx.x] = r;
 }
 
 __global__ void allclose_final(int nb, const double2* part, double* flag) {
-  double2 acc = make_double2(0.0, 0.0);
-  for (int i = threadIdx.x; i < nb; i += VT) acc.x += part[i].x;
-  const double2 r = block_sum(acc);
+  const double2 r = final_sum(nb, part);
   if (threadIdx.x == 0) flag[0] = r.x == 0.0 ? 1.0 : 0.0;
+}
+
+// ---------------------------------------------------------------- grouped
+// One operation on many vectors: item p owns blocks first[p] .. first[p+1]-1
+// of the launch (its single call's vec_blocks(n) of them, in the same order)
+// and slots first[p].. of the partial-sum workspace.
+struct VecGroup {
+  reno_vec_item it[RENO_VEC_GROUP_MAX];
+  int first[RENO_VEC_GROUP_MAX + 1];
+  int count, op;
+  double rtol, atol;
+};
+
+__device__ __forceinline__ int group_item(const VecGroup& g, int blk) {
+  int lo = 0, hi = g.count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (g.first[mid] <= blk) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void vec_group_partial(const __grid_constant__ VecGroup g, double2* part) {
+  const int p = group_item(g, blockIdx.x);
+  const reno_vec_item& it = g.it[p];
+  const int64_t b = blockIdx.x - g.first[p], nb = g.first[p + 1] - g.first[p];
+  const bool cplx = it.dtype == RENO_C128;
+  double2 acc;
+  if (g.op == RENO_VOP_NORM)
+    acc = dot_body(it.n, cplx, it.x, it.x, 1, b, nb);
+  else if (g.op == RENO_VOP_ALPHA)
+    acc = dot_body(it.n, cplx, it.x, it.y, 0, b, nb);
+  else if (g.op == RENO_VOP_ORTH)
+    acc = orth_body(it.n, cplx, it.out, it.x, it.y, it.scalars, it.j, b, nb);
+  else
+    acc = allclose_body(it.n, cplx, it.x, it.y, g.rtol, g.atol, b, nb);
+  const double2 r = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void vec_group_final(const __grid_constant__ VecGroup g, const double2* part) {
+  const int p = blockIdx.x;
+  const reno_vec_item& it = g.it[p];
+  const double2 r = final_sum(g.first[p + 1] - g.first[p], part + g.first[p]);
+  if (threadIdx.x == 0) {
+    if (g.op == RENO_VOP_NORM)
+      it.scalars[0] = sqrt(r.x);
+    else if (g.op == RENO_VOP_ALPHA)
+      it.scalars[2 * it.j] = r.x;
+    else if (g.op == RENO_VOP_ORTH)
+      it.scalars[2 * it.j + 1] = sqrt(r.x);
+    else
+      it.scalars[0] = r.x == 0.0 ? 1.0 : 0.0;
+  }
+}
+
+__global__ void vec_group_elementwise(const __grid_constant__ VecGroup g) {
+  const int p = group_item(g, blockIdx.x);
+  const reno_vec_item& it = g.it[p];
+  const int64_t b = blockIdx.x - g.first[p], nb = g.first[p + 1] - g.first[p];
+  const bool cplx = it.dtype == RENO_C128;
+  if (g.op == RENO_VOP_SCALE_INV)
+    scale_inv_body(it.n, cplx, it.x, it.s, it.out, b, nb);
+  else
+    lincomb_body(it.n, it.j, cplx, it.x, it.ldv, it.s, it.out, b, nb);
 }
 
 __global__ void axpy_kernel(int64_t n, bool cplx, void* y, const void* x, const double* c, double sgn) {
@@ -287,4 +389,54 @@ extern "C" int reno_vec_precond(reno_ctx* ctx, int64_t n, int32_t dtype, const v
   count_launch(1);
   precond_kernel<<<vec_blocks(n), VT, 0, ctx->stream>>>(n, dtype == RENO_C128, r, hdiag, e, shift, out);
   return check_cuda(ctx, cudaGetLastError(), "reno_vec_precond");
+}
+
+extern "C" int reno_vec_grouped_workspace_bytes(int32_t count, size_t* bytes) {
+  if (!bytes || count < 0 || count > RENO_VEC_GROUP_MAX) return RENO_ERR_INVALID;
+  *bytes = (size_t)(count > 0 ? count : 1) * VMAX_BLOCKS * sizeof(double2);
+  return RENO_OK;
+}
+
+extern "C" int reno_vec_grouped(reno_ctx* ctx, int32_t op, int32_t count, const reno_vec_item* items, double rtol,
+                                double atol, void* ws, size_t ws_bytes) {
+  if (!ctx) return RENO_ERR_INVALID;
+  if (op < RENO_VOP_NORM || op > RENO_VOP_ALLCLOSE || count < 0 || count > RENO_VEC_GROUP_MAX ||
+      (count > 0 && !items))
+    return set_error(ctx, RENO_ERR_INVALID, "reno_vec_grouped: bad op or count");
+  if (count == 0) return RENO_OK;
+  const bool reduces = op != RENO_VOP_SCALE_INV && op != RENO_VOP_LINCOMB;
+  if (reduces && (!ws || ws_bytes < (size_t)count * VMAX_BLOCKS * sizeof(double2)))
+    return set_error(ctx, RENO_ERR_WORKSPACE, "reno_vec_grouped: workspace too small");
+  VecGroup g;
+  g.count = count;
+  g.op = op;
+  g.rtol = rtol;
+  g.atol = atol;
+  int total = 0;
+  for (int p = 0; p < count; ++p) {
+    const reno_vec_item& it = items[p];
+    bool ok = dt_ok(it.dtype) && it.n >= 0;
+    switch (op) {
+      case RENO_VOP_NORM: ok = ok && it.x && it.scalars; break;
+      case RENO_VOP_ALPHA: ok = ok && it.x && it.y && it.scalars && it.j >= 0; break;
+      case RENO_VOP_ORTH: ok = ok && it.out && it.x && it.scalars && it.j >= 0 && (it.j == 0 || it.y); break;
+      case RENO_VOP_SCALE_INV: ok = ok && it.x && it.s && it.out; break;
+      case RENO_VOP_LINCOMB: ok = ok && it.x && it.s && it.out && it.j >= 0 && it.ldv >= it.n; break;
+      default: ok = ok && it.x && it.y && it.scalars; break;
+    }
+    if (!ok) return set_error(ctx, RENO_ERR_INVALID, "reno_vec_grouped: bad item " + std::to_string(p));
+    g.it[p] = it;
+    g.first[p] = total;
+    total += vec_blocks(it.n);
+  }
+  g.first[count] = total;
+  if (reduces) {
+    count_launch(2);
+    vec_group_partial<<<total, VT, 0, ctx->stream>>>(g, (double2*)ws);
+    vec_group_final<<<count, VT, 0, ctx->stream>>>(g, (const double2*)ws);
+  } else {
+    count_launch(1);
+    vec_group_elementwise<<<total, VT, 0, ctx->stream>>>(g);
+  }
+  return check_cuda(ctx, cudaGetLastError(), "reno_vec_grouped");
 }

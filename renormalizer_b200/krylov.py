@@ -185,26 +185,186 @@ def expm_krylov_batch(group_apply, dts, vstarts, block_size=50):
     Krylov vectors xs of the problems idx (a list) to their images, normally
     in one grouped launch (hop_expr.apply_grouped); ``dts`` is one step for
     all or one per problem.  Returns [(vector, number of matvecs)] in input
-    order, each identical to that problem's own expm_krylov."""
+    order, each identical to that problem's own expm_krylov.
+
+    All problems start together, so at every round they sit at the same
+    Krylov index j: each vector operation of a round is one grouped launch
+    (reno_vec_grouped, every problem's result bitwise its single call's), and
+    the host reads the scalars of all problems that reach a check point
+    (every even j > 3, or the end of their Krylov space) in one transfer."""
     m = len(vstarts)
     if np.ndim(dts) == 0:
         dts = [dts] * m
-    gens = [_expm_krylov_steps(dt, v, block_size) for dt, v in zip(dts, vstarts)]
-    out = [None] * m
-    pending = {}
-    for i, g in enumerate(gens):
-        try:
-            pending[i] = next(g)
-        except StopIteration as stop:
-            out[i] = stop.value
-    while pending:
-        idx = sorted(pending)
-        ys = group_apply(idx, [pending[i] for i in idx])
-        nxt = {}
-        for i, y in zip(idx, ys):
-            try:
-                nxt[i] = gens[i].send(y)
-            except StopIteration as stop:
-                out[i] = stop.value
-        pending = nxt
-    return out
+    if m == 0:
+        return []
+    return _LockstepKrylov(dts, vstarts, block_size).run(group_apply)
+
+
+class _LockstepKrylov:
+    """The state of expm_krylov (_expm_krylov_steps) for m problems, with the
+    alpha/beta arrays of all problems in one device array AB (row p) and the
+    start norms / allclose flags in SC (columns 0 / 2)."""
+
+    def __init__(self, dts, vstarts, block_size):
+        from ._native import VOP_NORM, VOP_SCALE_INV
+        self.block_size = block_size
+        self.dts, self.vs, self.n, self.dtype = [], [], [], []
+        for dt, v0 in zip(dts, vstarts):
+            if not np.iscomplex(dt):
+                dt = dt.real
+            v = as_device(v0).reshape(-1)
+            dt_cplx = np.iscomplexobj(dt) and np.iscomplex(dt)
+            work_dtype = torch.complex128 if (v.is_complex() or dt_cplx) else torch.float64
+            if v.dtype != work_dtype:
+                v = v.to(work_dtype)
+            self.dts.append(dt)
+            self.vs.append(v)
+            self.n.append(v.numel())
+            self.dtype.append(work_dtype)
+        dev = self.vs[0].device
+        assert all(v.device == dev for v in self.vs), "lockstep problems share one device"
+        self.device = dev
+        self.eng = Engine.get(dev)
+        m = len(self.vs)
+        self.V = [torch.empty((block_size, n), dtype=dt, device=dev) for n, dt in zip(self.n, self.dtype)]
+        self.AB = torch.zeros((m, 2 * block_size + 2), dtype=torch.float64, device=dev)
+        self.SC = torch.zeros((m, 4), dtype=torch.float64, device=dev)
+        self.out = [(torch.empty(n, dtype=dt, device=dev), torch.empty(n, dtype=dt, device=dev))
+                    for n, dt in zip(self.n, self.dtype)]
+        self.nrmv = [None] * m
+        self.checked = [0] * m
+        self.res = [None] * m
+        # nrmv = ||vstart|| ; V[0] = vstart / nrmv
+        self._op(VOP_NORM, [(p, 0, self.vs[p], None, None, self.SC[p], None) for p in range(m)])
+        self._op(VOP_SCALE_INV, [(p, 0, self.vs[p], None, self.V[p][0], None, self.SC[p]) for p in range(m)])
+
+    def _code(self, p):
+        from ._native import RENO_C128, RENO_F64
+        return RENO_C128 if self.dtype[p] == torch.complex128 else RENO_F64
+
+    def _op(self, op, rows, rtol=0.0, atol=0.0):
+        """rows: (p, j, x, y, out, scalars, s) per problem"""
+        if rows:
+            self.eng.vec_grouped(op, [(self.n[p], self._code(p), j, x, y, out, sc, s, self.n[p])
+                                      for p, j, x, y, out, sc, s in rows], rtol, atol)
+
+    def _grow(self, p):
+        bs = self.block_size
+        V = torch.empty((self.V[p].shape[0] + bs, self.n[p]), dtype=self.dtype[p], device=self.device)
+        V[: self.V[p].shape[0]] = self.V[p]
+        self.V[p] = V
+        need = 2 * V.shape[0] + 2
+        if self.AB.shape[1] < need:
+            AB = torch.zeros((self.AB.shape[0], need), dtype=torch.float64, device=self.device)
+            AB[:, : self.AB.shape[1]] = self.AB
+            self.AB = AB
+
+    def _coeffs(self, p, alpha, beta, k):
+        a, b = alpha[: k + 1], beta[:k]
+        if not (np.all(np.isfinite(a)) and np.all(np.isfinite(b))):
+            raise FloatingPointError("expm_krylov: Lanczos scalars are not finite")
+        return _tridiag_coeffs(a, b, self.nrmv[p], self.dts[p])
+
+    def _breakdown_before(self, p, j, beta):
+        for i in range(self.checked[p], j):
+            if beta[i] < 100 * self.n[p] * EPS:
+                return i
+        self.checked[p] = j
+        return None
+
+    def _combine(self, jobs):
+        """jobs: (p, k, coeffs, out) -> out = V[p][:k] @ coeffs, one grouped launch"""
+        from ._native import VOP_LINCOMB
+        if not jobs:
+            return
+        cs = []
+        for _, k, coeffs, _ in jobs:
+            c = np.zeros(2 * k)
+            c[0::2] = np.real(coeffs)
+            c[1::2] = np.imag(coeffs) if np.iscomplexobj(coeffs) else 0.0
+            cs.append(c)
+        flat = np.concatenate(cs)
+        coef = h2d(flat, self.device) if self.device.type == "cuda" else torch.from_numpy(flat)
+        rows, off = [], 0
+        for (p, k, _, out), c in zip(jobs, cs):
+            rows.append((p, k, self.V[p], None, out, None, coef[off: off + c.size]))
+            off += c.size
+        self._op(VOP_LINCOMB, rows)
+
+    def run(self, group_apply):
+        from ._native import VOP_ALLCLOSE, VOP_ALPHA, VOP_ORTH, VOP_SCALE_INV
+        m = len(self.vs)
+        result = [None] * m
+        active = list(range(m))
+        j = 0
+        while active:
+            ws = group_apply(active, [self.V[p][j] for p in active])
+            W = {}
+            for p, w in zip(active, ws):
+                w = w.reshape(-1)
+                if w.dtype != self.dtype[p]:
+                    w = w.to(self.dtype[p])
+                if not w.is_contiguous():
+                    w = w.contiguous()
+                W[p] = w
+            self._op(VOP_ALPHA, [(p, j, W[p], self.V[p][j], None, self.AB[p], None) for p in active])
+            term = [p for p in active if j == self.n[p] - 1]
+            cont = [p for p in active if j < self.n[p] - 1]
+            for p in cont:
+                if self.V[p].shape[0] == j + 1:
+                    self._grow(p)
+            self._op(VOP_ORTH, [(p, j, self.V[p][j], self.V[p][j - 1] if j > 0 else None, W[p], self.AB[p], None)
+                                for p in cont])
+            self._op(VOP_SCALE_INV, [(p, 0, W[p], None, self.V[p][j + 1], None, self.AB[p][2 * j + 1:])
+                                     for p in cont])
+            check = cont if (3 < j and j % 2 == 0) else []
+            finished = set()
+            if term or check:
+                ab = self.AB[:, : 2 * j + 2].cpu().numpy()
+                if any(self.nrmv[p] is None for p in term + check):
+                    sc = self.SC[:, 0].cpu().numpy()
+                    for p in term + check:
+                        if self.nrmv[p] is None:
+                            nrmv = float(sc[p])
+                            assert nrmv > 0
+                            if not np.isfinite(nrmv):
+                                raise FloatingPointError("expm_krylov: start vector is not finite")
+                            self.nrmv[p] = nrmv
+                jobs, tests = [], []
+                for p in term:
+                    alpha, beta = ab[p, 0::2], ab[p, 1::2]
+                    i = self._breakdown_before(p, j, beta)
+                    k = j if i is None else i
+                    out = self.out[p][0]
+                    jobs.append((p, k + 1, self._coeffs(p, alpha, beta, k), out))
+                    result[p] = (out, k + 1)
+                    finished.add(p)
+                for p in check:
+                    alpha, beta = ab[p, 0::2], ab[p, 1::2]
+                    i = self._breakdown_before(p, j + 1, beta)
+                    if i is not None:
+                        out = self.out[p][0]
+                        jobs.append((p, i + 1, self._coeffs(p, alpha, beta, i), out))
+                        result[p] = (out, i + 1)
+                        finished.add(p)
+                        continue
+                    coeffs = self._coeffs(p, alpha, beta, j)
+                    prev = self.res[p]
+                    a, b = self.out[p]
+                    new = b if prev is a else a
+                    jobs.append((p, j + 1, coeffs, new))
+                    if prev is not None:
+                        tests.append((p, prev, new))
+                    self.res[p] = new
+                self._combine(jobs)
+                if tests:
+                    self._op(VOP_ALLCLOSE, [(p, 0, prev, new, None, self.SC[p][2:], None) for p, prev, new in tests],
+                             tolerance.rtol, tolerance.atol)
+                    flags = self.SC[:, 2].cpu().numpy()
+                    for p, _, new in tests:
+                        if flags[p] == 1.0:
+                            result[p] = (new, j + 1)
+                            finished.add(p)
+            active = [p for p in cont if p not in finished]
+            j += 1
+        return result

@@ -129,6 +129,23 @@ class FakeEngine:
     def allclose(self, a, b, rtol, atol, flag):
         flag[0] = 1.0 if bool(torch.all(torch.abs(a - b) <= atol + rtol * torch.abs(b))) else 0.0
 
+    def vec_grouped(self, op, items, rtol=0.0, atol=0.0):
+        """reno_vec_grouped: the single operation on every item, in order"""
+        for n, dt, j, x, y, out, sc, s, ldv in items:
+            _chk(x, y, out, sc, s)
+            if op == 0:
+                self.vec_norm(x, sc)
+            elif op == 1:
+                self.krylov_alpha(x, y, sc, j)
+            elif op == 2:
+                self.krylov_orth(out, x, y, sc, j)
+            elif op == 3:
+                self.scale_inv(x, s, out)
+            elif op == 4:
+                self.lincomb(x, j, s, out)
+            else:
+                self.allclose(x, y, rtol, atol, sc)
+
     def axpy(self, y, x, c, sign=1.0):
         cc = complex(c[0].item(), c[1].item() if y.is_complex() else 0.0) * sign
         y += (cc if y.is_complex() else cc.real) * x

@@ -175,3 +175,94 @@ def test_evolve_batch_per_instance_precision_host_logic(cpu_engine, monkeypatch,
     by_b = [p for d, p in seen if 3 in d]
     assert by_a and by_b
     assert set(by_a) == {"bf16x3"} and set(by_b) == {"fp64"}
+
+
+@pytest.mark.gpu
+def test_grouped_vector_ops_match_single():
+    """reno_vec_grouped gives every item bitwise the result of the single
+    vector call: ragged lengths across the block partition (1 .. 3 x 1184
+    blocks), real and complex, every operation."""
+    from renormalizer_b200._native import (Engine, VOP_ALLCLOSE, VOP_ALPHA, VOP_LINCOMB, VOP_NORM, VOP_ORTH,
+                                           VOP_SCALE_INV, dtype_code)
+    eng = Engine.get(0)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    sizes = (1, 7, 256, 1025, 300_001, 3_700_000)
+    vecs = []
+    for i, n in enumerate(sizes):
+        dt = torch.complex128 if i % 2 else torch.float64
+        mk = (lambda: torch.randn(n, dtype=torch.float64, device="cuda", generator=g)) if dt == torch.float64 else \
+            (lambda: torch.complex(torch.randn(n, dtype=torch.float64, device="cuda", generator=g),
+                                   torch.randn(n, dtype=torch.float64, device="cuda", generator=g)))
+        V = torch.stack([mk() for _ in range(4)])
+        vecs.append((n, dt, V, mk()))
+    j = 2
+    single_ab, group_ab = [], []
+    single_w, group_w = [], []
+    for n, dt, V, w in vecs:
+        ab_s = torch.zeros(8, dtype=torch.float64, device="cuda")
+        ab_s[2 * j - 1] = 0.37
+        ab_g = ab_s.clone()
+        ws, wg = w.clone(), w.clone()
+        eng.krylov_alpha(ws, V[j], ab_s, j)
+        eng.krylov_orth(ws, V[j], V[j - 1], ab_s, j)
+        single_ab.append(ab_s), group_ab.append(ab_g), single_w.append(ws), group_w.append(wg)
+    items = lambda rows: [(n, dtype_code(V), jj, x, y, out, sc, s, n) for (n, dt, V, w), (jj, x, y, out, sc, s)
+                          in zip(vecs, rows)]
+    eng.vec_grouped(VOP_ALPHA, items([(j, wg, V[j], None, ab, None)
+                                      for (n, dt, V, w), wg, ab in zip(vecs, group_w, group_ab)]))
+    eng.vec_grouped(VOP_ORTH, items([(j, V[j], V[j - 1], wg, ab, None)
+                                     for (n, dt, V, w), wg, ab in zip(vecs, group_w, group_ab)]))
+    for a, b in zip(single_ab, group_ab):
+        assert torch.equal(a, b)
+    for a, b in zip(single_w, group_w):
+        assert torch.equal(a, b)
+    # norm, scale_inv, lincomb, allclose
+    s_norm = [torch.zeros(4, dtype=torch.float64, device="cuda") for _ in vecs]
+    g_norm = [torch.zeros(4, dtype=torch.float64, device="cuda") for _ in vecs]
+    for (n, dt, V, w), o in zip(vecs, s_norm):
+        eng.vec_norm(V[1], o)
+    eng.vec_grouped(VOP_NORM, items([(0, V[1], None, None, o, None) for (n, dt, V, w), o in zip(vecs, g_norm)]))
+    assert all(torch.equal(a, b) for a, b in zip(s_norm, g_norm))
+    s_sc = [torch.empty_like(w) for _, _, _, w in vecs]
+    g_sc = [torch.empty_like(w) for _, _, _, w in vecs]
+    for (n, dt, V, w), o, nr in zip(vecs, s_sc, s_norm):
+        eng.scale_inv(V[1], nr, o)
+    eng.vec_grouped(VOP_SCALE_INV, items([(0, V[1], None, o, None, nr)
+                                          for (n, dt, V, w), o, nr in zip(vecs, g_sc, g_norm)]))
+    assert all(torch.equal(a, b) for a, b in zip(s_sc, g_sc))
+    coef = torch.randn(8, dtype=torch.float64, device="cuda", generator=g)
+    s_lc = [torch.empty_like(w) for _, _, _, w in vecs]
+    g_lc = [torch.empty_like(w) for _, _, _, w in vecs]
+    for (n, dt, V, w), o in zip(vecs, s_lc):
+        eng.lincomb(V, 3, coef, o)
+    eng.vec_grouped(VOP_LINCOMB, items([(3, V, None, o, None, coef) for (n, dt, V, w), o in zip(vecs, g_lc)]))
+    assert all(torch.equal(a, b) for a, b in zip(s_lc, g_lc))
+    s_fl = [torch.full((4,), -1.0, dtype=torch.float64, device="cuda") for _ in vecs]
+    g_fl = [torch.full((4,), -1.0, dtype=torch.float64, device="cuda") for _ in vecs]
+    pert = [w * (1 + 1e-7 * (i % 2)) for i, (_, _, _, w) in enumerate(vecs)]
+    for (n, dt, V, w), p, o in zip(vecs, pert, s_fl):
+        eng.allclose(w, p, 1e-9, 0.0, o)
+    eng.vec_grouped(VOP_ALLCLOSE, items([(0, w, p, None, o, None) for (n, dt, V, w), p, o in zip(vecs, pert, g_fl)]),
+                    1e-9, 0.0)
+    assert all(torch.equal(a, b) for a, b in zip(s_fl, g_fl))
+    assert [float(f[0]) for f in g_fl] == [1.0, 0.0] * 3
+
+
+@pytest.mark.gpu
+def test_expm_krylov_batch_matches_single_gpu():
+    """the grouped lockstep Lanczos exponential equals each problem's own
+    expm_krylov bit for bit on the GPU (sizes from 3 to 4000, real and
+    imaginary steps, early and late convergence)"""
+    from renormalizer_b200.krylov import expm_krylov, expm_krylov_batch
+    rng = np.random.default_rng(3)
+    mats, vecs, dts = [], [], []
+    for n, dt in ((3, -1j), (6, -0.3j), (40, -0.05j), (25, 0.2), (700, -0.02j), (4000, -0.01j)):
+        h = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        mats.append(torch.as_tensor((h + h.conj().T) / np.sqrt(n), device="cuda"))
+        vecs.append(torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n), device="cuda"))
+        dts.append(dt)
+    single = [expm_krylov(lambda x, m=m: m @ x, dt, v) for m, dt, v in zip(mats, dts, vecs)]
+    batch = expm_krylov_batch(lambda idx, xs: [mats[i] @ x for i, x in zip(idx, xs)], dts, vecs)
+    for (vs, js), (vb, jb) in zip(single, batch):
+        assert js == jb
+        assert torch.equal(vs, vb)
