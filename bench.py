@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--envelope", action="store_true",
                     help="--accuracy mode: also evolve FP64 from the start state perturbed by one ulp per entry "
                          "and report its distance from the unperturbed FP64 run (the FP64 engine's own envelope)")
+    ap.add_argument("--inject", default="",
+                    help="--accuracy mode: comma-separated relative sizes delta; each adds an FP64 arm whose site "
+                         "tensors get a seeded random relative perturbation of size delta after every step")
     ap.add_argument("--out", default="", help="append the per-step JSON lines of --accuracy mode to this file")
     ap.add_argument("--krylov-tol", default="",
                     help="rtol,atol of the Lanczos convergence test for every arm (default: the reference's "
@@ -731,6 +734,21 @@ def perturb_ulp(mps, seed=11):
     return new
 
 
+def perturb_rel(mps, delta, seed):
+    """A copy of mps with every site-tensor entry x replaced by x (1 + delta r),
+    r uniform in (-1, 1) per entry and per real/imaginary part: a step's worth
+    of relative error delta injected into an FP64 trajectory."""
+    import torch
+    new = mps.copy()
+    g = torch.Generator(device=new[0].device).manual_seed(seed)
+    for i, t in enumerate(new._mp):
+        r = torch.view_as_real(t) if t.is_complex() else t
+        u = torch.rand(r.shape, dtype=torch.float64, device=r.device, generator=g) * 2 - 1
+        r2 = (r * (1 + delta * u)).contiguous()
+        new._mp[i] = torch.view_as_complex(r2) if t.is_complex() else r2
+    return new
+
+
 def run_accuracy(args):
     """max |population(prec) - population(FP64)| after every step, for each
     precision in --accuracy-precs, from the same start state; with
@@ -749,6 +767,9 @@ def run_accuracy(args):
     arms = {p: mps0 for p in precs}
     if args.envelope:
         arms["fp64_ulp"] = perturb_ulp(mps0)
+    inject = {f"fp64_inject_{d}": float(d) for d in args.inject.split(",") if d}
+    for k in inject:
+        arms[k] = mps0
     ref = mps0
     out = open(args.out, "a") if args.out else None
     worst = {k: 0.0 for k in arms}
@@ -772,9 +793,11 @@ def run_accuracy(args):
             # their truncations share the batched eigensolver launches
             t1 = time.time()
             res = evolve_batch([ref] + [arms[k] for k in names], mpo, args.dt,
-                               precs=["fp64"] + ["fp64" if k == "fp64_ulp" else k for k in names])
+                               precs=["fp64"] + ["fp64" if k.startswith("fp64_") else k for k in names])
             ref = res[0]
             arms = dict(zip(names, res[1:]))
+            for k, d in inject.items():
+                arms[k] = perturb_rel(arms[k], d, seed=1000 * (step + 1) + names.index(k))
             step_s["lockstep"] = step_s.get("lockstep", 0.0) + time.time() - t1
             pref = ref.e_occupations
             kref = (ref.evolve_config.stat or {}).get("counts", [])
@@ -793,9 +816,11 @@ def run_accuracy(args):
         pref = ref.e_occupations
         step_s["fp64"] += time.time() - t1
         for k in arms:
-            backend.prec = "fp64" if k == "fp64_ulp" else k
+            backend.prec = "fp64" if k.startswith("fp64_") else k
             t1 = time.time()
             arms[k] = arms[k].evolve(mpo, args.dt)
+            if k in inject:
+                arms[k] = perturb_rel(arms[k], inject[k], seed=1000 * (step + 1) + names.index(k))
             d = float(np.abs(arms[k].e_occupations - pref).max())
             step_s[k] += time.time() - t1
             worst[k] = max(worst[k], d)

@@ -75,9 +75,25 @@ class QNBlock:
     vpad: int = 0
 
 
+def _i64_many(arrays, device):
+    """several int64 index lists (and float64 lists, carried as their bits)
+    in one host-to-device transfer; returns one device view per list"""
+    host = [np.asarray(a, dtype=np.int64) if np.asarray(a).dtype != np.float64 else np.asarray(a).view(np.int64)
+            for a in arrays]
+    flat = np.concatenate(host) if host else np.zeros(0, np.int64)
+    dev = h2d(flat, device, np.int64) if device.type == "cuda" else torch.as_tensor(flat, device=device)
+    out, off = [], 0
+    for a, h in zip(arrays, host):
+        v = dev[off: off + h.size]
+        out.append(v.view(torch.float64) if np.asarray(a).dtype == np.float64 else v)
+        off += h.size
+    return out
+
+
 def _gather(eng: Engine, mat: torch.Tensor, lset, rset) -> torch.Tensor:
     out = torch.empty((len(lset), len(rset)), dtype=mat.dtype, device=mat.device)
-    eng.qn_gather(mat, _i64(lset, mat.device), _i64(rset, mat.device), out)
+    rows, cols = _i64_many([lset, rset], mat.device)
+    eng.qn_gather(mat, rows, cols, out)
     return out
 
 
@@ -181,10 +197,12 @@ def _scatter(eng: Engine, src: torch.Tensor, rows, scols, dcols, sigma, dst: tor
         raise IndexError(f"qn scatter out of range: src {tuple(src.shape)}, {len(r)} rows (max {r.max()}), "
                          f"source columns up to {c.max()}, dst {tuple(dst.shape)}")
     dev = dst.device
-    sig = None
-    if sigma is not None:
-        sig = h2d(sigma, dev, np.float64) if dev.type == "cuda" else torch.as_tensor(np.asarray(sigma, np.float64))
-    eng.qn_scatter(src, _i64(rows, dev), _i64(scols, dev), _i64(dcols, dev), sig, dst, dst_rs, dst_cs)
+    if sigma is None:
+        ri, ci, di = _i64_many([r, c, dc], dev)
+        sig = None
+    else:
+        ri, ci, di, sig = _i64_many([r, c, dc, np.asarray(sigma, dtype=np.float64)], dev)
+    eng.qn_scatter(src, ri, ci, di, sig, dst, dst_rs, dst_cs)
 
 
 def _select_by_code(sset: np.ndarray, codes: np.ndarray, visit: List[int], Mmax: int, percent=0) -> List[int]:
