@@ -38,7 +38,7 @@ from .krylov import expm_krylov
 from .lib import Environ, contract_one_site
 from .model import Model, Op
 from .mpo import Mpo
-from .svd_qn import (qn_sectors, add_outer, get_qn_mask, qr_split, select_basis_indices, svd_truncate,
+from .svd_qn import (qn_sectors, add_outer, get_qn_mask, qr_split, qr_split_batch, select_basis_indices, svd_truncate,
                      svd_truncate_batch)
 from .svd_qn import refine as svd_refine
 
@@ -56,6 +56,14 @@ def _krylov_stats(steps):
 class TruncRequest:
     """A truncation a sweep generator yields (svd_truncate's keyword
     arguments); it receives the TruncatedSplit back."""
+
+    def __init__(self, kwargs: dict):
+        self.kwargs = kwargs
+
+
+class QrRequest:
+    """A canonicalising QR / RQ a sweep generator yields (qr_split's keyword
+    arguments); it receives qr_split's result back."""
 
     def __init__(self, kwargs: dict):
         self.kwargs = kwargs
@@ -422,10 +430,16 @@ class Mps:
 
     def _push_cano(self, idx):
         """mp.py:890-908 with _update_ms (245-295, sigma=None)"""
-        mt = self._mp[idx]
+        self._push_cano_place(idx, qr_split(**self._push_cano_call(idx)))
+
+    def _push_cano_call(self, idx) -> dict:
         qnbigl, qnbigr, _ = self._get_big_qn([idx], with_mat=False)
-        system = "L" if self.to_right else "R"
-        u, qnlset, vt, qnrset = qr_split(mt, qnbigl, qnbigr, self.qntot, system)
+        return dict(coef=self._mp[idx], qnbigl=qnbigl, qnbigr=qnbigr, qntot=self.qntot,
+                    system="L" if self.to_right else "R")
+
+    def _push_cano_place(self, idx, res):
+        mt = self._mp[idx]
+        u, qnlset, vt, qnrset = res
         m_trunc = u.shape[1]
         pd = list(mt.shape[1:-1])
         if self.to_right:
@@ -921,6 +935,8 @@ class Mps:
             while True:
                 if isinstance(req, TruncRequest):
                     req = steps.send(svd_truncate(**req.kwargs))
+                elif isinstance(req, QrRequest):
+                    req = steps.send(qr_split(**req.kwargs))
                 else:
                     req = steps.send(self._krylov(*req))
         except StopIteration as stop:
@@ -954,7 +970,8 @@ class Mps:
                 local_steps.append(j)
                 mps_t = mps_t.reshape(shape)
                 qnbigl, qnbigr, _ = mps._get_big_qn([imps], with_mat=False)
-                u, qnlset, vt, qnrset = qr_split(mps_t, qnbigl, qnbigr, mps.qntot, system)
+                u, qnlset, vt, qnrset = yield QrRequest(dict(coef=mps_t, qnbigl=qnbigl, qnbigr=qnbigr,
+                                                             qntot=mps.qntot, system=system))
                 if not mps.to_right and imps != 0:
                     mps[imps] = vt.reshape([-1] + shape[1:])
                     mps.qn[imps] = np.array(qnrset).reshape(vt.shape[0], -1)
@@ -1021,7 +1038,8 @@ class Mps:
                 mps_t, j = yield (hop1, 1j * evolve_dt / 2, ms1)
                 local_steps.append(j)
                 mps[cidx2] = mps_t.reshape(ms1.shape)
-                mps._push_cano(cidx2)
+                res = yield QrRequest(mps._push_cano_call(cidx2))
+                mps._push_cano_place(cidx2, res)
             mps._switch_direction()
         mps.evolve_config.stat = _krylov_stats(local_steps)
         return mps
@@ -1093,8 +1111,14 @@ def evolve_batch(mps_list: List[Mps], mpo_list, evolve_dt, normalize=True, precs
                 res = svd_truncate_batch([pending[i].kwargs for i in tidx])
                 for i, r in zip(tidx, res):
                     resume(i, r, nxt)
+            # canonicalising QRs of this round: their QN blocks in shared launches
+            qidx = sorted(i for i in pending if isinstance(pending[i], QrRequest))
+            if qidx:
+                res = qr_split_batch([pending[i].kwargs for i in qidx])
+                for i, r in zip(qidx, res):
+                    resume(i, r, nxt)
             # local exponentials of this round in lockstep, grouped matvecs
-            idx = sorted(i for i in pending if not isinstance(pending[i], TruncRequest))
+            idx = sorted(i for i in pending if not isinstance(pending[i], (TruncRequest, QrRequest)))
             if idx:
                 reqs = [pending[i] for i in idx]
                 ops = [r[0] for r in reqs]

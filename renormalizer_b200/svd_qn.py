@@ -142,15 +142,10 @@ def qn_block_svd(coef: torch.Tensor, qnbigl, qnbigr, qntot, full_matrices=True, 
     return blocks, rows, cols
 
 
-def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
-    """Per-block QR (system "L") or RQ (system "R"), economic (svd_qn.py:195-204),
-    every QN block of the site in one batched Householder QR (reno_qr_blocks,
-    LAPACK's sign conventions).  RQ comes from the QR of the reversed
-    conjugate transpose: (J A J)^H = Q1 R1 gives A = (J R1^H J)(J Q1^H J), with
-    J R1^H J upper triangular.  Householder QR processes the entries in the
-    same order as LAPACK's RQ (last row first, pivot on its last entry), so R
-    and Q agree with scipy.linalg.rq including the signs, not only up to a
-    rotation."""
+def _qr_begin(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
+    """The QN blocks of one QR / RQ (qn_block_qr) gathered and, for RQ,
+    reversed and conjugate-transposed: (found, rows, cols), found holding
+    (nl, nr, lset, rset, block to factorise) per block."""
     if system not in ("L", "R"):
         raise AssertionError("system must be L or R for QR")
     eng = Engine.get(coef.device)
@@ -174,7 +169,10 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
         found.append((nl, nr, lset, rset, blk))
     if not found:
         raise ValueError("Invalid quantum number")
-    Qs, Rs = eng.qr_blocks([f[4] for f in found])
+    return found, rows, cols
+
+
+def _qr_end(found, Qs, Rs, system: str):
     blocks = []
     for (nl, nr, lset, rset, _), Q, R in zip(found, Qs, Rs):
         if system == "L":
@@ -182,7 +180,21 @@ def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
         else:
             blocks.append(QNBlock(nl, nr, lset, rset, R.mH.flip([0, 1]).resolve_conj().contiguous(), None, None,
                                   Q.mH.flip([0, 1]).resolve_conj().contiguous()))
-    return blocks, rows, cols
+    return blocks
+
+
+def qn_block_qr(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
+    """Per-block QR (system "L") or RQ (system "R"), economic (svd_qn.py:195-204),
+    every QN block of the site in one batched Householder QR (reno_qr_blocks,
+    LAPACK's sign conventions).  RQ comes from the QR of the reversed
+    conjugate transpose: (J A J)^H = Q1 R1 gives A = (J R1^H J)(J Q1^H J), with
+    J R1^H J upper triangular.  Householder QR processes the entries in the
+    same order as LAPACK's RQ (last row first, pivot on its last entry), so R
+    and Q agree with scipy.linalg.rq including the signs, not only up to a
+    rotation."""
+    found, rows, cols = _qr_begin(coef, qnbigl, qnbigr, qntot, system)
+    Qs, Rs = Engine.get(coef.device).qr_blocks([f[4] for f in found])
+    return _qr_end(found, Qs, Rs, system), rows, cols
 
 
 def _scatter(eng: Engine, src: torch.Tensor, rows, scols, dcols, sigma, dst: torch.Tensor, dst_rs, dst_cs):
@@ -889,6 +901,28 @@ def qr_split(coef: torch.Tensor, qnbigl, qnbigr, qntot, system: str):
     """svd_qn(QR=True, full_matrices=False) of mp.py:890-908 / mps.py:1318-1327:
     returns (u (rows, k), qnl list, vt (k, cols), qnr list) as device tensors."""
     blocks, rows, cols = qn_block_qr(coef, qnbigl, qnbigr, qntot, system)
+    return _qr_assemble(blocks, rows, cols, coef)
+
+
+def qr_split_batch(calls):
+    """qr_split for several independent calls (keyword dicts of qr_split), the
+    QN blocks of all of them in shared batched QR launches (lockstep
+    realisations); every result is that call's own qr_split."""
+    begun = [_qr_begin(**c) for c in calls]
+    mats = [f[4] for found, _, _ in begun for f in found]
+    if not mats:
+        return []
+    Qs, Rs = Engine.get(mats[0].device).qr_blocks(mats)
+    out, off = [], 0
+    for c, (found, rows, cols) in zip(calls, begun):
+        k = len(found)
+        blocks = _qr_end(found, Qs[off:off + k], Rs[off:off + k], c["system"])
+        off += k
+        out.append(_qr_assemble(blocks, rows, cols, c["coef"]))
+    return out
+
+
+def _qr_assemble(blocks, rows, cols, coef):
     eng = Engine.get(coef.device)
     ks = [min(len(b.lset), len(b.rset)) for b in blocks]
     ktot = sum(ks)
