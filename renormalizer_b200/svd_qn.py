@@ -639,11 +639,18 @@ def svd_truncate_batch(calls) -> List["TruncatedSplit"]:
     parts = [_trunc_host_tensors(st) for st in states]
     lens = [sum(t.numel() for t in p) for p in parts]
     host = torch.cat([t for p in parts for t in p]).cpu().numpy()
-    out, off = [], 0
+    sels, off = [], 0
     for st, n in zip(states, lens):
-        out.append(_trunc_end(st, host[off:off + n]))
+        sels.append(_trunc_select(st, host[off:off + n]))
         off += n
-    return out
+    # the small-sigma refinements of every call that asks for one: one pass
+    need = [i for i, sel in enumerate(sels) if sel["refine"]]
+    if need:
+        hit = _refine_groups(states[0]["eng"], [(states[i]["blocks"], states[i]["keep_left"]) for i in need])
+        for i, h in zip(need, hit):
+            if h:
+                sels[i]["sig"], sels[i]["sidx"] = sels[i]["select"]()
+    return [_trunc_place(st, sel) for st, sel in zip(states, sels)]
 
 
 def _trunc_begin(coef, qnbigl, qnbigr, qntot, keep_left, m_trunc_fn, percent=0, full_matrices=True, kcap=None,
@@ -723,29 +730,53 @@ def _refine_clusters(eng: Engine, blocks, keep_left: bool) -> bool:
     ``Sh`` already known): all cluster Gram matrices in one device
     eigensolver call, their checks and refined sigma in one host transfer.
     Returns whether any block was refined."""
+    return _refine_groups(eng, [(blocks, keep_left)])[0]
+
+
+def _refine_groups(eng: Engine, groups) -> List[bool]:
+    """_refine_clusters for several truncations at once (groups of (blocks,
+    keep_left)): the cluster Gram matrices of all of them in one device
+    eigensolver call and one host transfer.  Returns per group whether any of
+    its blocks was refined."""
     todo = []
-    for b in blocks:
-        kt = b["K"].shape[1]
-        head = np.asarray(b["Sh"][:kt], dtype=np.float64)
-        if kt < 2 or not np.all(np.isfinite(head)) or head.max() <= 0:
-            continue
-        cl = np.nonzero(head < refine.tau * head.max())[0]
-        if len(cl) == 0:
-            continue
-        lg = np.nonzero(head >= refine.tau * head.max())[0]
-        dev = b["S"].device
-        ic, il = _i64(cl, dev), _i64(lg, dev)
-        Z = b["P"] if keep_left else b["P"].transpose(0, 1).conj()
-        Zc, Zl = Z.index_select(0, ic), Z.index_select(0, il)
-        sl2 = b["S"].index_select(0, il) ** 2
-        for _ in range(2):
-            coef = eng.matmul(Zc, Zl.transpose(0, 1), conj_b=True) / sl2[None, :]
-            Zc = Zc - eng.matmul(coef, Zl)
-        C = eng.matmul(Zc, Zc.transpose(0, 1), conj_b=True)
-        scale = torch.clamp(torch.diagonal(C).real.sum(), min=1e-300)
-        todo.append(dict(b=b, cl=cl, ic=ic, C=(C / scale).contiguous(), scale=scale))
+    for g, (blocks, keep_left) in enumerate(groups):
+        for b in blocks:
+            t = _refine_prepare(eng, b, keep_left)
+            if t is not None:
+                t["g"] = g
+                todo.append(t)
     if not todo:
-        return False
+        return [False] * len(groups)
+    _refine_apply(eng, todo)
+    hit = set(t["g"] for t in todo)
+    return [g in hit for g in range(len(groups))]
+
+
+def _refine_prepare(eng: Engine, b, keep_left: bool):
+    """the projected cluster Gram matrix of block b, or None when b has no
+    cluster below the refinement threshold"""
+    kt = b["K"].shape[1]
+    head = np.asarray(b["Sh"][:kt], dtype=np.float64)
+    if kt < 2 or not np.all(np.isfinite(head)) or head.max() <= 0:
+        return None
+    cl = np.nonzero(head < refine.tau * head.max())[0]
+    if len(cl) == 0:
+        return None
+    lg = np.nonzero(head >= refine.tau * head.max())[0]
+    dev = b["S"].device
+    ic, il = _i64(cl, dev), _i64(lg, dev)
+    Z = b["P"] if keep_left else b["P"].transpose(0, 1).conj()
+    Zc, Zl = Z.index_select(0, ic), Z.index_select(0, il)
+    sl2 = b["S"].index_select(0, il) ** 2
+    for _ in range(2):
+        coef = eng.matmul(Zc, Zl.transpose(0, 1), conj_b=True) / sl2[None, :]
+        Zc = Zc - eng.matmul(coef, Zl)
+    C = eng.matmul(Zc, Zc.transpose(0, 1), conj_b=True)
+    scale = torch.clamp(torch.diagonal(C).real.sum(), min=1e-300)
+    return dict(b=b, cl=cl, ic=ic, C=(C / scale).contiguous(), scale=scale, keep_left=keep_left)
+
+
+def _refine_apply(eng: Engine, todo):
     refine.calls += 1
     refine.blocks += len(todo)
     dev_idx = [i for i, t in enumerate(todo) if _device_eig_ok(t["C"])]
@@ -771,7 +802,7 @@ def _refine_clusters(eng: Engine, blocks, keep_left: bool) -> bool:
             off += 3
     off = 0
     for t in todo:
-        b, ic, R = t["b"], t["ic"], t["R"]
+        b, ic, R, keep_left = t["b"], t["ic"], t["R"], t["keep_left"]
         c = len(t["cl"])
         sig_h = t.get("sig_h", host[off:off + c])
         off += c
@@ -788,13 +819,13 @@ def _refine_clusters(eng: Engine, blocks, keep_left: bool) -> bool:
             # unprojected tail values stay below every projected one
             Sh[kt:] = np.minimum(Sh[kt:], Sh[:kt].min())
         b["Sh"] = Sh
-    return True
 
 
-def _trunc_end(st, host):
-    """Checks (redo of failed blocks), the reference's selection and the
-    scatter of the kept columns, from the host copy of _trunc_host_tensors."""
-    eng, coef, rows, cols = st["eng"], st["coef"], st["rows"], st["cols"]
+def _trunc_select(st, host):
+    """Checks (redo of failed blocks) and the reference's selection, from the
+    host copy of _trunc_host_tensors; says whether the cut asks for the
+    small-sigma refinement."""
+    eng = st["eng"]
     keep_left, m_trunc_fn, percent, blocks = st["keep_left"], st["m_trunc_fn"], st["percent"], st["blocks"]
     sub = [b for b in blocks if "res" in b]
     dev_eig = [b for b in blocks if "chk" in b]
@@ -861,10 +892,26 @@ def _trunc_end(st, host):
 
     sig, sidx = select()
     keeps_all = len(sidx) >= sum(b["dim"] for b in blocks)
-    if refine.tau > 0 and len(sidx) and sig.max() > 0 and sig[sidx].min() < 2 * refine.tau * sig.max() and \
-            (keeps_all or sig[sidx].min() >= st["refine_floor"] * sig.max()):
-        if _refine_clusters(eng, blocks, keep_left):
-            sig, sidx = select()
+    wants = bool(refine.tau > 0 and len(sidx) and sig.max() > 0 and sig[sidx].min() < 2 * refine.tau * sig.max()
+                 and (keeps_all or sig[sidx].min() >= st["refine_floor"] * sig.max()))
+    return dict(select=select, sig=sig, sidx=sidx, refine=wants, blk=blk, pos=pos, qkey=qkey)
+
+
+def _trunc_end(st, host):
+    """_trunc_select, the small-sigma refinement where the cut asks for it
+    and the scatter of the kept columns (_trunc_place)."""
+    sel = _trunc_select(st, host)
+    if sel["refine"] and _refine_clusters(st["eng"], st["blocks"], st["keep_left"]):
+        sel["sig"], sel["sidx"] = sel["select"]()
+    return _trunc_place(st, sel)
+
+
+def _trunc_place(st, sel):
+    """The kept columns of the selection scattered into the new left / right
+    tensors (completion columns drawn where selected)."""
+    eng, coef, rows, cols = st["eng"], st["coef"], st["rows"], st["cols"]
+    keep_left, blocks = st["keep_left"], st["blocks"]
+    sig, sidx, blk, pos, qkey = sel["sig"], sel["sidx"], sel["blk"], sel["pos"], sel["qkey"]
     mdim = len(sidx)
     left = torch.zeros((rows, mdim), dtype=coef.dtype, device=coef.device)
     right = torch.zeros((mdim, cols), dtype=coef.dtype, device=coef.device)
