@@ -75,18 +75,21 @@ class QNBlock:
     vpad: int = 0
 
 
-def _i64_many(arrays, device):
-    """several int64 index lists (and float64 lists, carried as their bits)
-    in one host-to-device transfer; returns one device view per list"""
-    host = [np.asarray(a, dtype=np.int64) if np.asarray(a).dtype != np.float64 else np.asarray(a).view(np.int64)
-            for a in arrays]
+def _i64_many(arrays, device, float_last=False):
+    """several int64 index lists (the last one float64, carried as its bits,
+    when ``float_last``) in one host-to-device transfer; returns one device
+    view per list"""
+    host = [np.asarray(a, dtype=np.int64) for a in (arrays[:-1] if float_last else arrays)]
+    if float_last:
+        host.append(np.ascontiguousarray(arrays[-1], dtype=np.float64).view(np.int64))
     flat = np.concatenate(host) if host else np.zeros(0, np.int64)
     dev = h2d(flat, device, np.int64) if device.type == "cuda" else torch.as_tensor(flat, device=device)
     out, off = [], 0
-    for a, h in zip(arrays, host):
-        v = dev[off: off + h.size]
-        out.append(v.view(torch.float64) if np.asarray(a).dtype == np.float64 else v)
+    for h in host:
+        out.append(dev[off: off + h.size])
         off += h.size
+    if float_last:
+        out[-1] = out[-1].view(torch.float64)
     return out
 
 
@@ -213,7 +216,7 @@ def _scatter(eng: Engine, src: torch.Tensor, rows, scols, dcols, sigma, dst: tor
         ri, ci, di = _i64_many([r, c, dc], dev)
         sig = None
     else:
-        ri, ci, di, sig = _i64_many([r, c, dc, np.asarray(sigma, dtype=np.float64)], dev)
+        ri, ci, di, sig = _i64_many([r, c, dc, sigma], dev, float_last=True)
     eng.qn_scatter(src, ri, ci, di, sig, dst, dst_rs, dst_cs)
 
 
