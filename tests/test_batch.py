@@ -283,3 +283,22 @@ def test_expm_krylov_batch_matches_single_gpu():
     for (vs, js), (vb, jb) in zip(single, batch):
         assert js == jb
         assert torch.equal(vs, vb)
+
+
+def test_qr_split_batch_matches_single(cpu_engine):
+    """the batched canonicalising QR (the QN blocks of several calls in shared
+    reno_qr_blocks launches) returns every call's own qr_split result, for
+    QR and RQ, real and complex, several QN sectors"""
+    from renormalizer_b200.svd_qn import qr_split, qr_split_batch
+    rng = np.random.default_rng(4)
+    calls = []
+    for rows, cols, cplx, system in ((12, 9, True, "L"), (7, 20, False, "R"), (16, 16, True, "R"), (5, 3, False, "L")):
+        a = rng.standard_normal((rows, cols)) + (1j * rng.standard_normal((rows, cols)) if cplx else 0)
+        ql = rng.integers(0, 3, rows).reshape(rows, 1)
+        qr = (2 - rng.integers(0, 3, cols)).reshape(cols, 1)
+        calls.append(dict(coef=torch.as_tensor(a), qnbigl=ql, qnbigr=qr, qntot=np.array([2]), system=system))
+    single = [qr_split(**c) for c in calls]
+    batch = qr_split_batch(calls)
+    for (u1, l1, v1, r1), (u2, l2, v2, r2) in zip(single, batch):
+        assert torch.equal(u1, u2) and torch.equal(v1, v2)
+        assert l1 == l2 and r1 == r2
