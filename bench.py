@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--envelope", action="store_true",
                     help="--accuracy mode: also evolve FP64 from the start state perturbed by one ulp per entry "
                          "and report its distance from the unperturbed FP64 run (the FP64 engine's own envelope)")
+    ap.add_argument("--accumulation", action="store_true",
+                    help="the split GEMM's FP32 accumulation error on exactly representable operands, K = 64 .. 16384")
     ap.add_argument("--inject", default="",
                     help="--accuracy mode: comma-separated relative sizes delta; each adds an FP64 arm whose site "
                          "tensors get a seeded random relative perturbation of size delta after every step")
@@ -749,6 +751,41 @@ def perturb_rel(mps, delta, seed):
     return new
 
 
+def run_accumulation(args):
+    """Accumulation error of the split GEMM alone: operands exactly
+    representable in the split's piece format (BF16 / TF32), so every
+    product is exact and only the tensor cores' FP32 accumulation rounds.
+    One JSON line per (sign, precision, K): normwise relative error against
+    FP64, the mean signed error over mean |C| (bias) and the fraction of
+    positive errors, for random-sign and all-positive operands."""
+    import torch
+    from renormalizer_b200._native import Engine
+    torch.cuda.set_device(0)
+    eng = Engine.get(0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+
+    def exact(x, prec):
+        if prec == "bf16x3":
+            return x.to(torch.bfloat16).to(torch.float64)
+        f = x.to(torch.float32)                     # TF32: 10 explicit mantissa bits
+        return (f.view(torch.int32) & ~((1 << 13) - 1)).view(torch.float32).to(torch.float64)
+
+    for sign in ("random", "positive"):
+        for prec in ("bf16x3", "tf32x3"):
+            for K in (64, 256, 1024, 4096, 16384):
+                A = torch.randn(256, K, dtype=torch.float64, device="cuda", generator=g)
+                B = torch.randn(K, 256, dtype=torch.float64, device="cuda", generator=g)
+                if sign == "positive":
+                    A, B = A.abs(), B.abs()
+                A, B = exact(A, prec).contiguous(), exact(B, prec).contiguous()
+                C = eng.matmul(A, B, prec=prec)
+                ref = eng.matmul(A, B, prec="fp64")
+                err = C - ref
+                print(json.dumps({"sign": sign, "prec": prec, "K": K, "rel": float(err.norm() / ref.norm()),
+                                  "bias": float(err.mean() / ref.abs().mean()),
+                                  "frac_positive_errors": float((err > 0).double().mean())}), flush=True)
+
+
 def run_accuracy(args):
     """max |population(prec) - population(FP64)| after every step, for each
     precision in --accuracy-precs, from the same start state; with
@@ -1089,6 +1126,9 @@ def main():
     if args.krylov_tol:
         tol = importlib.import_module("renormalizer_b200.krylov").tolerance
         tol.rtol, tol.atol = (float(x) for x in args.krylov_tol.split(","))
+    if args.accumulation:
+        run_accumulation(args)
+        return
     if args.accuracy:
         run_accuracy(args)
         return
