@@ -780,7 +780,7 @@ def _refine_prepare(eng: Engine, b, keep_left: bool):
 
 
 def _refine_apply(eng: Engine, todo):
-    refine.calls += 1
+    refine.calls += len(set(t.get("g", 0) for t in todo))  # truncations refined
     refine.blocks += len(todo)
     dev_idx = [i for i, t in enumerate(todo) if _device_eig_ok(t["C"])]
     if dev_idx:
