@@ -113,7 +113,22 @@ def test_expm_krylov_batch_matches_single(cpu_engine):
         mats.append(torch.as_tensor(h + h.conj().T))
         vecs.append(torch.as_tensor(rng.standard_normal(n) + 1j * rng.standard_normal(n)))
         dts.append(dt)
-    single = [expm_krylov(lambda x, m=m: m @ x, dt, v) for m, dt, v in zip(mats, dts, vecs)]
+    # a start vector inside a 3-dimensional invariant subspace: the Lanczos
+    # iteration breaks down (beta_2 ~ 0) and stops at the next check point
+    d = np.arange(1.0, 31.0)
+    mats.append(torch.as_tensor(np.diag(d).astype(complex)))
+    v = np.zeros(30, dtype=complex)
+    v[[3, 11, 20]] = (1.0, 0.5j, -0.25)
+    vecs.append(torch.as_tensor(v))
+    dts.append(-0.1j)
+    issued = [0] * len(mats)
+
+    def counted(i, x):
+        issued[i] += 1
+        return mats[i] @ x
+
+    single = [expm_krylov(lambda x, i=i: counted(i, x), dt, v) for i, (dt, v) in enumerate(zip(dts, vecs))]
+    assert single[-1][1] == 3
     seen = []
 
     def group_apply(idx, xs):
@@ -124,9 +139,10 @@ def test_expm_krylov_batch_matches_single(cpu_engine):
     for (vs, js), (vb, jb) in zip(single, batch):
         assert js == jb
         assert torch.equal(vs, vb)
-    assert seen[0] == [0, 1, 2, 3]
+    assert seen[0] == [0, 1, 2, 3, 4]
     assert all(len(a) >= len(b) for a, b in zip(seen, seen[1:]))
-    assert sum(len(s) for s in seen) == sum(j for _, j in single)
+    # every problem gets exactly the matvecs its own expm_krylov asks for
+    assert [sum(i in s for s in seen) for i in range(len(mats))] == issued
 
 
 def test_apply_grouped_dispatch_host_logic(cpu_engine, monkeypatch):
