@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--envelope", action="store_true",
                     help="--accuracy mode: also evolve FP64 from the start state perturbed by one ulp per entry "
                          "and report its distance from the unperturbed FP64 run (the FP64 engine's own envelope)")
+    ap.add_argument("--acc-chunk", type=int, default=0, metavar="K",
+                    help="promote the split GEMMs' tensor-core accumulation every K elements of K "
+                         "(reno_set_split_accumulation_chunk; 0 = off)")
     ap.add_argument("--accumulation", action="store_true",
                     help="the split GEMM's FP32 accumulation error on exactly representable operands, K = 64 .. 16384")
     ap.add_argument("--inject", default="",
@@ -757,10 +760,12 @@ def perturb_rel(mps, delta, seed):
 def run_accumulation(args):
     """Accumulation error of the split GEMM alone: operands exactly
     representable in the split's piece format (BF16 / TF32), so every
-    product is exact and only the tensor cores' FP32 accumulation rounds.
-    One JSON line per (sign, precision, K): normwise relative error against
-    FP64, the mean signed error over mean |C| (bias) and the fraction of
-    positive errors, for random-sign and all-positive operands."""
+    product is exact and only the accumulation rounds.  One JSON line per
+    (chunk, sign, precision, K): normwise relative error against FP64, the
+    mean signed error over mean |C| (bias) and the fraction of positive
+    errors, for random-sign and all-positive operands; chunk 0 is the
+    tensor cores' accumulation over all of K, chunk 128 the promoted form
+    (reno_set_split_accumulation_chunk)."""
     import torch
     from renormalizer_b200._native import Engine
     torch.cuda.set_device(0)
@@ -773,20 +778,24 @@ def run_accumulation(args):
         f = x.to(torch.float32)                     # TF32: 10 explicit mantissa bits
         return (f.view(torch.int32) & ~((1 << 13) - 1)).view(torch.float32).to(torch.float64)
 
-    for sign in ("random", "positive"):
-        for prec in ("bf16x3", "tf32x3"):
-            for K in (64, 256, 1024, 4096, 16384):
-                A = torch.randn(256, K, dtype=torch.float64, device="cuda", generator=g)
-                B = torch.randn(K, 256, dtype=torch.float64, device="cuda", generator=g)
-                if sign == "positive":
-                    A, B = A.abs(), B.abs()
-                A, B = exact(A, prec).contiguous(), exact(B, prec).contiguous()
-                C = eng.matmul(A, B, prec=prec)
-                ref = eng.matmul(A, B, prec="fp64")
-                err = C - ref
-                print(json.dumps({"sign": sign, "prec": prec, "K": K, "rel": float(err.norm() / ref.norm()),
-                                  "bias": float(err.mean() / ref.abs().mean()),
-                                  "frac_positive_errors": float((err > 0).double().mean())}), flush=True)
+    from renormalizer_b200._native import load_library
+    lib = load_library()
+    for chunk, sign, prec in [(c, s, p) for c in (0, 128) for s in ("random", "positive") for p in ("bf16x3", "tf32x3")]:
+        assert lib.reno_set_split_accumulation_chunk(chunk) == 0
+        for K in (64, 256, 1024, 4096, 16384):
+            A = torch.randn(256, K, dtype=torch.float64, device="cuda", generator=g)
+            B = torch.randn(K, 256, dtype=torch.float64, device="cuda", generator=g)
+            if sign == "positive":
+                A, B = A.abs(), B.abs()
+            A, B = exact(A, prec).contiguous(), exact(B, prec).contiguous()
+            C = eng.matmul(A, B, prec=prec)
+            ref = eng.matmul(A, B, prec="fp64")
+            err = C - ref
+            print(json.dumps({"chunk": chunk, "sign": sign, "prec": prec, "K": K,
+                              "rel": float(err.norm() / ref.norm()),
+                              "bias": float(err.mean() / ref.abs().mean()),
+                              "frac_positive_errors": float((err > 0).double().mean())}), flush=True)
+    lib.reno_set_split_accumulation_chunk(0)
 
 
 def run_accuracy(args):
@@ -823,7 +832,7 @@ def run_accuracy(args):
             out.flush()
 
     emit({"start": args.start, "start_s": t_start, "bond_dims": mps0.bond_dims, "nmol": args.nmol, "M": args.M,
-          "dt": args.dt, "arms": list(arms), "lockstep": bool(args.accuracy_lockstep),
+          "dt": args.dt, "arms": list(arms), "lockstep": bool(args.accuracy_lockstep), "acc_chunk": args.acc_chunk,
           "krylov_tol": args.krylov_tol or "1e-5,1e-8"})
     names = list(arms)
     for step in range(args.accuracy):
@@ -1129,6 +1138,9 @@ def main():
     if args.krylov_tol:
         tol = importlib.import_module("renormalizer_b200.krylov").tolerance
         tol.rtol, tol.atol = (float(x) for x in args.krylov_tol.split(","))
+    if args.acc_chunk:
+        from renormalizer_b200._native import load_library
+        assert load_library().reno_set_split_accumulation_chunk(args.acc_chunk) == 0
     if args.accumulation:
         run_accumulation(args)
         return

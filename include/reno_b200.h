@@ -129,6 +129,15 @@ int reno_device_error(reno_ctx* ctx, int32_t* code);
  * the tensor-core GEMM and the grid barriers of the eigensolver reduction --
  * for launches made after the call; 1 ms .. 60 s, default 2 s. */
 int reno_set_wait_limit_ns(uint64_t ns);
+/* Promoted accumulation of the split-precision products (no counterpart in
+ * the reference, which computes in FP64 on the host): the tensor cores'
+ * FP32 accumulation truncates toward zero, so its relative error is a bias
+ * that grows linearly with K.  With k_elems > 0, split GEMMs launched after
+ * the call accumulate each run of k_elems K elements (rounded to whole 64-
+ * (BF16) / 32- (TF32) element K tiles, at least one) in tensor memory and
+ * add the runs' partial sums into round-to-nearest FP32 registers; the bias
+ * then grows with k_elems instead of K.  0 (the default) turns it off. */
+int reno_set_split_accumulation_chunk(int32_t k_elems);
 /* Test hook of the failure path (no counterpart in the reference, which has
  * no device code): the NEXT launch of the named kernel has CTA 0 leave one
  * wait without its arrival, so that wait runs out after the limit above and

@@ -89,6 +89,7 @@ _SIGS = {
     "reno_qn_svd_truncate": (_c_int, [_vp, ctypes.POINTER(TruncDesc), _vp, _vp, _vp, _c_int, _vp, _vp,
                                       ctypes.POINTER(ctypes.c_int32), _vp, _c_sz]),
     "reno_set_wait_limit_ns": (_c_int, [ctypes.c_uint64]),
+    "reno_set_split_accumulation_chunk": (_c_int, [ctypes.c_int32]),
     "reno_test_skip_arrival": (_c_int, [ctypes.c_int32, ctypes.c_int32]),
     "reno_heff_apply_noalloc": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp, _vp]),
     "reno_heff_diag": (_c_int, [_vp, ctypes.POINTER(HeffDesc), _vp, _vp, _vp, _vp, _vp]),

@@ -53,6 +53,12 @@ extern "C" int reno_set_wait_limit_ns(uint64_t ns) {
   return RENO_OK;
 }
 
+extern "C" int reno_set_split_accumulation_chunk(int32_t k_elems) {
+  if (k_elems < 0) return RENO_ERR_INVALID;
+  g_split_chunk_k.store(k_elems, std::memory_order_relaxed);
+  return RENO_OK;
+}
+
 extern "C" int reno_test_skip_arrival(int32_t kind, int32_t at) {
   if (at < -1) return RENO_ERR_INVALID;
   if (kind == RENO_SKIP_SPLIT_STAGE) g_skip_split_stage.store(at);

@@ -31,6 +31,9 @@ inline std::atomic<unsigned long long> g_wait_ns{2000000000ull};
 // without its arrival, so the bounded wait runs out and the kernel returns
 // with its error status set.  -1 = none.
 inline std::atomic<int> g_skip_split_stage{-1};
+// K elements per promoted accumulation chunk of the split GEMM (0 = off),
+// reno_set_split_accumulation_chunk
+inline std::atomic<int> g_split_chunk_k{0};
 inline std::atomic<int> g_skip_hetrd_column{-1};
 
 // every kernel launch of the library bumps this (host-side, per process)

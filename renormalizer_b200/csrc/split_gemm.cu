@@ -250,19 +250,14 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 // (32 columns at a time) -> the output in the Epi mode.  Warp w reads TMEM
 // lane quarter q = w % 4, i.e. tile rows q*32 .. q*32+31; two warps share a
 // quarter, each taking half of the BN columns.
+// Output of 32 accumulated columns c0 .. c0+31 of tile row q*32 + lane in the
+// Epi mode.
 template <int ESZ>
-__device__ __forceinline__ void epilogue_tile(const Epi& epi, uint32_t tacc, int q, int lane, int m_tile, int n_tile,
-                                              int bz, int c_begin, int c_end) {
+__device__ __forceinline__ void epilogue_store(const Epi& epi, const float* v, int q, int lane, int m_tile, int n_tile,
+                                               int bz, int c0) {
   const int row = q * 32 + lane;  // tile row of this thread
   const int rp = m_tile * BM + row;
-  for (int c0 = c_begin; c0 < c_end; c0 += 32) {
-    uint32_t r[32];
-    const uint32_t taddr = tacc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
-    TMEM_LD32(taddr, r);
-    asm volatile("tcgen05.wait::ld.sync.aligned;");
-    float v[32];
-#pragma unroll
-    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+  {
     const int cp = n_tile * BN + c0;  // product column of v[0]
     if (epi.mode == OUT_PACK) {
       const int m = epi.inter == 1 ? (rp >> 1) : rp;
@@ -336,6 +331,21 @@ __device__ __forceinline__ void epilogue_tile(const Epi& epi, uint32_t tacc, int
   }
 }
 
+template <int ESZ>
+__device__ __forceinline__ void epilogue_tile(const Epi& epi, uint32_t tacc, int q, int lane, int m_tile, int n_tile,
+                                              int bz, int c_begin, int c_end) {
+  for (int c0 = c_begin; c0 < c_end; c0 += 32) {
+    uint32_t r[32];
+    const uint32_t taddr = tacc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+    TMEM_LD32(taddr, r);
+    asm volatile("tcgen05.wait::ld.sync.aligned;");
+    float v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+    epilogue_store<ESZ>(epi, v, q, lane, m_tile, n_tile, bz, c0);
+  }
+}
+
 // tile t of the (bz, slow, fast) raster: M tiles fastest when m_fast
 __device__ __forceinline__ void tile_coords(int t, int mt, int nt, int m_fast, int& m_tile, int& n_tile, int& bz) {
   const int per = mt * nt;
@@ -376,12 +386,20 @@ __device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity, uint6
 // (MMA -> epilogue, per buffer, tcgen05.commit), tmem_empty (epilogue -> MMA,
 // per buffer, one arrive per epilogue warp, 8 warps), drain (the MMA thread's last
 // commit, waited for before TMEM is freed).
-template <int ESZ>
+//
+// PROMOTE (opt-in, reno_set_split_accumulation_chunk): the tensor cores'
+// FP32 accumulation truncates, so its error is a bias that grows with the
+// number of terms.  In this form a tile's K range is cut into chunks of kc K
+// tiles; each chunk accumulates in one TMEM buffer (the two buffers
+// alternate chunk by chunk, so the MMA fills one while the epilogue reads the
+// other), and the epilogue warps add every chunk's partial sums into FP32
+// registers with round-to-nearest additions before the tile's output.
+template <int ESZ, bool PROMOTE>
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                       const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, Epi epi,
                       int num_k_tiles, int k_elems, int a_batched, int b_batched, int m_fast, int mt, int nt,
-                      int ntiles, uint64_t wait_ns, int skip_stage) {
+                      int ntiles, uint64_t wait_ns, int skip_stage, int kc) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -457,14 +475,20 @@ __global__ void __launch_bounds__(THREADS, 1)
                            ((uint32_t)(BM >> 4) << 24);
     uint32_t g = 0;
     bool ok = true;
-    int i = 0;
-    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
+    int i = 0;  // accumulation units: tiles, or (tile, chunk) pairs under PROMOTE
+    const int chunk = PROMOTE ? kc : num_k_tiles;
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x)
+     for (int k0 = 0; k0 < num_k_tiles && ok; k0 += chunk, ++i) {
       const int b = i & 1;
       const uint32_t use = (uint32_t)(i >> 1);
-      if (!mbar_wait(&tmem_empty[b], (use & 1) ^ 1, abort_flag, 4, wait_ns)) break;
+      if (!mbar_wait(&tmem_empty[b], (use & 1) ^ 1, abort_flag, 4, wait_ns)) {
+        ok = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t tacc = tmem + (uint32_t)(b * TMEM_COLS);
-      for (int kt = 0; kt < num_k_tiles; ++kt) {
+      const int k1 = min(num_k_tiles, k0 + chunk);
+      for (int kt = k0; kt < k1; ++kt) {
         const int s = g % STAGES;
         const uint32_t ph = (g / STAGES) & 1;
         if (!mbar_wait(&full[s], ph, abort_flag, 2, wait_ns)) {
@@ -483,7 +507,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int kk = 0; kk < 4; ++kk) {
           if (kk < nsub) {
             const uint64_t adv = (uint64_t)((kk * 32) >> 4);  // 32 bytes of K per instruction
-            const uint32_t first = (kt == 0 && kk == 0) ? 0u : 1u;
+            const uint32_t first = (kt == k0 && kk == 0) ? 0u : 1u;
             umma<ESZ>(tacc, dah + adv, dbh + adv, idesc, first);
             umma<ESZ>(tacc, dah + adv, dbl + adv, idesc, 1u);
             umma<ESZ>(tacc, dal + adv, dbh + adv, idesc, 1u);
@@ -502,6 +526,39 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int q = warp % 4;                      // TMEM lane quarter this warp may access
     const int c_begin = ((warp - 2) / 4) * (BN / 2);  // warps 2-5: columns [0, BN/2), warps 6-9: the rest
     int i = 0;
+    if constexpr (PROMOTE) {
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        float acc[BN / 2];  // this thread's row, columns c_begin .. c_begin + BN/2 - 1
+        for (int k0 = 0; k0 < num_k_tiles; k0 += kc, ++i) {
+          const int b = i & 1;
+          const uint32_t use = (uint32_t)(i >> 1);
+          if (!mbar_wait(&tmem_full[b], use & 1, abort_flag, 3, wait_ns) || *abort_flag) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t tacc = tmem + (uint32_t)(b * TMEM_COLS) + ((uint32_t)(q * 32) << 16) + (uint32_t)c_begin;
+#pragma unroll
+          for (int p = 0; p < BN / 64; ++p) {
+            uint32_t r[32];
+            TMEM_LD32(tacc + (uint32_t)(32 * p), r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              acc[32 * p + j] = k0 == 0 ? __uint_as_float(r[j]) : __fadd_rn(acc[32 * p + j], __uint_as_float(r[j]));
+          }
+          asm volatile("tcgen05.fence::before_thread_sync;");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tmem_empty[b]);
+        }
+        if (!ok) break;
+        int m_tile, n_tile, bz;
+        tile_coords(t, mt, nt, m_fast, m_tile, n_tile, bz);
+#pragma unroll
+        for (int p = 0; p < BN / 64; ++p) epilogue_store<ESZ>(epi, acc + 32 * p, q, lane, m_tile, n_tile, bz, c_begin + 32 * p);
+      }
+    } else {
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
       const int b = i & 1;
       const uint32_t use = (uint32_t)(i >> 1);
@@ -515,6 +572,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
       if (lane == 0) mbar_arrive(&tmem_empty[b]);
+    }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -813,12 +871,15 @@ static cudaError_t launch_split(const SplitPacked& A, const SplitPacked& B, int 
     epi.accumulate = c->accumulate;
     epi.c_f32 = c->c_f32;
   }
-  static std::atomic<unsigned long long> smem_set{0};
+  const int64_t kstep = KROW_BYTES / ESZ;
+  const int chunk_k = g_split_chunk_k.load(std::memory_order_relaxed);
+  const int kc = chunk_k > 0 ? (int)std::max<int64_t>(1, chunk_k / kstep) : 0;
+  static std::atomic<unsigned long long> smem_set{0}, smem_set_p{0};
   {
-    cudaError_t e = smem_optin_once(split_gemm_kernel<ESZ>, SMEM_BYTES, smem_set);
+    cudaError_t e = kc > 0 ? smem_optin_once(split_gemm_kernel<ESZ, true>, SMEM_BYTES, smem_set_p)
+                           : smem_optin_once(split_gemm_kernel<ESZ, false>, SMEM_BYTES, smem_set);
     if (e != cudaSuccess) return e;
   }
-  const int64_t kstep = KROW_BYTES / ESZ;
   const int64_t mt = ceil_div(A.rows, BM), nt = ceil_div(B.rows, BN);
   // walk the smaller operand's tiles fastest (packed rows per batch decide)
   const int m_fast = (A.rows <= B.rows && mt > 1) ? 1 : 0;
@@ -827,11 +888,17 @@ static cudaError_t launch_split(const SplitPacked& A, const SplitPacked& B, int 
   const int sms = sm_count_current_device();
   const int grid = (int)std::min<int64_t>(ntiles, sms);  // one persistent CTA per SM
   count_launch();
-  split_gemm_kernel<ESZ><<<grid, THREADS, SMEM_BYTES, st>>>(tAh, tAl, tBh, tBl, epi, (int)ceil_div(A.kext, kstep),
-                                                            (int)A.kext, A.nb > 1 ? 1 : 0, B.nb > 1 ? 1 : 0, m_fast,
-                                                            (int)mt, (int)nt, (int)ntiles,
-                                                            (uint64_t)g_wait_ns.load(std::memory_order_relaxed),
-                                                            g_skip_split_stage.exchange(-1));
+  const uint64_t wait_ns = g_wait_ns.load(std::memory_order_relaxed);
+  const int skip = g_skip_split_stage.exchange(-1);
+  const int nkt = (int)ceil_div(A.kext, kstep);
+  if (kc > 0)
+    split_gemm_kernel<ESZ, true><<<grid, THREADS, SMEM_BYTES, st>>>(
+        tAh, tAl, tBh, tBl, epi, nkt, (int)A.kext, A.nb > 1 ? 1 : 0, B.nb > 1 ? 1 : 0, m_fast, (int)mt, (int)nt,
+        (int)ntiles, wait_ns, skip, kc);
+  else
+    split_gemm_kernel<ESZ, false><<<grid, THREADS, SMEM_BYTES, st>>>(
+        tAh, tAl, tBh, tBl, epi, nkt, (int)A.kext, A.nb > 1 ? 1 : 0, B.nb > 1 ? 1 : 0, m_fast, (int)mt, (int)nt,
+        (int)ntiles, wait_ns, skip, 0);
   return cudaGetLastError();
 }
 

@@ -157,3 +157,48 @@ def test_split_tdvp_short_trajectory(prec, atol):
         backend.prec = "fp64"
     dev = np.abs(np.array(pops) - TDVP["ps_hol4/pops"]).max()
     assert dev < atol, dev
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+def test_split_promoted_accumulation(prec):
+    """reno_set_split_accumulation_chunk: on operands the split represents
+    exactly (so only the accumulation rounds), all-positive, K = 4096, the
+    tensor cores' accumulation leaves every output too small (truncation);
+    promoting every 128 K elements into round-to-nearest FP32 cuts the bias by
+    more than 8x, keeps complex / tile-edge products within the split
+    tolerance, and switching it off restores the default kernel's results
+    bit for bit."""
+    from renormalizer_b200._native import Engine, load_library
+    eng, lib = Engine.get(0), load_library()
+    g = torch.Generator(device="cuda").manual_seed(2)
+
+    def exact(x):
+        if prec == "bf16x3":
+            return x.to(torch.bfloat16).to(torch.float64)
+        f = x.to(torch.float32)
+        return (f.view(torch.int32) & ~((1 << 13) - 1)).view(torch.float32).to(torch.float64)
+
+    A = exact(torch.rand(256, 4096, dtype=torch.float64, device="cuda", generator=g)).contiguous()
+    B = exact(torch.rand(4096, 256, dtype=torch.float64, device="cuda", generator=g)).contiguous()
+    ref = eng.matmul(A, B, prec="fp64")
+    try:
+        plain = eng.matmul(A, B, prec=prec)
+        assert lib.reno_set_split_accumulation_chunk(128) == 0
+        prom = eng.matmul(A, B, prec=prec)
+        bias_plain = float((plain - ref).mean() / ref.mean())
+        bias_prom = float((prom - ref).mean() / ref.mean())
+        assert bias_plain < 0 and bool(((plain - ref) < 0).all())
+        assert abs(bias_prom) * 8 < abs(bias_plain), (bias_plain, bias_prom)
+        # general operands through the promoted kernel: complex, ragged tiles
+        Ac = torch.complex(torch.randn(300, 777, dtype=torch.float64, device="cuda", generator=g),
+                           torch.randn(300, 777, dtype=torch.float64, device="cuda", generator=g))
+        Bc = torch.randn(777, 190, dtype=torch.float64, device="cuda", generator=g)
+        c_ref = eng.matmul(Ac, Bc, prec="fp64")
+        c_prom = eng.matmul(Ac, Bc, prec=prec)
+        tol = 5e-5 if prec == "bf16x3" else 5e-6
+        assert float((c_prom - c_ref).abs().max() / c_ref.abs().max()) < tol
+    finally:
+        assert lib.reno_set_split_accumulation_chunk(0) == 0
+    assert torch.equal(eng.matmul(A, B, prec=prec), plain)
+    assert eng.device_error() == 0
