@@ -57,6 +57,7 @@ ACCURACY_200 = {"steps": 200, "nmol": 8, "max_abs_dpop": {"bf16x3": 1.074e-5, "t
                 "fp64_envelope": 1.63e-9, "first_step_above_1e-6": {"bf16x3": 24, "tf32x3": 29},
                 "holds_1e-6": False, "record": "profiles/accuracy_tdvp_ps2_holstein24_M256.md",
                 "fp64_random_1e-9_per_step_30_steps": 9.3e-9,
+                "promoted_accumulation_chunk128_max": {"tf32x3 (25 steps)": 7.95e-8, "bf16x3 (30 steps)": 3.09e-6},
                 "cause": "the tensor cores' FP32 accumulation truncates toward zero: a bias linear in K "
                          "(-1.4e-5 BF16x3, -3.0e-5 TF32x3 relative at K = 4096, bench.py --accumulation)"}
 
